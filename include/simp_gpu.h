@@ -1,0 +1,199 @@
+/*
+ * simp_gpu.h — C ABI of the B200 (sm_100a) implementation of SIMP's per-step
+ * Smoothed Particle Hydrodynamics hot path.
+ *
+ * SIMP's Fortran host talks to its physics through argument-less subroutines
+ * that read and write module globals (fortran/src/modules/data_variables.f90:
+ * 26-124).  This library keeps those globals resident on the GPU between calls
+ * and exposes one entry point per reference subroutine on the path, with plain
+ * pointers and sizes only, so an ISO_C_BINDING interface block can bind them
+ * directly (see fortran/shim/simp_gpu_mod.f90 in this repository).
+ *
+ * Conventions shared by every entry point:
+ *   - Return value: SIMP_OK (0) or one of the SIMP_ERR_* codes below.  The
+ *     reference STOPs with a banner on the same conditions; here the caller
+ *     gets the code plus the banner text from simp_gpu_last_error().
+ *   - Host arrays use the reference's Fortran layout: a 2-vector field such as
+ *     x(dim, maxn) is interleaved [x1, y1, x2, y2, ...] (column-major), scalar
+ *     fields are double[n].  Pair indices are 1-based like p_i/p_j.
+ *   - All arithmetic is IEEE FP64 unless the context was created with
+ *     precision = SIMP_PREC_MIXED (FP32 pair sums with Kahan compensation,
+ *     FP64 positions, integrator state and reductions).
+ *   - A context is bound to one CUDA stream and is not thread-safe; the
+ *     reference calls single_step from one thread (time_integration.f90:204).
+ *   - The library owns all device memory; host arrays stay the caller's.
+ */
+#ifndef SIMP_GPU_H
+#define SIMP_GPU_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SIMP_API __attribute__((visibility("default")))
+#else
+#define SIMP_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+enum {
+    SIMP_OK = 0,
+    SIMP_ERR_BADARG = 1,    /* unsupported switch, null pointer, bad size      */
+    SIMP_ERR_MAXN = 2,      /* ntotal > maxn: initialize.f90:156-163           */
+    SIMP_ERR_PAIR_CAP = 3,  /* too many pairs: nnps.f90:132-139, 415-423       */
+    SIMP_ERR_IND_INT = 4,   /* > max_ind_int interactions: nnps.f90:660-668    */
+    SIMP_ERR_CUDA = 5,      /* CUDA runtime error (message in last_error)      */
+    SIMP_ERR_NONFINITE = 6, /* NaN/Inf in the state after a step               */
+    SIMP_ERR_TIMEOUT = 7,   /* a bounded device-side wait gave up              */
+    SIMP_ERR_NOMEM = 8,     /* device allocation failed                        */
+    SIMP_ERR_STATE = 9      /* entry point called before simp_gpu_set_state    */
+};
+
+/* Smoothing kernel selector: the reference's skf codes (globals.f90:136-147). */
+enum {
+    SIMP_SKF_WENDLAND_C6 = 6, /* kernel.f90:471-520, boundary_kernel.f90:438-504 */
+    SIMP_SKF_CUBIC = 9        /* kernel.f90:297-352 (commented out in the
+                                 reference, restored here with scale_h = 2)     */
+};
+
+enum { SIMP_PREC_FP64 = 0, SIMP_PREC_MIXED = 1 };
+enum { SIMP_WIND_UNIFORM = 0, SIMP_WIND_VORTEX = 1 };
+
+/*
+ * Every switch and constant the hot path reads.  The reference holds these as
+ * compile-time PARAMETERs (globals.f90:58-187, data_variables.f90:153-180);
+ * simp_params_reference_default() fills in the shipped values.
+ */
+typedef struct simp_params {
+    /* algorithm switches, reference codes */
+    int32_t int_algorithm;     /* 2 predictor-corrector (time_integration.f90:155-282) */
+    int32_t nnps_algorithm;    /* 2 bucket search, 1 direct find (nnps.f90:21-30)       */
+    int32_t sle;               /* 0 keep hsml, 2 Marquis hsml (smoothing_length.f90)    */
+    int32_t tse;               /* 0 keep dt, 2 VP criterion (time_step.f90:132-157)     */
+    int32_t rheology;          /* 1 elliptical yield curve                              */
+    int32_t eos_alg;           /* 1 Hibler, 3 Kreyscher replacement pressure            */
+    int32_t pa_sph;            /* 1 (p_i/rho_i^2 + p_j/rho_j^2) form                    */
+    int32_t skf;               /* SIMP_SKF_*                                            */
+    int32_t den_alg;           /* 3 diagnostic, 1 summation (density.f90:20-30)         */
+    int32_t bfa;               /* 1 Monaghan boundary force                             */
+    int32_t viscosity;         /* globals.f90:180-187 logical switches (0/1)            */
+    int32_t pressure_force;
+    int32_t wind_force;
+    int32_t water_force;
+    int32_t boundary_pressure;
+    int32_t boundary_friction; /* must be 0: friction branch not on this path          */
+    int32_t mass_from_area;    /* 1: mass_update_from_area when sle is 0 or 1 (as the
+                                  reference); 0: particle mass held constant         */
+    int32_t max_ind_int;       /* 200 (globals.f90:24)                                 */
+    int32_t hsml_multiplicity; /* 3 (data_variables.f90:105)                           */
+    int32_t wind_kind;         /* SIMP_WIND_*                                          */
+    int32_t precision;         /* SIMP_PREC_*                                          */
+    int32_t reserved0;
+    /* material constants */
+    double P_star, c_eos, e, delta_min, k_t;
+    double rho_ice, rho_air, rho_water, c_wind, c_water;
+    double b_length, kappa_n, kappa_t;
+    double alpha;              /* area factor of mass_update_from_area                 */
+    /* forcing */
+    double wind_u, wind_v;     /* uniform wind (m/s)                                   */
+    double current_u, current_v;
+    double vortex_x, vortex_y, vortex_umax, vortex_radius;
+    /* numerics */
+    double dt;                 /* fixed (tse = 0) or initial time step (s)             */
+    double max_hsml;           /* Marquis_hsml cap; <= 0: 10 * max(hsml) at set_state
+                                  (initialize.f90:191)                                */
+    double skin;               /* GPU cell-list skin (m); < 0: automatic               */
+} simp_params;
+
+/* Shipped values of globals.f90 and data_variables.f90, including the
+ * reference's default-real literals (rho_air = 1.3 is stored as the
+ * single-precision value 1.2999999523162842). */
+SIMP_API void simp_params_reference_default(simp_params *p);
+
+typedef struct simp_ctx simp_ctx;
+
+/* Allocate device storage for up to maxn particles and maxnb boundary
+ * particles (the reference's maxn / maxnb capacities, globals.f90:21-25). */
+SIMP_API int32_t simp_gpu_create(const simp_params *params, int32_t maxn, int32_t maxnb,
+                        simp_ctx **out);
+SIMP_API int32_t simp_gpu_destroy(simp_ctx *ctx);
+
+/* Upload the particle and boundary state (the globals initialize.f90:
+ * particle_placing / boundary_placing_1 produce).  x and vx are interleaved
+ * 2*ntotal arrays, xb is 2*ntotalb.  dt and current_time are the
+ * integrator's.  Returns SIMP_ERR_MAXN when ntotal > maxn. */
+SIMP_API int32_t simp_gpu_set_state(simp_ctx *ctx, int32_t ntotal, const double *x,
+                           const double *vx, const double *mass,
+                           const double *rho, const double *hsml,
+                           const double *A, const double *h, int32_t ntotalb,
+                           const double *xb, const double *massb, double dt,
+                           double current_time);
+
+/* Download the state in the caller's original particle order.  Any pointer
+ * may be NULL to skip that field. */
+SIMP_API int32_t simp_gpu_get_state(simp_ctx *ctx, double *x, double *vx, double *mass,
+                           double *rho, double *hsml, double *A, double *h,
+                           double *dt, double *current_time);
+
+/* Diagnostics of the last kinematic pass (the globals epsilon_11..sigma_22,
+ * zeta, eta, p after single_step).  Only valid when diagnostics were kept:
+ * single_step always keeps them; simp_gpu_step keeps them when
+ * simp_gpu_keep_diag(ctx, 1) was called. */
+SIMP_API int32_t simp_gpu_keep_diag(simp_ctx *ctx, int32_t keep);
+SIMP_API int32_t simp_gpu_get_diag(simp_ctx *ctx, double *eps11, double *eps12,
+                          double *eps22, double *zeta, double *eta, double *p,
+                          double *sig11, double *sig12, double *sig22);
+
+/* NNPS (nnps.f90:5-30 -> bucket_search :155-517).  Emits the unordered pair
+ * set with the reference's bucket-search semantics, sorted by (p_i, p_j) with
+ * p_i < p_j, 1-based original indices.  r_ij and hsml_ij are bit-exact FP64.
+ * Boundary pairs are (bp_i = boundary index, bp_j = particle index) sorted by
+ * (bp_i, bp_j).  nip / bnip always receive the true counts; when they exceed
+ * cap / bcap the arrays hold the first cap / bcap entries and
+ * SIMP_ERR_PAIR_CAP is returned.  Any array pointer may be NULL. */
+SIMP_API int32_t simp_gpu_nnps(simp_ctx *ctx, int32_t *nip, int32_t *p_i, int32_t *p_j,
+                      double *r_ij, double *hsml_ij, int32_t cap,
+                      int32_t *bnip, int32_t *bp_i, int32_t *bp_j,
+                      double *br_ij, int32_t bcap);
+
+/* One right-hand-side evaluation, single_step.f90:5-109, on the resident
+ * state at the given current_time (drag is off while current_time <= 0,
+ * wind_forcing.f90:35).  Outputs are interleaved 2*ntotal (dxdt, dvxdt) or
+ * ntotal (dhdt, dAdt) in the original particle order; any may be NULL. */
+SIMP_API int32_t simp_gpu_single_step(simp_ctx *ctx, double current_time, double *dxdt,
+                             double *dvxdt, double *dhdt, double *dAdt);
+
+/* Density pair sum, density.f90:41-100 (sum_density), on the resident state:
+ * rho_out[i] = (k0_i m_i + sum_j m_j W_ij) / (k0_i m_i / rho_i +
+ * sum_j m_j W_ij / rho_j), k0_i = W(0) with hsml_i. */
+SIMP_API int32_t simp_gpu_sum_density(simp_ctx *ctx, double *rho_out);
+
+/* Advance nsteps predictor-corrector steps (time_integration.f90:146-181 with
+ * predictor_corrector :263-390), state resident on the device.  On return
+ * *current_time and *dt hold the integrator's values; current_time advances
+ * by the dt computed at the end of each step, as the reference does
+ * (time_integration.f90:179). */
+SIMP_API int32_t simp_gpu_step(simp_ctx *ctx, int32_t nsteps, double *current_time,
+                      double *dt);
+
+/* Interaction statistics of the last NNPS (nnps.f90:613-670): maximal,
+ * minimal and summed per-particle interaction counts (boundary pairs
+ * included) and the number of particles without interactions. */
+SIMP_API int32_t simp_gpu_interaction_stats(simp_ctx *ctx, int32_t *maxip,
+                                   int32_t *minip, int64_t *sumip,
+                                   int32_t *noip);
+
+/* Human-readable text of the last error on this context ("" if none). */
+SIMP_API const char *simp_gpu_last_error(const simp_ctx *ctx);
+
+/* Library version string. */
+SIMP_API const char *simp_gpu_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SIMP_GPU_H */

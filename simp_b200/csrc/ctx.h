@@ -1,0 +1,99 @@
+// Host-side context of one resident basin (the C ABI's opaque simp_ctx).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+struct simp_ctx {
+    simp_params prm{};
+    simp::Phys phys{};
+    int maxn = 0, maxnb = 0;
+    int n = 0, nb = 0;
+    bool have_state = false;
+    bool keep_diag = false;
+    std::string err;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+
+    // particle state sets (device, cell order)
+    simp::State s0{}, s1{};
+    double *mass1 = nullptr;       // half-step mass when the mass update is on
+    double *xr = nullptr, *yr = nullptr;  // positions at the last rebuild
+    int *cell = nullptr;           // rebuild-time cell id per particle
+    int *id = nullptr;             // original index per particle
+    int *inv_id = nullptr;         // cell-order position of original index
+    // per-RHS intermediates from the kinematic pass
+    double *tau11 = nullptr, *tau12 = nullptr, *tau22 = nullptr, *div = nullptr;
+    // diagnostics (epsilon_11.. sigma_22, zeta, eta, p)
+    double *diag = nullptr;        // 9 * maxn
+    // rates of the last single_step (cell order): ax, ay, dhdt, dAdt
+    double *rates = nullptr;       // 4 * maxn
+    // boundary particles (cell order in the same grid)
+    double *bx = nullptr, *by = nullptr, *bm = nullptr;
+    int *bid = nullptr;            // original wall index per wall slot
+    int *bcell = nullptr;          // cell id per wall slot
+    int *bcell_start = nullptr;
+    // cell grid
+    simp::Grid grid{};
+    int *cell_start = nullptr;
+    size_t cell_cap = 0;
+    // rebuild scratch
+    int *cnt = nullptr;            // per-cell counters (cell_cap)
+    int *perm = nullptr;           // maxn
+    double *tmp = nullptr;         // maxn * 12 doubles reorder scratch
+    int *itmp = nullptr;           // maxn * 3 ints
+    void *scan_tmp = nullptr;
+    size_t scan_tmp_bytes = 0;
+    // scalars
+    simp::Scalars *sc = nullptr;
+    simp::Scalars *sc_host = nullptr;  // pinned mirror: [0] synchronous reads,
+                                       // [1..kSnapRing] per-step snapshots
+    // host copies of the walls (re-binned when the grid is resized)
+    std::vector<double> host_xb, host_massb;
+    // NNPS export scratch
+    int *pair_cnt = nullptr;       // maxn + 1
+    int *bpair_cnt = nullptr;      // maxnb + 1
+    int *pair_buf_i = nullptr, *pair_buf_j = nullptr;
+    double *pair_buf_r = nullptr, *pair_buf_h = nullptr;
+    size_t pair_buf_cap = 0;
+    // step graph
+    cudaGraphExec_t step_graph = nullptr;
+    bool graph_diag = false;
+    // rebuild policy
+    int steps_since_rebuild = 0;
+    long long rebuilds = 0;
+};
+
+namespace simp {
+
+// cell_list.cu
+int rebuild(simp_ctx *c);               // sort particles into cell order
+void launch_scan_i32(const int *in, int *out, int n, void *tmp, cudaStream_t s);
+size_t scan_tmp_bytes(int n);
+
+// passes.cu
+enum EpiMode : int { EPI_RATES = 0, EPI_PREDICT = 1, EPI_CORRECT = 2 };
+void launch_kinematic(simp_ctx *c, const State &s, bool diag);
+void launch_stress(simp_ctx *c, const State &nb, const State &own, EpiMode mode);
+void launch_step_finish(simp_ctx *c);
+void launch_reset_stats(simp_ctx *c);
+
+// nnps_export.cu
+int export_pairs(simp_ctx *c, int32_t *nip, int32_t *p_i, int32_t *p_j, double *r_ij,
+                 double *hsml_ij, int32_t cap, int32_t *bnip, int32_t *bp_i, int32_t *bp_j,
+                 double *br_ij, int32_t bcap);
+int sum_density(simp_ctx *c, double *rho_out_dev);
+
+}  // namespace simp
+
+int simp_fail(simp_ctx *c, int code, const std::string &msg);
+int simp_cuda_check(simp_ctx *c, cudaError_t e, const char *what);
+#define SIMP_CUDA(c, expr)                                        \
+    do {                                                          \
+        cudaError_t _e = (expr);                                  \
+        if (_e != cudaSuccess) return simp_cuda_check(c, _e, #expr); \
+    } while (0)

@@ -1,0 +1,187 @@
+"""Parity of the CUDA path (through the C ABI) with the FP64 CPU oracle.
+
+Bars: neighbour lists bit-exact as sorted index sets, with r_ij, hsml_ij and
+br_ij bit-exact; FP64 fields within a relative L2 tolerance stated per test
+(the GPU gathers each pair from both sides, so only the summation order
+differs from the reference's scatter loop).
+"""
+import numpy as np
+import pytest
+
+from helpers import assert_same_pairs, rel_l2, smooth_velocity
+from simp_b200 import basins
+from simp_b200.params import SKF_WENDLAND_C6
+from simp_b200.simp import (SIMP_ERR_IND_INT, SIMP_ERR_MAXN, SIMP_ERR_PAIR_CAP, Simp,
+                            SimpError)
+
+pytestmark = pytest.mark.gpu
+
+# FP64, one right-hand side on identical inputs: summation order only.
+TOL_RHS = 1e-11
+# FP64 trajectories: order-of-summation differences amplified by the
+# non-smooth VP rheology over the stated number of steps.
+TOL_TRAJ_20 = 1e-8
+
+
+def _pair(b, oracle_mod, params=None):
+    prm = b.params if params is None else params
+    g = Simp.from_basin(b, prm)
+    o = oracle_mod.Oracle.from_basin(b, prm)
+    return g, o
+
+
+def test_library_version(gpu_lib):
+    from simp_b200.simp import version
+    assert "sm_100a" in version()
+
+
+@pytest.mark.parametrize("cfg", ["cfg1", "cfg1_c6", "cfg1_direct"])
+def test_nnps_bit_exact_cfg1(gpu_lib, oracle_mod, cfg):
+    b = basins.cfg1()
+    prm = b.params.copy()
+    if cfg == "cfg1_c6":
+        prm.skf = SKF_WENDLAND_C6
+    if cfg == "cfg1_direct":
+        prm.nnps_algorithm = 1   # direct_find (nnps.f90:41-148): same pair set
+    g, o = _pair(b, oracle_mod, prm)
+    assert_same_pairs(g.nnps(), o.nnps())
+    assert g.interaction_stats() == o.interaction_stats()
+
+
+def test_nnps_bit_exact_cfg2(gpu_lib, oracle_mod):
+    b = basins.cfg2()
+    g, o = _pair(b, oracle_mod)
+    assert_same_pairs(g.nnps(), o.nnps())
+
+
+def test_nnps_after_motion(gpu_lib, oracle_mod):
+    """Pair sets stay exact after particles moved (cell list not re-sorted)."""
+    b = basins.cfg1()
+    g, o = _pair(b, oracle_mod)
+    g.time_integration(30)
+    st = g.get_state()
+    o.set_state(st["x"], st["vx"], st["mass"], st["rho"], st["hsml"], st["A"], st["h"],
+                b.xb, b.massb, b.params.dt, st["current_time"])
+    assert_same_pairs(g.nnps(), o.nnps())
+
+
+def test_nnps_variable_hsml_bucket_rule(gpu_lib, oracle_mod):
+    """max(hsml) > 2 min(hsml): the reference's bucket stencil drops pairs."""
+    b = basins.cfg1()
+    rng = np.random.default_rng(7)
+    b.hsml = b.hsml * rng.uniform(0.45, 1.05, size=b.n)
+    g, o = _pair(b, oracle_mod)
+    rg, ro = g.nnps(), o.nnps()
+    assert_same_pairs(rg, ro)
+    # the rule is active: brute force finds more pairs than the bucket search
+    prm = b.params.copy()
+    prm.nnps_algorithm = 1
+    o2 = oracle_mod.Oracle.from_basin(b, prm)
+    assert o2.nnps()["nip"] > ro["nip"]
+
+
+def test_nnps_ties_and_half_buckets(gpu_lib, oracle_mod):
+    """Unjittered lattice: pairs at exactly d == mhsml are kept (<=), and
+    positions sit exactly on bucket half-boundaries (NINT ties)."""
+    b = basins.make_basin(24, 1000.0, 3, jitter=0.0, walls="+x-x+y-y")
+    b.hsml[:] = 2000.0          # mhsml = 2 dx = exact lattice distance
+    b.x += 500.0                # x / (2 min hsml) = k / 4: every other column is a NINT tie
+    b.xb += 500.0
+    g, o = _pair(b, oracle_mod)
+    rg, ro = g.nnps(), o.nnps()
+    assert_same_pairs(rg, ro)
+    # every interior particle has the 12 lattice neighbours within 2 dx
+    assert ro["nip"] > 0
+
+
+def test_nnps_pair_capacity(gpu_lib, oracle_mod):
+    b = basins.cfg1()
+    g = Simp.from_basin(b)
+    with pytest.raises(SimpError) as e:
+        g.nnps(cap=100)
+    assert e.value.code == SIMP_ERR_PAIR_CAP
+
+
+def test_maxn_error(gpu_lib):
+    b = basins.cfg1()
+    g = Simp(b.params, b.n - 1, b.nb)
+    with pytest.raises(SimpError) as e:
+        g.set_state(b.x, b.vx, b.mass, b.rho, b.hsml, b.A, b.h, b.xb, b.massb, 1.0)
+    assert e.value.code == SIMP_ERR_MAXN
+
+
+def test_max_ind_int_error(gpu_lib):
+    b = basins.cfg1()
+    prm = b.params.copy()
+    prm.max_ind_int = 10
+    g = Simp.from_basin(b, prm)
+    with pytest.raises(SimpError) as e:
+        g.time_integration(1)
+    assert e.value.code == SIMP_ERR_IND_INT
+
+
+@pytest.mark.parametrize("skf", [9, 6])
+def test_single_step_fields(gpu_lib, oracle_mod, skf):
+    """One RHS (single_step.f90) on a sheared, drifting state with drag on."""
+    b = basins.cfg1()
+    b.vx = smooth_velocity(b.x, b.L, seed=skf)
+    prm = b.params.copy()
+    prm.skf = skf
+    g, o = _pair(b, oracle_mod, prm)
+    rg, ro = g.single_step(3600.0), o.single_step(3600.0)
+    for k in ("dxdt", "dvxdt", "dhdt", "dAdt"):
+        assert rel_l2(rg[k], ro[k]) < TOL_RHS, (k, rel_l2(rg[k], ro[k]))
+    dg, do = g.get_diag(), o.get_diag()
+    for k in dg:
+        assert rel_l2(dg[k], do[k]) < TOL_RHS, (k, rel_l2(dg[k], do[k]))
+
+
+def test_single_step_at_rest_no_drag(gpu_lib, oracle_mod):
+    """t = 0, v = 0: strain, stress and drag vanish; only walls act."""
+    b = basins.cfg1()
+    g, o = _pair(b, oracle_mod)
+    rg, ro = g.single_step(0.0), o.single_step(0.0)
+    assert rel_l2(rg["dvxdt"], ro["dvxdt"]) < TOL_RHS
+    assert np.all(rg["dhdt"] == 0.0) and np.all(ro["dhdt"] == 0.0)
+    d = g.get_diag()
+    assert np.all(d["sig11"] == 0.0) and np.all(d["eps12"] == 0.0)
+
+
+def test_sum_density(gpu_lib, oracle_mod):
+    b = basins.cfg1()
+    for prm_skf in (9, 6):
+        prm = b.params.copy()
+        prm.skf = prm_skf
+        g, o = _pair(b, oracle_mod, prm)
+        assert rel_l2(g.sum_density(), o.sum_density(k0_mode=1)) < TOL_RHS
+
+
+def test_trajectory_cfg1_20_steps(gpu_lib, oracle_mod):
+    b = basins.cfg1()
+    g, o = _pair(b, oracle_mod)
+    tg, dtg = g.time_integration(20)
+    to, dto = o.step(20)
+    assert tg == to and dtg == dto
+    sg, so = g.get_state(), o.get_state()
+    for k in ("x", "vx", "h", "A", "rho"):
+        assert rel_l2(sg[k] - (b.x if k == "x" else 0), so[k] - (b.x if k == "x" else 0)) < TOL_TRAJ_20, k
+
+
+def test_trajectory_vp_timestep_and_marquis_hsml(gpu_lib, oracle_mod):
+    """Reference default switches: sle = 2 (Marquis hsml), tse = 2 (VP dt),
+    Wendland C6, mass from the lattice."""
+    from simp_b200.params import reference_default
+    b = basins.cfg1()
+    prm = reference_default()
+    prm.wind_u, prm.wind_v = 10.0, 0.0
+    prm.b_length = 4.0 * b.dx
+    b.hsml[:] = 3.0 * b.dx   # hsml_multiplicity * dx (initialize.f90:190)
+    # initialize.f90:199 calls time_step before the loop: the VP dt
+    prm.dt = prm.rho_ice * (3.0 * b.dx) ** 2 * prm.delta_min / (prm.P_star * (1.0 + prm.k_t))
+    g, o = _pair(b, oracle_mod, prm)
+    tg, dtg = g.time_integration(10)
+    to, dto = o.step(10)
+    assert abs(tg - to) <= 1e-12 * abs(to) and dtg == dto
+    sg, so = g.get_state(), o.get_state()
+    for k in ("vx", "h", "hsml"):
+        assert rel_l2(sg[k], so[k]) < TOL_TRAJ_20, k
