@@ -186,6 +186,24 @@ SIMP_API int32_t simp_gpu_interaction_stats(simp_ctx *ctx, int32_t *maxip,
                                    int32_t *minip, int64_t *sumip,
                                    int32_t *noip);
 
+/* The CUDA stream (cudaStream_t) every kernel of this context runs on, for
+ * event timing and interop.  No reference counterpart (the reference has no
+ * device). */
+SIMP_API void *simp_gpu_stream(simp_ctx *ctx);
+
+/* Number of kernels this context has launched so far (graph replays count
+ * each captured kernel).  No reference counterpart. */
+SIMP_API int64_t simp_gpu_kernel_launches(const simp_ctx *ctx);
+
+/* Per-kernel timing of simp_gpu_step: when on, CUDA events recorded inside
+ * the step graph time each kernel of every step; simp_gpu_kernel_times then
+ * returns, for the n_kernels kernels of a step (kinematic, stress-predict,
+ * kinematic, stress-correct, step-finish), the summed milliseconds and the
+ * number of steps timed.  No reference counterpart. */
+SIMP_API int32_t simp_gpu_profile(simp_ctx *ctx, int32_t on);
+SIMP_API int32_t simp_gpu_kernel_times(simp_ctx *ctx, double *ms, int32_t n_kernels,
+                                       int64_t *steps_timed);
+
 /* Human-readable text of the last error on this context ("" if none). */
 SIMP_API const char *simp_gpu_last_error(const simp_ctx *ctx);
 

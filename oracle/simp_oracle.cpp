@@ -73,6 +73,42 @@ inline double p8(double a) { double a2 = a * a; double a4 = a2 * a2; return a4 *
 // Fortran NINT: nearest integer, halves away from zero.
 inline long fnint(double v) { return lround(v); }
 
+int num_threads() {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+int thread_id() {
+#ifdef _OPENMP
+    return omp_get_thread_num();
+#else
+    return 0;
+#endif
+}
+
+// OpenMP reduction of an array over a pair loop, with the private copies on
+// the heap (array-section reductions live on thread stacks).  Each thread
+// accumulates into a zeroed copy; copies are added to dst in thread order,
+// which with one thread reproduces the serial summation exactly.
+template <class Body>
+void reduce_pairs(int npairs, double *dst, size_t len, int chunk, Body body) {
+    const int nthr = num_threads();
+    std::vector<std::vector<double>> priv(nthr);
+#pragma omp parallel num_threads(nthr)
+    {
+        std::vector<double> &acc = priv[thread_id()];
+        acc.assign(len, 0.0);
+#pragma omp for schedule(dynamic, chunk)
+        for (int k = 0; k < npairs; ++k) body(k, acc.data());
+    }
+    for (int t = 0; t < nthr; ++t)
+        if (!priv[t].empty())
+            for (size_t i = 0; i < len; ++i) dst[i] = dst[i] + priv[t][i];
+}
+
 // ---------------------------------------------------------------------------
 // Pair kernel, kernel.f90:5-45 dispatch.
 //   in : r, hij (hsml_ij), dx(2)  out: w, dw(2), k0 (kernel_zero value)
@@ -324,12 +360,9 @@ void internal_stress(Orc &o) {
         o.sig22[i] = (o.zeta[i] + o.eta[i]) * o.eps22[i] + (o.zeta[i] - o.eta[i]) * o.eps11[i] -
                      o.p[i] * (1.0 - P.k_t) / 2.0;
     }
-    // stress_1 :103-137
-    double *dv = o.dvxdt.data();
-    const int nip = o.nip;
+    // stress_1 :103-137 (REDUCTION(+:dvxdt))
     const double rho_ice = P.rho_ice;
-#pragma omp parallel for schedule(static) reduction(+ : dv[:2 * n])
-    for (int k = 0; k < nip; ++k) {
+    reduce_pairs(o.nip, o.dvxdt.data(), 2 * (size_t)n, 4096, [&](int k, double *dv) {
         const int i = o.p_i[k] - 1, j = o.p_j[k] - 1;
         const double g1 = o.dwdx[2 * k], g2 = o.dwdx[2 * k + 1];
         double cj = (o.sig11[j] * g1 + o.sig12[j] * g2) / p2(o.rho[j]);
@@ -340,7 +373,7 @@ void internal_stress(Orc &o) {
         ci = (o.sig12[i] * g1 + o.sig22[i] * g2) / p2(o.rho[i]);
         dv[2 * i + 1] = dv[2 * i + 1] + o.rho[i] * o.mass[j] / rho_ice / o.h[i] * (ci + cj);
         dv[2 * j + 1] = dv[2 * j + 1] + o.rho[j] * o.mass[i] / rho_ice / o.h[j] * (-ci - cj);
-    }
+    });
 }
 
 // boundary_kernel.f90:477-502 + boundary_force.f90:74-84 (bf_Monaghan,
@@ -409,7 +442,9 @@ void single_step(Orc &o) {
     std::fill(o.dvxdt.begin(), o.dvxdt.begin() + 2 * n, 0.0);
     std::fill(o.dAdt.begin(), o.dAdt.begin() + n, 0.0);
     std::fill(o.dhdt.begin(), o.dhdt.begin() + n, 0.0);
-    std::vector<double> div(n, 0.0), grad(4 * (size_t)n, 0.0);
+    // div_v_sum (n) and grad_v_sum (4 n) in one buffer
+    std::vector<double> dg(5 * (size_t)n, 0.0);
+    double *div = dg.data(), *grad = dg.data() + n;
     std::fill(o.eps11.begin(), o.eps11.begin() + n, 0.0);
     std::fill(o.eps12.begin(), o.eps12.begin() + n, 0.0);
     std::fill(o.eps22.begin(), o.eps22.begin() + n, 0.0);
@@ -418,11 +453,10 @@ void single_step(Orc &o) {
     const int nip = o.nip;
     o.w.assign(nip, 0.0);
     o.dwdx.assign(2 * (size_t)nip, 0.0);
-    double *dv = div.data(), *gv = grad.data();
     double *kz = o.kernel_zero.data();
-    // :50-77 kinematic pair loop
-#pragma omp parallel for schedule(dynamic, 256) reduction(- : dv[:n], gv[:4 * n])
-    for (int k = 0; k < nip; ++k) {
+    // :50-77 kinematic pair loop, REDUCTION(-:div_v_sum, grad_v_sum)
+    reduce_pairs(nip, dg.data(), dg.size(), 256, [&](int k, double *acc) {
+        double *dv = acc, *gv = acc + n;
         const int ci = o.p_i[k] - 1, cj = o.p_j[k] - 1;
         const double dx[2] = {o.x[2 * ci] - o.x[2 * cj], o.x[2 * ci + 1] - o.x[2 * cj + 1]};
         const double dvx[2] = {o.vx[2 * ci] - o.vx[2 * cj], o.vx[2 * ci + 1] - o.vx[2 * cj + 1]};
@@ -437,7 +471,7 @@ void single_step(Orc &o) {
             gv[4 * (size_t)ci + c] = gv[4 * (size_t)ci + c] - o.mass[cj] * wdvx[c] / o.rho[cj];
             gv[4 * (size_t)cj + c] = gv[4 * (size_t)cj + c] - o.mass[ci] * wdvx[c] / o.rho[ci];
         }
-    }
+    });
     if (o.P.pressure_force || o.P.viscosity) {                      // :80-84
         for (int i = 0; i < n; ++i) {
             o.eps11[i] = grad[4 * (size_t)i];

@@ -51,6 +51,23 @@ __global__ void k_to_orig1(int n, const int *__restrict__ id, const double *__re
     out[id[k]] = a[k];
 }
 
+// Whole state to original order in one pass: stage = [x,y interleaved | vx,vy
+// interleaved | mass | rho | hsml | A | h], 9 n doubles.
+__global__ void k_pack_state(int n, const int *__restrict__ id, State s, double *__restrict__ stage) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const size_t o = (size_t)id[k], N = (size_t)n;
+    stage[2 * o] = s.x[k];
+    stage[2 * o + 1] = s.y[k];
+    stage[2 * N + 2 * o] = s.vx[k];
+    stage[2 * N + 2 * o + 1] = s.vy[k];
+    stage[4 * N + o] = s.m[k];
+    stage[5 * N + o] = s.rho[k];
+    stage[6 * N + o] = s.hs[k];
+    stage[7 * N + o] = s.A[k];
+    stage[8 * N + o] = s.h[k];
+}
+
 __global__ void k_init_ids(int n, int *id, const double *m, const double *rho, double *mor) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
@@ -146,6 +163,8 @@ void free_all(simp_ctx *c) {
         if (p) cudaFree(p);
     if (c->sc_host) cudaFreeHost(c->sc_host);
     if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+    for (cudaEvent_t e : c->prof_ev)
+        if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -163,6 +182,7 @@ int size_grid(simp_ctx *c, double xmin, double xmax, double ymin, double ymax, d
     const double cap = std::max(4.0 * (double)c->maxn, 65536.0);
     while (std::ceil(w / cs) * std::ceil(h / cs) > cap) cs *= 1.25;
     Grid &g = c->grid;
+    c->grid_hmax = hmax;
     g.x0 = x0;
     g.y0 = y0;
     g.cs = cs;
@@ -229,10 +249,10 @@ int bin_walls(simp_ctx *c, int nb, const double *xb, const double *massb) {
     return SIMP_OK;
 }
 
-int upload_interleaved(simp_ctx *c, const double *h2, double *a, double *b, int n) {
-    double *stage = c->tmp;  // 2n doubles
+int upload_interleaved(simp_ctx *c, const double *h2, double *a, double *b, int n, double *stage) {
     SIMP_CUDA(c, cudaMemcpyAsync(stage, h2, sizeof(double) * 2 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
     k_deinterleave<<<nblk(n, kB), kB, 0, c->stream>>>(n, stage, a, b);
+    c->launches += 1;
     SIMP_CUDA(c, cudaGetLastError());
     return SIMP_OK;
 }
@@ -240,6 +260,7 @@ int upload_interleaved(simp_ctx *c, const double *h2, double *a, double *b, int 
 int download2(simp_ctx *c, const double *a, const double *b, double *h2) {
     double *stage = c->tmp;
     k_to_orig2<<<nblk(c->n, kB), kB, 0, c->stream>>>(c->n, c->id, a, b, stage);
+    c->launches += 1;
     SIMP_CUDA(c, cudaMemcpyAsync(h2, stage, sizeof(double) * 2 * (size_t)c->n, cudaMemcpyDeviceToHost, c->stream));
     SIMP_CUDA(c, cudaStreamSynchronize(c->stream));
     return SIMP_OK;
@@ -248,6 +269,7 @@ int download2(simp_ctx *c, const double *a, const double *b, double *h2) {
 int download1(simp_ctx *c, const double *a, double *h1) {
     double *stage = c->tmp;
     k_to_orig1<<<nblk(c->n, kB), kB, 0, c->stream>>>(c->n, c->id, a, stage);
+    c->launches += 1;
     SIMP_CUDA(c, cudaMemcpyAsync(h1, stage, sizeof(double) * (size_t)c->n, cudaMemcpyDeviceToHost, c->stream));
     SIMP_CUDA(c, cudaStreamSynchronize(c->stream));
     return SIMP_OK;
@@ -260,29 +282,47 @@ int read_scalars(simp_ctx *c) {
 }
 
 // One predictor-corrector step (time_integration.f90:263-390).
-void enqueue_step(simp_ctx *c, bool diag) {
+// One predictor-corrector step (time_integration.f90:263-390).  With
+// profiling on, external event records between the kernels time each one.
+void enqueue_step(simp_ctx *c, bool diag, bool prof) {
+    auto mark = [&](int k) {
+        if (prof) cudaEventRecordWithFlags(c->prof_ev[k], c->stream, cudaEventRecordExternal);
+    };
+    mark(0);
     launch_kinematic(c, c->s0, false);
+    mark(1);
     launch_stress(c, c->s0, c->s0, EPI_PREDICT);
+    mark(2);
     launch_kinematic(c, c->s1, diag);
+    mark(3);
     launch_stress(c, c->s1, c->s0, EPI_CORRECT);
+    mark(4);
     launch_step_finish(c);
+    mark(5);
 }
 
 int ensure_graph(simp_ctx *c, bool diag) {
-    if (c->step_graph && c->graph_diag == diag) return SIMP_OK;
+    const bool prof = c->profile;
+    if (c->step_graph && c->graph_diag == diag && c->graph_profiled == prof) return SIMP_OK;
     if (c->step_graph) {
         cudaGraphExecDestroy(c->step_graph);
         c->step_graph = nullptr;
     }
+    if (prof && !c->prof_ev[0])
+        for (auto &e : c->prof_ev) SIMP_CUDA(c, cudaEventCreate(&e));
     cudaGraph_t g = nullptr;
+    const long long before = c->launches;
     SIMP_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    enqueue_step(c, diag);
+    enqueue_step(c, diag, prof);
     cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    c->graph_kernels = c->launches - before;   // captured, not yet launched
+    c->launches = before;
     if (e != cudaSuccess) return simp_cuda_check(c, e, "cudaStreamEndCapture");
     e = cudaGraphInstantiate(&c->step_graph, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return simp_cuda_check(c, e, "cudaGraphInstantiate");
     c->graph_diag = diag;
+    c->graph_profiled = prof;
     return SIMP_OK;
 }
 
@@ -302,8 +342,9 @@ bool wants_rebuild(const simp_ctx *c, const Scalars &s) {
     return (s.hmax + 2.0 * disp_of(s)) * c->grid.inv_cs > 0.98;
 }
 
-// Resize the grid when hsml itself outgrew the cell side (sle = 2).
-bool wants_regrid(const simp_ctx *c, const Scalars &s) { return s.hmax * c->grid.inv_cs > 0.9; }
+// Resize the grid when hsml grew 5% past the bound the grid was sized for
+// (sle = 2); until then the device-side stencil radius covers the growth.
+bool wants_regrid(const simp_ctx *c, const Scalars &s) { return s.hmax > 1.05 * c->grid_hmax; }
 
 int size_grid(simp_ctx *c, double xmin, double xmax, double ymin, double ymax, double hmax);
 int bin_walls(simp_ctx *c, int nb, const double *xb, const double *massb);
@@ -507,16 +548,15 @@ int32_t simp_gpu_set_state(simp_ctx *c, int32_t ntotal, const double *x, const d
     c->phys = make_phys(c->prm, max_hsml);
     TRY(size_grid(c, xmin, xmax, ymin, ymax, hmax));
     // particle arrays (original order)
-    TRY(upload_interleaved(c, x, c->s0.x, c->s0.y, n));
-    SIMP_CUDA(c, cudaStreamSynchronize(s));
-    TRY(upload_interleaved(c, vx, c->s0.vx, c->s0.vy, n));
-    SIMP_CUDA(c, cudaStreamSynchronize(s));
+    TRY(upload_interleaved(c, x, c->s0.x, c->s0.y, n, c->tmp));
+    TRY(upload_interleaved(c, vx, c->s0.vx, c->s0.vy, n, c->tmp + 2 * (size_t)n));
     SIMP_CUDA(c, cudaMemcpyAsync(c->s0.m, mass, sizeof(double) * n, cudaMemcpyHostToDevice, s));
     SIMP_CUDA(c, cudaMemcpyAsync(c->s0.rho, rho, sizeof(double) * n, cudaMemcpyHostToDevice, s));
     SIMP_CUDA(c, cudaMemcpyAsync(c->s0.hs, hsml, sizeof(double) * n, cudaMemcpyHostToDevice, s));
     SIMP_CUDA(c, cudaMemcpyAsync(c->s0.A, A, sizeof(double) * n, cudaMemcpyHostToDevice, s));
     SIMP_CUDA(c, cudaMemcpyAsync(c->s0.h, h, sizeof(double) * n, cudaMemcpyHostToDevice, s));
     k_init_ids<<<nblk(n, kB), kB, 0, s>>>(n, c->id, c->s0.m, c->s0.rho, c->s0.mor);
+    c->launches += 1;
     SIMP_CUDA(c, cudaGetLastError());
     c->host_xb.assign(xb, xb + 2 * (size_t)ntotalb);
     c->host_massb.assign(massb, massb + ntotalb);
@@ -548,18 +588,24 @@ int32_t simp_gpu_get_state(simp_ctx *c, double *x, double *vx, double *mass, dou
                            double *hsml, double *A, double *h, double *dt, double *current_time) {
     if (!c) return SIMP_ERR_BADARG;
     if (!c->have_state) return simp_fail(c, SIMP_ERR_STATE, "get_state before set_state");
-    if (x) TRY(download2(c, c->s0.x, c->s0.y, x));
-    if (vx) TRY(download2(c, c->s0.vx, c->s0.vy, vx));
-    if (mass) TRY(download1(c, c->s0.m, mass));
-    if (rho) TRY(download1(c, c->s0.rho, rho));
-    if (hsml) TRY(download1(c, c->s0.hs, hsml));
-    if (A) TRY(download1(c, c->s0.A, A));
-    if (h) TRY(download1(c, c->s0.h, h));
-    if (dt || current_time) {
-        TRY(read_scalars(c));
-        if (dt) *dt = c->sc_host->dt;
-        if (current_time) *current_time = c->sc_host->t;
-    }
+    const int n = c->n;
+    const size_t N = (size_t)n;
+    cudaStream_t s = c->stream;
+    double *stage = c->tmp;  // 9 n doubles
+    k_pack_state<<<nblk(n, kB), kB, 0, s>>>(n, c->id, c->s0, stage);
+    c->launches += 1;
+    SIMP_CUDA(c, cudaGetLastError());
+    struct Out { double *dst; size_t off, len; } outs[] = {
+        {x, 0, 2 * N}, {vx, 2 * N, 2 * N}, {mass, 4 * N, N}, {rho, 5 * N, N},
+        {hsml, 6 * N, N}, {A, 7 * N, N}, {h, 8 * N, N}};
+    for (const Out &o : outs)
+        if (o.dst)
+            SIMP_CUDA(c, cudaMemcpyAsync(o.dst, stage + o.off, sizeof(double) * o.len,
+                                         cudaMemcpyDeviceToHost, s));
+    SIMP_CUDA(c, cudaMemcpyAsync(c->sc_host, c->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, s));
+    SIMP_CUDA(c, cudaStreamSynchronize(s));
+    if (dt) *dt = c->sc_host->dt;
+    if (current_time) *current_time = c->sc_host->t;
     return SIMP_OK;
 }
 
@@ -605,6 +651,7 @@ int32_t simp_gpu_single_step(simp_ctx *c, double current_time, double *dxdt, dou
     if (!c->have_state) return simp_fail(c, SIMP_ERR_STATE, "single_step before set_state");
     cudaStream_t s = c->stream;
     k_set_time<<<1, 1, 0, s>>>(c->sc, current_time);
+    c->launches += 1;
     launch_reset_stats(c);
     launch_kinematic(c, c->s0, true);
     launch_stress(c, c->s0, c->s0, EPI_RATES);
@@ -632,6 +679,9 @@ int32_t simp_gpu_step(simp_ctx *c, int32_t nsteps, double *current_time, double 
     if (!c || nsteps < 0) return SIMP_ERR_BADARG;
     if (!c->have_state) return simp_fail(c, SIMP_ERR_STATE, "step before set_state");
     cudaStream_t s = c->stream;
+    // bounds read at the end of the previous call (or by set_state)
+    if (wants_regrid(c, *c->sc_host)) TRY(regrid(c));
+    else if (wants_rebuild(c, *c->sc_host)) TRY(rebuild(c));
     launch_reset_stats(c);
     TRY(ensure_graph(c, c->keep_diag));
     // The cell list stays exact between sorts (the stencil radius adapts on
@@ -663,9 +713,21 @@ int32_t simp_gpu_step(simp_ctx *c, int32_t nsteps, double *current_time, double 
         }
         cudaError_t e = cudaGraphLaunch(c->step_graph, s);
         if (e != cudaSuccess) { rc = simp_cuda_check(c, e, "cudaGraphLaunch"); break; }
+        c->launches += c->graph_kernels;
         cudaMemcpyAsync(&c->sc_host[1 + st % kSnapRing], c->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, s);
         cudaEventRecord(ev[st % kSnapRing], s);
         c->steps_since_rebuild++;
+        if (c->graph_profiled) {
+            // timing mode: wait for this step and add up its kernel times
+            e = cudaEventSynchronize(c->prof_ev[simp_ctx::kProfKernels]);
+            if (e != cudaSuccess) { rc = simp_cuda_check(c, e, "profile event"); break; }
+            for (int k = 0; k < simp_ctx::kProfKernels; ++k) {
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, c->prof_ev[k], c->prof_ev[k + 1]);
+                c->prof_ms[k] += ms;
+            }
+            c->prof_steps += 1;
+        }
     }
     cudaError_t e = cudaStreamSynchronize(s);
     for (int k = 0; k < kSnapRing; ++k) cudaEventDestroy(ev[k]);
@@ -675,6 +737,25 @@ int32_t simp_gpu_step(simp_ctx *c, int32_t nsteps, double *current_time, double 
     if (current_time) *current_time = c->sc_host->t;
     if (dt) *dt = c->sc_host->dt;
     return check_after(c);
+}
+
+void *simp_gpu_stream(simp_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int64_t simp_gpu_kernel_launches(const simp_ctx *c) { return c ? (int64_t)c->launches : 0; }
+
+int32_t simp_gpu_profile(simp_ctx *c, int32_t on) {
+    if (!c) return SIMP_ERR_BADARG;
+    c->profile = on != 0;
+    for (double &v : c->prof_ms) v = 0.0;
+    c->prof_steps = 0;
+    return SIMP_OK;
+}
+
+int32_t simp_gpu_kernel_times(simp_ctx *c, double *ms, int32_t n_kernels, int64_t *steps_timed) {
+    if (!c || !ms || n_kernels < 0) return SIMP_ERR_BADARG;
+    for (int k = 0; k < n_kernels; ++k) ms[k] = (k < simp_ctx::kProfKernels) ? c->prof_ms[k] : 0.0;
+    if (steps_timed) *steps_timed = c->prof_steps;
+    return SIMP_OK;
 }
 
 const char *simp_gpu_last_error(const simp_ctx *c) { return c ? c->err.c_str() : "null context"; }

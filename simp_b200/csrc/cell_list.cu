@@ -230,6 +230,7 @@ int rebuild(simp_ctx *c) {
     SIMP_CUDA(c, cudaMemcpyAsync(c->id, id_new, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, s));
     k_finish_rebuild<<<nblk(n, B), B, 0, s>>>(n, c->s0.x, c->s0.y, c->xr, c->yr, c->id, c->inv_id);
     k_reset_disp<<<1, 1, 0, s>>>(c->sc);
+    c->launches += 7 + kScanKernels;
     SIMP_CUDA(c, cudaGetLastError());
     c->steps_since_rebuild = 0;
     c->rebuilds += 1;

@@ -39,6 +39,7 @@ struct simp_ctx {
     int *bcell_start = nullptr;
     // cell grid
     simp::Grid grid{};
+    double grid_hmax = 0.0;        // max(hsml) the grid was sized for
     int *cell_start = nullptr;
     size_t cell_cap = 0;
     // rebuild scratch
@@ -63,6 +64,15 @@ struct simp_ctx {
     // step graph
     cudaGraphExec_t step_graph = nullptr;
     bool graph_diag = false;
+    bool graph_profiled = false;
+    long long graph_kernels = 0;   // kernels per replay
+    long long launches = 0;        // kernels launched by this context
+    // per-kernel timing (events recorded inside the step graph)
+    static constexpr int kProfKernels = 5;
+    bool profile = false;
+    cudaEvent_t prof_ev[kProfKernels + 1] = {};
+    double prof_ms[kProfKernels] = {};
+    long long prof_steps = 0;
     // rebuild policy
     int steps_since_rebuild = 0;
     long long rebuilds = 0;
@@ -73,6 +83,7 @@ namespace simp {
 // cell_list.cu
 int rebuild(simp_ctx *c);               // sort particles into cell order
 void launch_scan_i32(const int *in, int *out, int n, void *tmp, cudaStream_t s);
+constexpr int kScanKernels = 4;         // kernels per launch_scan_i32
 size_t scan_tmp_bytes(int n);
 
 // passes.cu

@@ -219,6 +219,7 @@ int export_pairs(simp_ctx *c, int32_t *nip, int32_t *p_i, int32_t *p_j, double *
     launch_reset_stats(c);
     k_count<<<nblk(n, kBlock), kBlock, 0, st>>>(a);
     launch_scan_i32(c->itmp, c->pair_cnt, n, c->scan_tmp, st);
+    c->launches += 1 + kScanKernels;
     int total = 0;
     SIMP_CUDA(c, cudaMemcpyAsync(&total, c->pair_cnt + n, sizeof(int), cudaMemcpyDeviceToHost, st));
     SIMP_CUDA(c, cudaStreamSynchronize(st));
@@ -241,6 +242,7 @@ int export_pairs(simp_ctx *c, int32_t *nip, int32_t *p_i, int32_t *p_j, double *
         w.emit = 0;
         k_wall<<<nblk(c->nb, kBlock), kBlock, 0, st>>>(w);
         launch_scan_i32(w.cnt, c->bpair_cnt, c->nb, c->scan_tmp, st);
+        c->launches += 1 + kScanKernels;
         SIMP_CUDA(c, cudaMemcpyAsync(&btotal, c->bpair_cnt + c->nb, sizeof(int), cudaMemcpyDeviceToHost, st));
         SIMP_CUDA(c, cudaStreamSynchronize(st));
     }
@@ -267,6 +269,7 @@ int export_pairs(simp_ctx *c, int32_t *nip, int32_t *p_i, int32_t *p_j, double *
     a.orr = c->pair_buf_r;
     a.oh = c->pair_buf_h;
     k_emit<<<nblk(n, kBlock), kBlock, 0, st>>>(a);
+    c->launches += 1;
     SIMP_CUDA(c, cudaGetLastError());
     if (nip) *nip = total;
     const int m = std::min(total, (int)std::max(cap, 0));
@@ -285,6 +288,7 @@ int export_pairs(simp_ctx *c, int32_t *nip, int32_t *p_i, int32_t *p_j, double *
         w.orr = c->pair_buf_r;
         w.emit = 1;
         k_wall<<<nblk(c->nb, kBlock), kBlock, 0, st>>>(w);
+        c->launches += 1;
         SIMP_CUDA(c, cudaGetLastError());
         const int mb = std::min(btotal, (int)std::max(bcap, 0));
         if (mb > 0) {
@@ -312,6 +316,7 @@ int sum_density(simp_ctx *c, double *rho_out_dev) {
     a.n = c->n;
     a.out = rho_out_dev;
     k_sum_density<<<nblk(c->n, kBlock), kBlock, 0, c->stream>>>(a);
+    c->launches += 1;
     SIMP_CUDA(c, cudaGetLastError());
     return SIMP_OK;
 }

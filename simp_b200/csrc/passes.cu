@@ -334,6 +334,7 @@ void launch_kinematic(simp_ctx *c, const State &s, bool diag) {
     a.n = c->n;
     a.maxn = c->maxn;
     k_kinematic<<<nblk(c->n, kBlock), kBlock, 0, c->stream>>>(a);
+    c->launches += 1;
 }
 
 void launch_stress(simp_ctx *c, const State &rhs, const State &base, EpiMode mode) {
@@ -362,6 +363,7 @@ void launch_stress(simp_ctx *c, const State &rhs, const State &base, EpiMode mod
     a.maxn = c->maxn;
     a.mode = mode;
     k_stress<<<nblk(c->n, kBlock), kBlock, 0, c->stream>>>(a);
+    c->launches += 1;
 }
 
 void launch_step_finish(simp_ctx *c) {
@@ -369,8 +371,12 @@ void launch_step_finish(simp_ctx *c) {
         cudaMemcpyAsync(c->s0.hs, c->tmp, sizeof(double) * (size_t)c->n, cudaMemcpyDeviceToDevice,
                         c->stream);
     k_step_finish<<<1, 1, 0, c->stream>>>(c->sc, c->prm.tse, c->prm.sle);
+    c->launches += 1;
 }
 
-void launch_reset_stats(simp_ctx *c) { k_reset_stats<<<1, 1, 0, c->stream>>>(c->sc); }
+void launch_reset_stats(simp_ctx *c) {
+    k_reset_stats<<<1, 1, 0, c->stream>>>(c->sc);
+    c->launches += 1;
+}
 
 }  // namespace simp

@@ -69,7 +69,8 @@ def test_nnps_variable_hsml_bucket_rule(gpu_lib, oracle_mod):
     """max(hsml) > 2 min(hsml): the reference's bucket stencil drops pairs."""
     b = basins.cfg1()
     rng = np.random.default_rng(7)
-    b.hsml = b.hsml * rng.uniform(0.45, 1.05, size=b.n)
+    b.hsml = b.hsml * rng.uniform(0.9, 1.05, size=b.n)
+    b.hsml[rng.choice(b.n, 5, replace=False)] *= 0.3   # bucket side 2 min(hsml) << max(hsml)
     g, o = _pair(b, oracle_mod)
     rg, ro = g.nnps(), o.nnps()
     assert_same_pairs(rg, ro)
