@@ -186,6 +186,28 @@ SIMP_API int32_t simp_gpu_interaction_stats(simp_ctx *ctx, int32_t *maxip,
                                    int32_t *minip, int64_t *sumip,
                                    int32_t *noip);
 
+/* Summation density (the same result as simp_gpu_sum_density) for callers
+ * that cannot allocate device memory.  No counterpart in the reference: it
+ * exists for hosts whose device memory belongs to another runtime (CUDA
+ * Fortran or OpenACC device arrays, a framework's caching allocator) and for
+ * loops that may not stall on cudaMalloc, which can synchronise the device.
+ *   x       device, 2*n interleaved positions   hsml, mass, rho: device, n
+ *   rho_out device, n (original order)          skf: SIMP_SKF_*
+ *   stream  cudaStream_t to run on (NULL: the legacy default stream)
+ * It calls no cudaMalloc, cudaFree or allocating library routine: its cell
+ * list lives in one fixed array inside the library (about 5 MB, held on
+ * every GPU that loads the library until the process exits).  n must be at
+ * most SIMP_NOALLOC_MAX_PARTICLES, else SIMP_ERR_BADARG.  The first call on
+ * each device looks up that array's device address, so make it before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * race and must be serialised by the caller.  Asynchronous: returns after
+ * enqueueing on stream. */
+#define SIMP_NOALLOC_MAX_PARTICLES 65536
+SIMP_API int32_t simp_gpu_sum_density_noalloc(const double *x, const double *hsml,
+                                              const double *mass, const double *rho,
+                                              int32_t n, int32_t skf, double *rho_out,
+                                              void *stream);
+
 /* The CUDA stream (cudaStream_t) every kernel of this context runs on, for
  * event timing and interop.  No reference counterpart (the reference has no
  * device). */
