@@ -62,6 +62,21 @@ def init_dist(world, backend):
     return dist
 
 
+def job_time_ms(dist, local_ms: float, device: str = "cuda") -> float:
+    """Slowest rank's device time (every rank takes the same collective)."""
+    if dist is None:
+        return float(local_ms)
+    import torch
+    t = torch.tensor([float(local_ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(world: int, particles: int, steps: int, job_ms: float) -> float:
+    """Whole-job particle-steps/s: all ranks' work over the slowest rank."""
+    return world * particles * steps / (job_ms / 1e3)
+
+
 # --- clocks sampled during the timed region --------------------------------
 
 class ClockSampler:
@@ -200,11 +215,8 @@ def run_ours(args):
     # device time of the K steps: sum of in-graph kernel times per step
     dev_ms = sum(kernel_ms)
     outer_ms = sum(a.elapsed_time(z) for a, z in zip(ev0, ev1))
-    t = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    dev_ms_max = float(t.item())
-    value = world * b.n * args.steps / (dev_ms_max / 1e3)
+    dev_ms_max = job_time_ms(dist, dev_ms)
+    value = job_value(world, b.n, args.steps, dev_ms_max)
 
     # roofline of the dominant kernel
     peak, peak_src = roofline.hbm_peak(ROOT)
@@ -307,13 +319,8 @@ def run_e2e(sim, b, stream, nsteps, dist):
         t_now, dt = tc.value, dtc.value
     e1.record(stream)
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    tt = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    world = 1
-    if dist:
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        world = dist.get_world_size()
-    ms = float(tt.item())
+    ms = job_time_ms(dist, e0.elapsed_time(e1))
+    world = dist.get_world_size() if dist else 1
     h2d = n * (2 * 16 + 5 * 8) + nb * 24
     d2h = n * (2 * 16 + 5 * 8) + 16
     return {"value": world * n * nsteps / (ms / 1e3), "unit": METRIC, "h2d_bytes_per_step": h2d,

@@ -1,0 +1,90 @@
+"""The C-ABI library without a GPU: symbols, struct layout, defaults."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+from simp_b200 import _lib, build
+from simp_b200.params import SimpParams, reference_default
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "simp_gpu.h")
+
+
+def declared_symbols():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"SIMP_API\s+[\w\s\*]*?\b(simp_\w+)\s*\(", txt)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    build.build()
+    return _lib.load()
+
+
+def test_every_declared_symbol_is_exported(lib):
+    names = declared_symbols()
+    assert len(names) >= 18
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) <= set(_lib.SIGNATURES), set(names) - set(_lib.SIGNATURES)
+
+
+def test_params_layout_matches_c(tmp_path):
+    fields = [f for f, _ in SimpParams._fields_]
+    src = tmp_path / "layout.c"
+    body = "\n".join(f'    printf("%s %zu\\n", "{f}", offsetof(simp_params, {f}));' for f in fields)
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "simp_gpu.h"\nint main(void){\n'
+                   f'    printf("sizeof %zu\\n", sizeof(simp_params));\n{body}\n    return 0;\n}}\n')
+    exe = tmp_path / "layout"
+    cc = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else "gcc"
+    subprocess.run([cc, "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                        check=True).stdout.splitlines())
+    assert int(out["sizeof"]) == ctypes.sizeof(SimpParams)
+    for f in fields:
+        assert int(out[f]) == getattr(SimpParams, f).offset, f
+
+
+def test_fortran_mirror_field_order():
+    """The bind(C) type in the Fortran shim lists the members in C order."""
+    src = open(os.path.join(ROOT, "fortran", "shim", "simp_gpu_mod.f90")).read()
+    body = src[src.index("type, bind(C) :: simp_params"):src.index("end type simp_params")]
+    body = re.sub(r"&\s*\n\s*", " ", body)
+    names = []
+    for line in body.splitlines()[1:]:
+        if "::" in line:
+            names += [n.strip() for n in line.split("::", 1)[1].split(",") if n.strip()]
+    assert [n.lower() for n in names] == [f.lower() for f, _ in SimpParams._fields_]
+
+
+def test_reference_default_matches_python_mirror(lib):
+    c = SimpParams()
+    lib.simp_params_reference_default(ctypes.byref(c))
+    py = reference_default()
+    for f, _ in SimpParams._fields_:
+        assert getattr(c, f) == getattr(py, f), f
+
+
+def test_version_string(lib):
+    assert b"sm_100a" in lib.simp_gpu_version()
+
+
+def test_noalloc_rejects_bad_sizes_before_touching_the_device(lib):
+    # n out of range and bad kernel codes are refused on the host
+    assert lib.simp_gpu_sum_density_noalloc(1, 1, 1, 1, 0, 9, 1, None) == 1
+    assert lib.simp_gpu_sum_density_noalloc(1, 1, 1, 1, 65537, 9, 1, None) == 1
+    assert lib.simp_gpu_sum_density_noalloc(1, 1, 1, 1, 10, 7, 1, None) == 1
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    with pytest.raises(_lib.NativeLibraryMissing):
+        _lib.load(str(tmp_path / "nope.so"))
+
+
+def test_null_context_calls_are_refused(lib):
+    assert lib.simp_gpu_step(None, 1, None, None) == 1
+    assert lib.simp_gpu_destroy(None) == 0
+    assert lib.simp_gpu_last_error(None) == b"null context"

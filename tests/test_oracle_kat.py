@@ -1,0 +1,162 @@
+"""Known-answer tests pinning the CPU oracle (no GPU).
+
+The reference has no tests or golden vectors and cannot be compiled here, so
+the oracle is pinned to closed-form values (tests/golden/, generated by
+tests/golden/make_golden.py from the formulas) and to exact invariants of
+the reference's algorithm.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from helpers import canonical_pairs, smooth_velocity
+from simp_b200 import basins
+from simp_b200.params import SKF_CUBIC, SKF_WENDLAND_C6, basin_params, reference_default
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _load(name):
+    with open(os.path.join(GOLD, name)) as f:
+        return json.load(f)
+
+
+def _params(skf):
+    p = basin_params(1000.0, skf=skf)
+    return p
+
+
+@pytest.mark.parametrize("skf,key", [(SKF_WENDLAND_C6, "wendland_c6"), (SKF_CUBIC, "cubic")])
+def test_kernel_matches_closed_form(oracle_mod, skf, key):
+    g = _load("kat_kernels.json")
+    p = _params(skf)
+    for e in g[key]:
+        w, gx, gy, _ = oracle_mod.kernel(p, e["r"], g["hsml_ij"], e["r"], 0.0)
+        assert w == pytest.approx(e["w"], rel=1e-13, abs=0.0)
+        assert gx == pytest.approx(e["dwdr"], rel=1e-12, abs=0.0)
+        assert gy == 0.0
+
+
+@pytest.mark.parametrize("skf", [SKF_WENDLAND_C6, SKF_CUBIC])
+def test_kernel_normalisation(oracle_mod, skf):
+    """integral of W over its support is 1 (cubic: to its single-precision
+    literals, ~3e-8)."""
+    p = _params(skf)
+    hij = 1000.0
+    support = hij  # SIMP hsml is the support radius for both kernels
+    r = np.linspace(0.0, support, 20001)[1:]
+    w = np.array([oracle_mod.kernel(p, ri, hij, ri, 0.0)[0] for ri in r])
+    integral = np.trapezoid(2 * np.pi * r * w, r)
+    assert integral == pytest.approx(1.0, abs=2e-6)
+
+
+@pytest.mark.parametrize("skf", [SKF_WENDLAND_C6, SKF_CUBIC])
+def test_gradient_is_odd(oracle_mod, skf):
+    p = _params(skf)
+    rng = np.random.default_rng(0)
+    for _ in range(50):
+        dx, dy = rng.uniform(-600, 600, size=2)
+        r = float(np.hypot(dx, dy))
+        a = oracle_mod.kernel(p, r, 1000.0, dx, dy)
+        b = oracle_mod.kernel(p, r, 1000.0, -dx, -dy)
+        assert a[1] == -b[1] and a[2] == -b[2]
+
+
+@pytest.mark.parametrize("ratio", ["2.4", "3.0"])
+def test_lattice_neighbour_counts(oracle_mod, ratio):
+    want = _load("kat_lattice.json")["support_over_dx"][ratio]
+    b = basins.make_basin(30, 1000.0, 1, jitter=0.0, walls="")
+    b.hsml[:] = float(ratio) * 1000.0
+    for alg in (1, 2):
+        p = b.params.copy()
+        p.nnps_algorithm = alg
+        o = oracle_mod.Oracle.from_basin(b, p)
+        o.nnps()
+        assert o.interaction_stats()["maxip"] == want
+
+
+def test_bucket_search_equals_direct_find(oracle_mod):
+    b = basins.cfg1()
+    res = []
+    for alg in (1, 2):
+        p = b.params.copy()
+        p.nnps_algorithm = alg
+        res.append(oracle_mod.Oracle.from_basin(b, p).nnps())
+    a, d = (canonical_pairs(r) for r in res)
+    assert res[0]["nip"] == res[1]["nip"]
+    for u, v in zip(a, d):
+        assert np.array_equal(u, v)
+
+
+def test_bucket_rule_drops_pairs_when_hsml_varies(oracle_mod):
+    """With max(hsml) > 2 min(hsml) the 3x3 bucket stencil of side
+    2 min(hsml) misses pairs that direct find keeps (nnps.f90:211, 259-407)."""
+    b = basins.cfg1()
+    rng = np.random.default_rng(7)
+    b.hsml = b.hsml * rng.uniform(0.9, 1.05, size=b.n)
+    b.hsml[rng.choice(b.n, 5, replace=False)] *= 0.3
+    p1, p2 = b.params.copy(), b.params.copy()
+    p1.nnps_algorithm = 1
+    d = oracle_mod.Oracle.from_basin(b, p1).nnps()
+    k = oracle_mod.Oracle.from_basin(b, p2).nnps()
+    assert k["nip"] < d["nip"]
+    dset = set(zip(*canonical_pairs(d)[:2]))
+    kset = set(zip(*canonical_pairs(k)[:2]))
+    assert kset < dset
+
+
+def test_rigid_translation_has_zero_strain_and_stress(oracle_mod):
+    b = basins.make_basin(30, 2000.0, 5, walls="")
+    b.vx[:] = (0.3, -0.1)
+    o = oracle_mod.Oracle.from_basin(b)
+    r = o.single_step(0.0)
+    d = o.get_diag()
+    for k in ("eps11", "eps12", "eps22", "sig11", "sig12", "sig22", "p"):
+        assert np.all(d[k] == 0.0), k
+    assert np.all(r["dvxdt"] == 0.0) and np.all(r["dhdt"] == 0.0)
+
+
+def test_internal_stress_conserves_momentum(oracle_mod):
+    """stress_1 with rho = rho_ice h adds m_j (c_i + c_j) to i and the
+    negative to j: sum_i m_i a_i = 0 to round-off."""
+    b = basins.make_basin(40, 2000.0, 6, walls="")
+    b.vx = smooth_velocity(b.x, b.L, seed=3)
+    o = oracle_mod.Oracle.from_basin(b)
+    a = o.single_step(0.0)["dvxdt"]
+    mom = (b.mass[:, None] * a).sum(axis=0)
+    scale = np.abs(b.mass[:, None] * a).sum(axis=0)
+    assert np.all(np.abs(mom) <= 1e-12 * scale)
+    assert np.all(scale > 0)
+
+
+def test_free_drift_speed(oracle_mod):
+    """Uniform ice, uniform wind, no walls: strain stays exactly zero and the
+    ice reaches the drag balance rho_a c_a (U-u)^2 = rho_w c_w u^2."""
+    phys = _load("kat_physics.json")
+    b = basins.make_basin(6, 2000.0, 2, walls="", wind=(phys["wind"], 0.0), dt=30.0)
+    o = oracle_mod.Oracle.from_basin(b)
+    o.step(1000)
+    st = o.get_state()
+    assert np.allclose(st["vx"][:, 0], phys["free_drift_speed"], rtol=1e-6, atol=0)
+    assert np.all(np.abs(st["vx"][:, 1]) < 1e-12)
+
+
+def test_mass_is_conserved(oracle_mod):
+    p = reference_default()
+    b = basins.cfg1()
+    p.wind_u, p.wind_v, p.b_length = 10.0, 0.0, 8000.0
+    b.hsml[:] = 3.0 * b.dx
+    p.dt = p.rho_ice * (3.0 * b.dx) ** 2 * p.delta_min / p.P_star
+    o = oracle_mod.Oracle.from_basin(b, p)
+    o.step(5)
+    assert np.array_equal(o.get_state()["mass"], b.mass)
+
+
+def test_reference_default_literals():
+    """Default-real literals of data_variables.f90 keep single precision."""
+    p = reference_default()
+    assert p.rho_air == np.float32(1.3)
+    assert p.rho_air != 1.3
+    assert p.e == 2.0 and p.k_t == 0.0 and p.P_star == 27500.0
