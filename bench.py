@@ -267,7 +267,7 @@ def run_ours(args):
 
 def profile_traffic(kernel: str):
     """DRAM bytes per launch from the committed ncu summary, if present."""
-    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    p = os.path.join(ROOT, "profiles", "ncu_traffic_cfg2.txt")
     try:
         with open(p) as f:
             v = json.load(f).get(kernel)
