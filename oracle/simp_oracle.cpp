@@ -61,6 +61,7 @@ struct Orc {
     std::vector<double> r_ij, hsml_ij, br_ij, w, dwdx;
     std::vector<int> count_np;
     std::string err;
+    bool bad = false;   // the state blew up (no bucket grid could be built)
 };
 
 // ---------------------------------------------------------------------------
@@ -220,6 +221,16 @@ void bucket_search(Orc &o) {
     for (int i = 0; i < n; ++i) {
         mnx = std::min(mnx, x[2 * i]); mxx = std::max(mxx, x[2 * i]);
         mny = std::min(mny, x[2 * i + 1]); mxy = std::max(mxy, x[2 * i + 1]);
+    }
+    // a state that blew up (non-finite or absurdly spread) has no bucket grid;
+    // the reference would index out of its arrays here
+    if (!std::isfinite(mnx + mxx + mny + mxy + bin_size) ||
+        (mxx - mnx) / bin_size > 1e6 || (mxy - mny) / bin_size > 1e6) {
+        o.bad = true;
+        o.nip = o.bnip = 0;
+        o.p_i.clear(); o.p_j.clear(); o.r_ij.clear(); o.hsml_ij.clear();
+        o.bp_i.clear(); o.bp_j.clear(); o.br_ij.clear();
+        return;
     }
     const long bc1 = fnint(mnx / bin_size), bc2 = fnint(mxx / bin_size);
     const long bc3 = fnint(mny / bin_size), bc4 = fnint(mxy / bin_size);
@@ -754,11 +765,12 @@ int orc_sum_density(void *hh, int k0_mode, double *rho_out) {
 // time_integration.f90:146-181 for nsteps iterations.
 int orc_step(void *hh, int nsteps, double *t, double *dt) {
     Orc *o = (Orc *)hh;
-    for (int s = 0; s < nsteps; ++s) {
+    for (int s = 0; s < nsteps && !o->bad; ++s) {
         predictor_corrector(*o);
         o->itimestep += 1;
         o->current_time = o->current_time + o->dt;
     }
+    if (o->bad) return fail(o, SIMP_ERR_NONFINITE, "state blew up: no bucket grid can be built");
     if (t) *t = o->current_time;
     if (dt) *dt = o->dt;
     for (int i = 0; i < 2 * o->ntotal; ++i)

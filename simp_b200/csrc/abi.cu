@@ -154,11 +154,13 @@ int dalloc(simp_ctx *c, T **p, size_t count) {
 void free_all(simp_ctx *c) {
     void *ptrs[] = {c->s0.x, c->s0.y, c->s0.vx, c->s0.vy, c->s0.m, c->s0.rho, c->s0.mor, c->s0.h,
                     c->s0.A, c->s0.hs, c->s1.x, c->s1.y, c->s1.vx, c->s1.vy, c->s1.rho, c->s1.mor,
-                    c->s1.h, c->s1.A, c->mass1, c->xr, c->yr, c->cell, c->id, c->inv_id,
+                    c->s1.h, c->s1.A, c->mass1, c->xr, c->yr, c->xl, c->yl, c->cell, c->id, c->inv_id,
                     c->tau11, c->tau12, c->tau22, c->div, c->diag, c->rates, c->bx, c->by, c->bm,
                     c->bid, c->bcell, c->bcell_start, c->cell_start, c->cnt, c->perm, c->tmp,
                     c->itmp, c->scan_tmp, c->sc, c->pair_cnt, c->bpair_cnt, c->pair_buf_i,
-                    c->pair_buf_j, c->pair_buf_r, c->pair_buf_h};
+                    c->pair_buf_j, c->pair_buf_r, c->pair_buf_h, c->nbr, c->nbr_count,
+                    c->pair_j, c->pair_count,
+                    c->s0.xf, c->s0.yf, c->s0.hsf, c->s1.xf, c->s1.yf};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->sc_host) cudaFreeHost(c->sc_host);
@@ -168,12 +170,18 @@ void free_all(simp_ctx *c) {
     if (c->stream) cudaStreamDestroy(c->stream);
 }
 
-// Grid sizing from host-side extents.  Cell side = (1 + skin) * max(hsml);
+// Verlet-list skin: the parameter when given, else 10% of max(hsml).
+double list_skin(const simp_ctx *c, double hmax) {
+    return (c->prm.skin >= 0.0) ? c->prm.skin : 0.1 * hmax;
+}
+
+// Grid sizing from host-side extents.  Cell side = 1.15 (hsml + skin);
 // the grid covers the particles and walls with a margin; the cell count is
 // capped (a larger side only adds candidates, never drops pairs).
 int size_grid(simp_ctx *c, double xmin, double xmax, double ymin, double ymax, double hmax) {
-    double skin = c->prm.skin;
-    double cs = (skin >= 0.0) ? hmax + skin : hmax * 1.1;
+    // cell side: the Verlet-list reach (hsml + skin) plus 15% for motion
+    // between sorts
+    double cs = (hmax + list_skin(c, hmax)) * 1.15;
     if (!(cs > 0.0)) cs = 1.0;
     const double ext = std::max(xmax - xmin, ymax - ymin);
     const double margin = std::max(2.0 * cs, 0.02 * ext);
@@ -339,7 +347,7 @@ double disp_of(const Scalars &s) {
 
 // Re-sort when the device-side stencil would grow past one cell ring.
 bool wants_rebuild(const simp_ctx *c, const Scalars &s) {
-    return (s.hmax + 2.0 * disp_of(s)) * c->grid.inv_cs > 0.98;
+    return (s.hmax + s.skin + 2.0 * disp_of(s)) * c->grid.inv_cs > 0.98;
 }
 
 // Resize the grid when hsml grew 5% past the bound the grid was sized for
@@ -461,7 +469,8 @@ int32_t simp_gpu_create(const simp_params *params, int32_t maxn, int32_t maxnb, 
     const size_t M = (size_t)maxn, MB = (size_t)c->maxnb, MX = std::max(M, MB);
     double **d1[] = {&c->s0.x, &c->s0.y, &c->s0.vx, &c->s0.vy, &c->s0.m, &c->s0.rho, &c->s0.mor, &c->s0.h,
                      &c->s0.A, &c->s0.hs, &c->s1.x, &c->s1.y, &c->s1.vx, &c->s1.vy, &c->s1.rho,
-                     &c->s1.mor, &c->s1.h, &c->s1.A, &c->xr, &c->yr, &c->tau11, &c->tau12, &c->tau22,
+                     &c->s1.mor, &c->s1.h, &c->s1.A, &c->xr, &c->yr, &c->xl, &c->yl,
+                     &c->tau11, &c->tau12, &c->tau22,
                      &c->div};
     for (double **p : d1) {
         rc = dalloc(c, p, M);
@@ -475,7 +484,15 @@ int32_t simp_gpu_create(const simp_params *params, int32_t maxn, int32_t maxnb, 
         c->s1.m = c->s0.m;
     }
     c->s1.hs = c->s0.hs;
-    if ((rc = dalloc(c, &c->diag, 9 * M)) || (rc = dalloc(c, &c->rates, 4 * M)) ||
+    float **f1[] = {&c->s0.xf, &c->s0.yf, &c->s0.hsf, &c->s1.xf, &c->s1.yf};
+    for (float **p : f1) {
+        rc = dalloc(c, p, M);
+        if (rc) { *out = c; return rc; }
+    }
+    c->s1.hsf = c->s0.hsf;
+    if ((rc = dalloc(c, &c->nbr, (size_t)kMaxNbr * M)) || (rc = dalloc(c, &c->nbr_count, M)) ||
+        (rc = dalloc(c, &c->pair_j, (size_t)kMaxPairs * M)) || (rc = dalloc(c, &c->pair_count, M)) ||
+        (rc = dalloc(c, &c->diag, 9 * M)) || (rc = dalloc(c, &c->rates, 4 * M)) ||
         (rc = dalloc(c, &c->cell, M)) || (rc = dalloc(c, &c->id, M)) || (rc = dalloc(c, &c->inv_id, M)) ||
         (rc = dalloc(c, &c->perm, M)) || (rc = dalloc(c, &c->tmp, 12 * MX)) ||
         (rc = dalloc(c, &c->itmp, 3 * MX)) || (rc = dalloc(c, &c->bx, MB)) || (rc = dalloc(c, &c->by, MB)) ||
@@ -570,12 +587,22 @@ int32_t simp_gpu_set_state(simp_ctx *c, int32_t ntotal, const double *x, const d
     sc.bs = 2.0 * hmin;
     sc.dmax2_bits = 0ull;
     {
+        // bound on |coordinate| for the FP32 prefilter (grows on the device)
+        const double xa = std::max(std::max(std::fabs(xmin), std::fabs(xmax)),
+                                   std::max(std::fabs(ymin), std::fabs(ymax)));
+        std::memcpy(&sc.xabs_bits, &xa, sizeof(double));
+    }
+    {
         const double inf = INFINITY;
         std::memcpy(&sc.acc_hmin, &inf, sizeof(double));
         std::memcpy(&sc.acc_dt, &inf, sizeof(double));
     }
     sc.acc_hmax = 0ull;
     sc.minip = 0x7fffffff;
+    sc.skin = list_skin(c, hmax);
+    sc.dlist2_bits = 0ull;
+    sc.list_scan = 1;
+    sc.blocks_done = 0u;
     *c->sc_host = sc;
     SIMP_CUDA(c, cudaMemcpyAsync(c->sc, c->sc_host, sizeof(Scalars), cudaMemcpyHostToDevice, s));
     TRY(rebuild(c));

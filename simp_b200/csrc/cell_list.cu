@@ -173,17 +173,26 @@ __global__ void k_gather(int n, const int *__restrict__ perm, Gather gd, int nar
     id_out[k] = id_in[o];
 }
 
-__global__ void k_finish_rebuild(int n, const double *__restrict__ x, const double *__restrict__ y,
-                                 double *__restrict__ xr, double *__restrict__ yr,
+// Rebuild-time positions, inverse index and the FP32 copies of the sorted state.
+__global__ void k_finish_rebuild(int n, State s, double *__restrict__ xr, double *__restrict__ yr,
                                  const int *__restrict__ id, int *__restrict__ inv_id) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    xr[k] = x[k];
-    yr[k] = y[k];
+    const double x = s.x[k], y = s.y[k];
+    xr[k] = x;
+    yr[k] = y;
+    s.xf[k] = (float)x;
+    s.yf[k] = (float)y;
+    s.hsf[k] = (float)s.hs[k];
     inv_id[id[k]] = k;
 }
 
-__global__ void k_reset_disp(Scalars *sc) { sc->dmax2_bits = 0ull; }
+// After a sort the cell-order indices in the Verlet lists are stale.
+__global__ void k_reset_disp(Scalars *sc) {
+    sc->dmax2_bits = 0ull;
+    sc->dlist2_bits = 0ull;
+    sc->list_scan = 1;
+}
 
 inline int nblk(long long n, int b) { return (int)((n + b - 1) / b); }
 
@@ -228,7 +237,7 @@ int rebuild(simp_ctx *c) {
         SIMP_CUDA(c, cudaMemcpyAsync(srcs[a], gd.dst[a], sizeof(double) * (size_t)n,
                                      cudaMemcpyDeviceToDevice, s));
     SIMP_CUDA(c, cudaMemcpyAsync(c->id, id_new, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, s));
-    k_finish_rebuild<<<nblk(n, B), B, 0, s>>>(n, c->s0.x, c->s0.y, c->xr, c->yr, c->id, c->inv_id);
+    k_finish_rebuild<<<nblk(n, B), B, 0, s>>>(n, c->s0, c->xr, c->yr, c->id, c->inv_id);
     k_reset_disp<<<1, 1, 0, s>>>(c->sc);
     c->launches += 7 + kScanKernels;
     SIMP_CUDA(c, cudaGetLastError());

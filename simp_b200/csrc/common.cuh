@@ -22,6 +22,29 @@ struct State {
     double *x, *y, *vx, *vy;
     double *m, *rho, *mor, *h, *A;
     double *hs;   // hsml (shared by S0 and S1: updated only at step end)
+    float *xf, *yf, *hsf;  // FP32 copies for the candidate prefilter (hsf shared)
+};
+
+// Verlet neighbour lists (cell-order indices): nbr[k * stride + i],
+// k < count[i], holding every j within mhsml + skin of i at the positions
+// (xl, yl) where the list was built; a count above kMaxNbr means the list
+// overflowed and that particle scans its cell stencil instead.
+constexpr int kMaxNbr = 48;
+struct NbrList {
+    int *nbr;
+    int *count;
+    double *xl, *yl;
+    int stride;
+};
+
+// Exact pairs of the current right-hand side, written by the kinematic pass
+// and consumed by the stress pass: pj[k * stride + i], k < count[i]; a count
+// above kMaxPairs means the stress pass finds that particle's pairs itself.
+constexpr int kMaxPairs = 48;
+struct PairList {
+    int *pj;
+    int *count;
+    int stride;
 };
 
 // Uniform cell grid.  cell = clamp(floor((x - x0) * inv_cs)); rows are y.
@@ -38,6 +61,13 @@ struct Scalars {
     double hmin, hmax;    // exact min / max of the current hsml
     double bs;            // reference bucket size 2 * hmin (nnps.f90:211)
     unsigned long long dmax2_bits;  // max squared displacement since rebuild
+    unsigned long long xabs_bits;   // max |coordinate| of any particle so far
+    // Verlet neighbour lists: members within mhsml + skin when built; valid
+    // while every particle moved less than skin / 2 since (and hsml fixed)
+    unsigned long long dlist2_bits; // max squared displacement since the lists were built
+    double skin;
+    int list_scan;                  // 1: the next kinematic pass rebuilds the lists
+    unsigned int blocks_done;       // last-block detection of the stress pass
     unsigned long long acc_hmin, acc_hmax;  // accumulators of the next hsml
     unsigned long long acc_dt;              // VP time step min accumulator
     int flags;            // bit 0: non-finite state seen

@@ -23,11 +23,16 @@ struct simp_ctx {
     simp::State s0{}, s1{};
     double *mass1 = nullptr;       // half-step mass when the mass update is on
     double *xr = nullptr, *yr = nullptr;  // positions at the last rebuild
+    double *xl = nullptr, *yl = nullptr;  // positions where each Verlet list was built
     int *cell = nullptr;           // rebuild-time cell id per particle
     int *id = nullptr;             // original index per particle
     int *inv_id = nullptr;         // cell-order position of original index
     // per-RHS intermediates from the kinematic pass
     double *tau11 = nullptr, *tau12 = nullptr, *tau22 = nullptr, *div = nullptr;
+    int *nbr = nullptr;            // kMaxNbr * maxn neighbour indices (column-major)
+    int *nbr_count = nullptr;      // maxn
+    int *pair_j = nullptr;         // kMaxPairs * maxn exact pairs of the current RHS
+    int *pair_count = nullptr;     // maxn
     // diagnostics (epsilon_11.. sigma_22, zeta, eta, p)
     double *diag = nullptr;        // 9 * maxn
     // rates of the last single_step (cell order): ax, ay, dhdt, dAdt

@@ -90,6 +90,27 @@ __device__ __forceinline__ int for_each_wall(const double *__restrict__ BX, cons
     return count;
 }
 
+// FP32 prefilter of the pair criterion.  The float copies of x, y, hsml are
+// within X 2^-24 (X = max |coordinate|) and hsml 2^-24 of the doubles; the
+// float subtraction of two nearby coordinates is exact.  So the float
+// squared distance and squared mhsml differ from the exact ones by at most
+// (5.7 X / hmin + 12) 2^-24 relative near the decision boundary (where
+// mhsml >= hmin).  The returned margin doubles that bound; a candidate is
+// decided in FP32 only outside the margin, otherwise by the exact FP64 test.
+__device__ __forceinline__ float prefilter_margin(const Scalars *sc) {
+    const double X = bitsd(sc->xabs_bits);
+    return (float)((12.0 * X / sc->hmin + 40.0) * 0x1p-24);
+}
+
+// 0: not a pair, 1: a pair, 2: undecided (use the FP64 test)
+__device__ __forceinline__ int prefilter(float dxf, float dyf, float mf, float margin) {
+    const float sf = dxf * dxf + dyf * dyf;
+    const float tf = mf * mf;
+    if (sf > tf * (1.0f + margin)) return 0;
+    if (sf < tf * (1.0f - margin)) return 1;
+    return 2;
+}
+
 // Stencil radius for wall pairs: walls are static, the particle moved at
 // most sqrt(dmax2) since it was binned.
 __device__ __forceinline__ int wall_radius(const Scalars *sc, const Grid &g, double b_length) {

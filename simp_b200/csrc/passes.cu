@@ -1,19 +1,24 @@
 // The two pair passes of one right-hand-side evaluation (single_step.f90:5-109)
 // and the predictor-corrector update fused into the second pass's epilogue.
 //
-// Kinematic pass (single_step.f90:50-84 + internal_stress.f90:20-42):
-//   gather over neighbours j of i:
-//     wdvx = (v_i - v_j) (x) grad W_ij             (kernel.f90:515-518)
-//     div_i  -= m_j (wdvx1 + wdvx4)                (vector_divergence.f90:27)
-//     grad_i -= m_j wdvx / rho_j                   (vector_gradient.f90:56-69)
-//   then, per particle, strain (single_step.f90:80-84), strength, bulk and
-//   shear viscosity, replacement pressure and stress (bulk_viscosity.f90:
-//   65-76, shear_viscosity.f90:57, eos.f90:141-147, stress_tensor.f90:31-39).
-//   Writes tau = sigma / rho^2 and div per particle.
+// Kinematic pass (single_step.f90:50-84 + internal_stress.f90:20-42), per
+// particle i, in two phases:
+//   1. candidate scan of the cell stencil with an FP32 prefilter and the
+//      exact FP64 criterion for undecided candidates (neighbors.cuh); the
+//      accepted neighbours go to a per-thread list in shared memory and to
+//      the neighbour list in HBM that the stress pass reuses;
+//   2. FP64 pair math over the dense list:
+//        wdvx = (v_i - v_j) (x) grad W_ij            (kernel.f90:515-518)
+//        div_i  -= m_j (wdvx1 + wdvx4)               (vector_divergence.f90:27)
+//        grad_i -= m_j wdvx / rho_j                  (vector_gradient.f90:56-69)
+//   then strain (single_step.f90:80-84), strength, bulk and shear viscosity,
+//   replacement pressure and stress (bulk_viscosity.f90:65-76,
+//   shear_viscosity.f90:57, eos.f90:141-147, stress_tensor.f90:31-39).
+//   Writes tau = sigma / rho^2 and div.
 //
 // Stress pass (internal_stress.f90:103-137 stress_1, boundary_kernel.f90 +
 // boundary_force.f90:74-84, wind_forcing.f90:35-51, water_drag.f90:35-53,
-// single_step.f90:104-106):
+// single_step.f90:104-106) over the kinematic pass's neighbour list:
 //   a_i = rho_i / (rho_ice h_i) sum_j m_j (tau_i + tau_j) . grad W_ij
 //         - sum_walls F_b / rho_i + wind + water drag
 //   followed by one of three epilogues: the rates (single_step), the
@@ -33,6 +38,132 @@ namespace simp {
 namespace {
 
 constexpr int kBlock = 128;
+// per-thread shared-memory list: the whole pair list of a particle with up
+// to kMaxPairs pairs (then written out row by row), flushed when full
+constexpr int kListSlots = kMaxPairs + 1;
+
+// Per-pair FP64 geometry and kernel gradient: dw = gfac * (dx, dy).
+// r = s * rsqrt(s) and 1/hsml_ij from the particle's own 1/hsml when the two
+// smoothing lengths are equal (then hsml_ij = hsml_i exactly).
+struct PairGeom {
+    double dx, dy, gfac, w;
+};
+
+template <bool WANT_W>
+__device__ __forceinline__ PairGeom pair_geom(const Phys &P, double xi, double yi, double hi, double inv_hi,
+                                              double xj, double yj, double hj) {
+    PairGeom g;
+    g.dx = xi - xj;
+    g.dy = yi - yj;
+    const double s = g.dx * g.dx + g.dy * g.dy;
+    const double rs = rsqrt(s);
+    const double r = s * rs;
+    const double inv_h = (hj == hi) ? inv_hi : 2.0 / (hi + hj);
+    const double sh = (double)P.scale_h;
+    const double shh = sh * inv_h;
+    const double q = r * shh;
+    double gq;
+    if (P.skf == SIMP_SKF_WENDLAND_C6) {
+        const double factor = (78.0 / (7.0 * kPi)) * (shh * shh);
+        const double om = 1.0 - q;
+        const double om2 = om * om, om4 = om2 * om2;
+        if (WANT_W) g.w = factor * (om4 * om4) * (((32.0 * q + 25.0) * q + 8.0) * q + 1.0);
+        gq = factor * (-22.0 * q * (om4 * om2 * om) * ((16.0 * q + 7.0) * q + 1.0));
+    } else {
+        const double factor = (15.0 / (7.0 * kPi)) * (shh * shh);
+        if (q <= 1.0) {
+            if (WANT_W) g.w = factor * ((double)(2.0f / 3.0f) - q * q + 0.5 * q * q * q);
+            gq = factor * (-2.0 * q + 1.5 * q * q);
+        } else {
+            const double u = 2.0 - q;
+            if (WANT_W) g.w = factor * ((double)(1.0f / 6.0f) * u * u * u);
+            gq = factor * (-0.5 * u * u);
+        }
+    }
+    g.gfac = gq * shh * rs;
+    return g;
+}
+
+// What a pass needs to decide the reference criterion for particle i.
+struct PairCtx {
+    double xi, yi, hi;
+    float xif, yif, hif;
+    float margin;
+    bool use_f32;
+    BinRule br;
+};
+
+__device__ __forceinline__ PairCtx pair_ctx(const State &s, const Scalars *sc, int i) {
+    PairCtx p;
+    p.xi = s.x[i];
+    p.yi = s.y[i];
+    p.hi = s.hs[i];
+    p.xif = s.xf[i];
+    p.yif = s.yf[i];
+    p.hif = s.hsf[i];
+    p.margin = prefilter_margin(sc);
+    p.use_f32 = p.margin < 0.25f;
+    p.br = make_bin_rule(sc, p.xi, p.yi, sc->hmax);
+    return p;
+}
+
+// The reference criterion for candidate j, decided exactly: FP32 prefilter,
+// the FP64 test of nnps.f90:277-281 when undecided, then the bucket rule.
+__device__ __forceinline__ bool is_pair(const State &s, const PairCtx &p, int j) {
+    int dec = 2;
+    if (p.use_f32) dec = prefilter(p.xif - s.xf[j], p.yif - s.yf[j], 0.5f * (p.hif + s.hsf[j]), p.margin);
+    if (dec == 0) return false;
+    if (dec == 2 || p.br.on) {
+        const double xj = s.x[j], yj = s.y[j];
+        if (dec == 2) {
+            double r;
+            const double mh = __dmul_rn(__dadd_rn(p.hi, s.hs[j]), 0.5);
+            if (!pair_test(__dsub_rn(p.xi, xj), __dsub_rn(p.yi, yj), mh, &r)) return false;
+        }
+        if (!bin_rule_ok(p.br, xj, yj)) return false;
+    }
+    return true;
+}
+
+// Visits the cell-stencil candidates of particle i (cell order).
+template <class F>
+__device__ __forceinline__ void for_stencil(const Grid &g, int i, int ci, int R, F &&f) {
+    const int cx = ci % g.ncx, cy = ci / g.ncx;
+    const int r0 = max(cy - R, 0), r1 = min(cy + R, g.ncy - 1);
+    const int c0 = max(cx - R, 0), c1 = min(cx + R, g.ncx - 1);
+    for (int row = r0; row <= r1; ++row) {
+        const int j0 = g.cell_start[row * g.ncx + c0];
+        const int j1 = g.cell_start[row * g.ncx + c1 + 1];
+        for (int j = j0; j < j1; ++j)
+            if (j != i) f(j);
+    }
+}
+
+// Every current pair of particle i: from its Verlet list when that list
+// still holds every pair, else from its cell stencil.  The lists were all
+// built at the same positions (xl, yl) with members within mhsml + skin; a
+// current pair (i, j) was then at most mhsml + |dx_i| + |dx_j| apart, so i's
+// list is complete while |dx_i| + max_j |dx_j| < skin.
+template <class F>
+__device__ __forceinline__ void for_each_current_pair(const State &s, const Grid &g, const NbrList &nl,
+                                                      const Scalars *sc, int i, int ci, const PairCtx &p,
+                                                      F &&on_pair) {
+    const int cnt = nl.count[i];
+    const double dxl = p.xi - nl.xl[i], dyl = p.yi - nl.yl[i];
+    const double own = sqrt(dxl * dxl + dyl * dyl);
+    const double all = sqrt(bitsd(sc->dlist2_bits));
+    const bool valid = (own + all) * (1.0 + 1e-9) < sc->skin;
+    if (cnt <= kMaxNbr && valid) {
+        for (int k = 0; k < cnt; ++k) {
+            const int j = nl.nbr[(size_t)k * nl.stride + i];
+            if (is_pair(s, p, j)) on_pair(j);
+        }
+    } else {
+        for_stencil(g, i, ci, stencil_radius(sc, g, 0.0), [&](int j) {
+            if (is_pair(s, p, j)) on_pair(j);
+        });
+    }
+}
 
 struct KinArgs {
     State s;
@@ -42,32 +173,72 @@ struct KinArgs {
     Scalars *sc;
     double *tau11, *tau12, *tau22, *div;
     double *diag;
+    NbrList nl;
+    PairList pl;
     int n, maxn;
 };
 
 __global__ void __launch_bounds__(kBlock) k_kinematic(KinArgs a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ int s_list[kListSlots * kBlock];
+    const int t = threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + t;
     if (i >= a.n) return;
     const State &s = a.s;
     const Phys &P = a.P;
-    const double xi = s.x[i], yi = s.y[i], vxi = s.vx[i], vyi = s.vy[i], hi = s.hs[i];
-    const int R = stencil_radius(a.sc, a.g, 0.0);
-    const BinRule br = make_bin_rule(a.sc, xi, yi, a.sc->hmax);
+    const PairCtx pc = pair_ctx(s, a.sc, i);
+    const double xi = pc.xi, yi = pc.yi, hi = pc.hi;
+    const double vxi = s.vx[i], vyi = s.vy[i];
+    const double inv_hi = 1.0 / hi;
     double dv = 0.0, g1 = 0.0, g2 = 0.0, g3 = 0.0, g4 = 0.0;
-    for_each_pair(s.x, s.y, s.hs, a.g, i, a.cell[i], R, br, xi, yi, hi,
-                  [&](int j, double dx, double dy, double r, double mh) {
-                      double gf;
-                      pair_kernel<false>(P, r, mh, nullptr, &gf);
-                      const double dwx = gf * dx, dwy = gf * dy;
-                      const double dvx = vxi - s.vx[j], dvy = vyi - s.vy[j];
-                      const double w1 = dvx * dwx, w2 = dvy * dwx, w3 = dvx * dwy, w4 = dvy * dwy;
-                      const double mj = s.m[j], mrj = s.mor[j];
-                      dv -= mj * (w1 + w4);
-                      g1 -= mrj * w1;
-                      g2 -= mrj * w2;
-                      g3 -= mrj * w3;
-                      g4 -= mrj * w4;
-                  });
+    int cnt = 0;       // entries in this thread's shared-memory list
+    int npairs = 0;    // exact pairs found so far
+    auto flush = [&]() {
+        for (int k = 0; k < cnt; ++k) {
+            const int j = s_list[k * kBlock + t];
+            const PairGeom pg = pair_geom<false>(P, xi, yi, hi, inv_hi, s.x[j], s.y[j], s.hs[j]);
+            const double dwx = pg.gfac * pg.dx, dwy = pg.gfac * pg.dy;
+            const double dvx = vxi - s.vx[j], dvy = vyi - s.vy[j];
+            const double w1 = dvx * dwx, w2 = dvy * dwx, w3 = dvx * dwy, w4 = dvy * dwy;
+            const double mj = s.m[j], mrj = s.mor[j];
+            dv -= mj * (w1 + w4);
+            g1 -= mrj * w1;
+            g2 -= mrj * w2;
+            g3 -= mrj * w3;
+            g4 -= mrj * w4;
+        }
+        cnt = 0;
+    };
+    auto on_pair = [&](int j) {
+        s_list[cnt * kBlock + t] = j;
+        ++npairs;
+        if (++cnt == kListSlots) flush();   // more than kMaxPairs pairs: no pair list
+    };
+    if (a.sc->list_scan) {
+        // rebuild the Verlet list from the cell stencil: members are the
+        // candidates not certainly beyond mhsml + skin (FP32, with margin)
+        const double skin = a.sc->skin;
+        const float skinf = (float)skin, grow = 1.0f + pc.margin;
+        int total = 0;
+        for_stencil(a.g, i, a.cell[i], stencil_radius(a.sc, a.g, a.sc->hmax + skin), [&](int j) {
+            const float dxf = pc.xif - s.xf[j], dyf = pc.yif - s.yf[j];
+            const float lim = 0.5f * (pc.hif + s.hsf[j]) + skinf;
+            if (dxf * dxf + dyf * dyf > lim * lim * grow) return;
+            if (total < kMaxNbr) a.nl.nbr[(size_t)total * a.nl.stride + i] = j;
+            ++total;
+            if (is_pair(s, pc, j)) on_pair(j);
+        });
+        a.nl.count[i] = total;
+        a.nl.xl[i] = xi;
+        a.nl.yl[i] = yi;
+        if (i == 0) atomicExch(&a.sc->dlist2_bits, 0ull);
+    } else {
+        for_each_current_pair(s, a.g, a.nl, a.sc, i, a.cell[i], pc, on_pair);
+    }
+    // the stress pass's pair list, one coalesced row per k
+    if (npairs <= kMaxPairs)
+        for (int k = 0; k < cnt; ++k) a.pl.pj[(size_t)k * a.pl.stride + i] = s_list[k * kBlock + t];
+    a.pl.count[i] = npairs;
+    flush();
     // strain rates, single_step.f90:80-84
     const double e11 = g1, e22 = g4, e12 = 0.5 * (g2 + g3);
     // rheology, internal_stress.f90:20-42
@@ -120,29 +291,48 @@ struct StressArgs {
     Phys P;
     Scalars *sc;
     const double *tau11, *tau12, *tau22, *div;
+    NbrList nl;
+    PairList pl;
     double *rates;
     const double *xr, *yr;
     double *hs_next;
     int n, maxn, mode;
 };
 
-__device__ __forceinline__ void warp_max_u64(unsigned long long *dst, unsigned long long v) {
+// Block-wide max / min folded into one device atomic per block (the
+// same-address atomics of every warp would serialise in L2).  Called by all
+// threads of the block at the same point.
+template <bool MAX>
+__device__ __forceinline__ void block_reduce_u64(unsigned long long *dst, unsigned long long v) {
+    __shared__ unsigned long long part[kBlock / 32];
     for (int o = 16; o > 0; o >>= 1) {
         const unsigned long long t = __shfl_xor_sync(0xffffffffu, v, o);
-        v = (t > v) ? t : v;
+        v = MAX ? (t > v ? t : v) : (t < v ? t : v);
     }
-    if ((threadIdx.x & 31) == 0) atomicMax(dst, v);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < kBlock / 32; ++w) v = MAX ? (part[w] > v ? part[w] : v) : (part[w] < v ? part[w] : v);
+        if (MAX) atomicMax(dst, v); else atomicMin(dst, v);
+    }
+    __syncthreads();
+}
+__device__ __forceinline__ void warp_max_u64(unsigned long long *dst, unsigned long long v) {
+    block_reduce_u64<true>(dst, v);
 }
 __device__ __forceinline__ void warp_min_u64(unsigned long long *dst, unsigned long long v) {
-    for (int o = 16; o > 0; o >>= 1) {
-        const unsigned long long t = __shfl_xor_sync(0xffffffffu, v, o);
-        v = (t < v) ? t : v;
-    }
-    if ((threadIdx.x & 31) == 0) atomicMin(dst, v);
+    block_reduce_u64<false>(dst, v);
 }
 __device__ __forceinline__ void warp_max_i32(int *dst, int v) {
+    __shared__ int part[kBlock / 32];
     for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(dst, v);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < kBlock / 32; ++w) v = max(v, part[w]);
+        atomicMax(dst, v);
+    }
+    __syncthreads();
 }
 
 __global__ void __launch_bounds__(kBlock) k_stress(StressArgs a) {
@@ -152,22 +342,31 @@ __global__ void __launch_bounds__(kBlock) k_stress(StressArgs a) {
     const State &s = a.rhs;
     const Phys &P = a.P;
     const double xi = s.x[i], yi = s.y[i], hi = s.hs[i];
+    const double inv_hi = 1.0 / hi;
     const int ci = a.cell[i];
-    const int R = stencil_radius(a.sc, a.g, 0.0);
-    const BinRule br = make_bin_rule(a.sc, xi, yi, a.sc->hmax);
     double Sx = 0.0, Sy = 0.0, Tx = 0.0, Ty = 0.0;
-    int cnt = for_each_pair(s.x, s.y, s.hs, a.g, i, ci, R, br, xi, yi, hi,
-                            [&](int j, double dx, double dy, double r, double mh) {
-                                double gf;
-                                pair_kernel<false>(P, r, mh, nullptr, &gf);
-                                const double dwx = gf * dx, dwy = gf * dy;
-                                const double mj = s.m[j];
-                                const double t11 = a.tau11[j], t12 = a.tau12[j], t22 = a.tau22[j];
-                                Sx += mj * dwx;
-                                Sy += mj * dwy;
-                                Tx += mj * (t11 * dwx + t12 * dwy);
-                                Ty += mj * (t12 * dwx + t22 * dwy);
-                            });
+    auto accumulate = [&](int j) {
+        const PairGeom pg = pair_geom<false>(P, xi, yi, hi, inv_hi, s.x[j], s.y[j], s.hs[j]);
+        const double dwx = pg.gfac * pg.dx, dwy = pg.gfac * pg.dy;
+        const double mj = s.m[j];
+        const double t11 = a.tau11[j], t12 = a.tau12[j], t22 = a.tau22[j];
+        Sx += mj * dwx;
+        Sy += mj * dwy;
+        Tx += mj * (t11 * dwx + t12 * dwy);
+        Ty += mj * (t12 * dwx + t22 * dwy);
+    };
+    int cnt = a.pl.count[i];
+    if (cnt <= kMaxPairs) {
+        // the kinematic pass of this right-hand side found the pairs
+        for (int k = 0; k < cnt; ++k) accumulate(a.pl.pj[(size_t)k * a.pl.stride + i]);
+    } else {
+        cnt = 0;
+        const PairCtx pc = pair_ctx(s, a.sc, i);
+        for_each_current_pair(s, a.g, a.nl, a.sc, i, ci, pc, [&](int j) {
+            accumulate(j);
+            ++cnt;
+        });
+    }
     const double rho = s.rho[i], hh = s.h[i], AA = s.A[i], mi = s.m[i];
     const double fi = rho / P.rho_ice / hh;
     double ax = fi * (a.tau11[i] * Sx + a.tau12[i] * Sy + Tx);
@@ -261,10 +460,15 @@ __global__ void __launch_bounds__(kBlock) k_stress(StressArgs a) {
     const double dxr = xn - a.xr[i], dyr = yn - a.yr[i];
     const double d2 = live ? dxr * dxr + dyr * dyr : 0.0;
     warp_max_u64(&a.sc->dmax2_bits, dbits(d2));
+    const double dxl = xn - a.nl.xl[i], dyl = yn - a.nl.yl[i];
+    warp_max_u64(&a.sc->dlist2_bits, dbits(live ? dxl * dxl + dyl * dyl : 0.0));
+    warp_max_u64(&a.sc->xabs_bits, dbits(fmax(fabs(xn), fabs(yn))));
     if (live) {
         const State &o = a.out;
         o.x[i] = xn;
         o.y[i] = yn;
+        o.xf[i] = (float)xn;
+        o.yf[i] = (float)yn;
         o.vx[i] = vxn;
         o.vy[i] = vyn;
         o.h[i] = hn;
@@ -287,6 +491,35 @@ __global__ void __launch_bounds__(kBlock) k_stress(StressArgs a) {
                            isfinite(hn) && isfinite(An));
         if (live && bad) atomicOr(&a.sc->flags, FLAG_NONFINITE);
     }
+    // The last block to finish decides whether the next kinematic pass
+    // rebuilds the Verlet lists: when the fastest particle moved 3/4 of the
+    // skin since they were built (lists are then complete only for particles
+    // that moved less than skin / 4), or when hsml changes (sle = 2).
+    // Threadfence reduction; no block waits on another.
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(&a.sc->blocks_done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        const double dl = sqrt(bitsd(atomicAdd(&a.sc->dlist2_bits, 0ull)));
+        const bool stale = (P.sle == 2) || !(dl < 0.75 * a.sc->skin);
+        a.sc->list_scan = stale ? 1 : 0;
+        a.sc->blocks_done = 0u;
+    }
+}
+
+// New hsml of the next step (sle = 2) and its FP32 copy.
+__global__ void k_commit_hsml(int n, const double *__restrict__ hs_next, double *__restrict__ hs,
+                              float *__restrict__ hsf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double v = hs_next[i];
+    hs[i] = v;
+    hsf[i] = (float)v;
 }
 
 // End of a predictor-corrector step: time_step's new dt, current_time += dt
@@ -317,6 +550,24 @@ __global__ void k_reset_stats(Scalars *sc) {
 
 inline int nblk(long long n, int b) { return (int)((n + b - 1) / b); }
 
+NbrList nbr_list(simp_ctx *c) {
+    NbrList nl;
+    nl.nbr = c->nbr;
+    nl.count = c->nbr_count;
+    nl.xl = c->xl;
+    nl.yl = c->yl;
+    nl.stride = c->maxn;
+    return nl;
+}
+
+PairList pair_list(simp_ctx *c) {
+    PairList pl;
+    pl.pj = c->pair_j;
+    pl.count = c->pair_count;
+    pl.stride = c->maxn;
+    return pl;
+}
+
 }  // namespace
 
 void launch_kinematic(simp_ctx *c, const State &s, bool diag) {
@@ -331,6 +582,8 @@ void launch_kinematic(simp_ctx *c, const State &s, bool diag) {
     a.tau22 = c->tau22;
     a.div = c->div;
     a.diag = diag ? c->diag : nullptr;
+    a.nl = nbr_list(c);
+    a.pl = pair_list(c);
     a.n = c->n;
     a.maxn = c->maxn;
     k_kinematic<<<nblk(c->n, kBlock), kBlock, 0, c->stream>>>(a);
@@ -355,10 +608,12 @@ void launch_stress(simp_ctx *c, const State &rhs, const State &base, EpiMode mod
     a.tau12 = c->tau12;
     a.tau22 = c->tau22;
     a.div = c->div;
+    a.nl = nbr_list(c);
+    a.pl = pair_list(c);
     a.rates = c->rates;
     a.xr = c->xr;
     a.yr = c->yr;
-    a.hs_next = c->tmp;   // hsml of the next step (copied back by the caller)
+    a.hs_next = c->tmp;   // hsml of the next step (committed by launch_step_finish)
     a.n = c->n;
     a.maxn = c->maxn;
     a.mode = mode;
@@ -367,9 +622,10 @@ void launch_stress(simp_ctx *c, const State &rhs, const State &base, EpiMode mod
 }
 
 void launch_step_finish(simp_ctx *c) {
-    if (c->prm.sle == 2)
-        cudaMemcpyAsync(c->s0.hs, c->tmp, sizeof(double) * (size_t)c->n, cudaMemcpyDeviceToDevice,
-                        c->stream);
+    if (c->prm.sle == 2) {
+        k_commit_hsml<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->n, c->tmp, c->s0.hs, c->s0.hsf);
+        c->launches += 1;
+    }
     k_step_finish<<<1, 1, 0, c->stream>>>(c->sc, c->prm.tse, c->prm.sle);
     c->launches += 1;
 }

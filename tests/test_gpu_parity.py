@@ -168,6 +168,43 @@ def test_trajectory_cfg1_20_steps(gpu_lib, oracle_mod):
         assert rel_l2(sg[k] - (b.x if k == "x" else 0), so[k] - (b.x if k == "x" else 0)) < TOL_TRAJ_20, k
 
 
+def test_single_step_after_motion_filters_lists_exactly(gpu_lib, oracle_mod):
+    """After steps in which the Verlet lists stay valid, one RHS on the moved
+    state equals the oracle's (which searches pairs from scratch)."""
+    b = basins.cfg1()
+    b.vx = smooth_velocity(b.x, b.L, amp=2.0, seed=4)
+    g = Simp.from_basin(b)
+    g.time_integration(12)
+    st = g.get_state()
+    o = oracle_mod.Oracle.from_basin(b)
+    o.set_state(st["x"], st["vx"], st["mass"], st["rho"], st["hsml"], st["A"], st["h"],
+                b.xb, b.massb, b.params.dt, st["current_time"])
+    rg, ro = g.single_step(st["current_time"]), o.single_step(st["current_time"])
+    for k in ("dvxdt", "dhdt", "dAdt"):
+        assert rel_l2(rg[k], ro[k]) < TOL_RHS, (k, rel_l2(rg[k], ro[k]))
+
+
+def test_trajectory_fast_motion_rebuilds(gpu_lib, oracle_mod):
+    """Displacements of tens of metres per step: the Verlet lists (skin
+    480 m) are rebuilt every few steps and the cell list is re-sorted; the
+    trajectory still follows the oracle's."""
+    b = basins.cfg1()
+    b.vx = smooth_velocity(b.x, b.L, amp=8.0, seed=5)
+    prm = b.params.copy()
+    prm.dt = 5.0
+    g, o = _pair(b, oracle_mod, prm)
+    for _ in range(4):
+        g.time_integration(5)
+        o.step(5)
+        sg, so = g.get_state(), o.get_state()
+        for k in ("vx", "h"):
+            assert rel_l2(sg[k], so[k]) < TOL_TRAJ_20, (k, rel_l2(sg[k], so[k]))
+        # same inputs for both from here on: pair lists bit-exact
+        o.set_state(sg["x"], sg["vx"], sg["mass"], sg["rho"], sg["hsml"], sg["A"], sg["h"],
+                    b.xb, b.massb, prm.dt, sg["current_time"])
+        assert_same_pairs(g.nnps(), o.nnps())
+
+
 def test_trajectory_vp_timestep_and_marquis_hsml(gpu_lib, oracle_mod):
     """Reference default switches: sle = 2 (Marquis hsml), tse = 2 (VP dt),
     Wendland C6, mass from the lattice."""
