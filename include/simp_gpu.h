@@ -186,6 +186,47 @@ SIMP_API int32_t simp_gpu_interaction_stats(simp_ctx *ctx, int32_t *maxip,
                                    int32_t *minip, int64_t *sumip,
                                    int32_t *noip);
 
+/* ---- batches of basins ---------------------------------------------------
+ * A batch context holds up to max_instances independent basins (instances)
+ * of different sizes and forcings, resident together and advanced together
+ * by simp_gpu_step: every kernel of a step covers all instances in one
+ * launch.  Each instance has its own cell grid and its own current_time; all
+ * share the context's simp_params (physics, fixed dt: tse = 0, fixed hsml:
+ * sle = 0).  An instance's results do not depend on which other instances
+ * share the batch.  No reference counterpart (the reference runs one basin
+ * per process). */
+typedef struct simp_forcing {
+    int32_t wind_kind;         /* SIMP_WIND_*                                   */
+    int32_t reserved0;
+    double wind_u, wind_v;     /* uniform wind (m/s)                            */
+    double vortex_x, vortex_y, vortex_umax, vortex_radius;
+} simp_forcing;
+
+/* maxn / maxnb: particle and wall capacities over all instances; at most
+ * 2,097,151 particles per instance; max_instances <= 1024. */
+SIMP_API int32_t simp_gpu_create_batch(const simp_params *params, int32_t maxn, int32_t maxnb,
+                                       int32_t max_instances, simp_ctx **out);
+/* Admits one basin (arrays as in simp_gpu_set_state; its current_time starts
+ * at 0) into a free slot, returned in *slot.  SIMP_ERR_MAXN when the
+ * capacities or the slots are exhausted. */
+SIMP_API int32_t simp_gpu_batch_add(simp_ctx *ctx, const simp_forcing *forcing, int32_t ntotal,
+                                    const double *x, const double *vx, const double *mass,
+                                    const double *rho, const double *hsml, const double *A,
+                                    const double *h, int32_t ntotalb, const double *xb,
+                                    const double *massb, int32_t *slot);
+/* Retires a basin and frees its slot and storage. */
+SIMP_API int32_t simp_gpu_batch_remove(simp_ctx *ctx, int32_t slot);
+/* State of one basin in its own particle order (pointers may be NULL). */
+SIMP_API int32_t simp_gpu_batch_get_state(simp_ctx *ctx, int32_t slot, double *x, double *vx,
+                                          double *mass, double *rho, double *hsml, double *A,
+                                          double *h, double *current_time);
+/* Particles, steps advanced and status flags (bit 0: non-finite) of a slot;
+ * *ntotal = 0 for a free slot.  In a batch, a basin whose state turns
+ * non-finite only sets its flag: simp_gpu_step keeps advancing the batch
+ * and the caller retires that basin. */
+SIMP_API int32_t simp_gpu_batch_info(simp_ctx *ctx, int32_t slot, int32_t *ntotal,
+                                     int64_t *steps, int32_t *flags);
+
 /* Summation density (the same result as simp_gpu_sum_density) for callers
  * that cannot allocate device memory.  No counterpart in the reference: it
  * exists for hosts whose device memory belongs to another runtime (CUDA

@@ -8,7 +8,7 @@ from __future__ import annotations
 import ctypes
 import os
 
-from .params import SimpParams
+from .params import SimpForcing, SimpParams
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsimp_gpu.so")
@@ -22,7 +22,13 @@ _i32 = ctypes.c_int32
 SIGNATURES = {
     "simp_params_reference_default": (None, [ctypes.POINTER(SimpParams)]),
     "simp_gpu_create": (_i32, [ctypes.POINTER(SimpParams), _i32, _i32, ctypes.POINTER(_vp)]),
+    "simp_gpu_create_batch": (_i32, [ctypes.POINTER(SimpParams), _i32, _i32, _i32, ctypes.POINTER(_vp)]),
     "simp_gpu_destroy": (_i32, [_vp]),
+    "simp_gpu_batch_add": (_i32, [_vp, ctypes.POINTER(SimpForcing), _i32, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
+                                  _i32, _dp, _dp, _ip]),
+    "simp_gpu_batch_remove": (_i32, [_vp, _i32]),
+    "simp_gpu_batch_get_state": (_i32, [_vp, _i32, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
+    "simp_gpu_batch_info": (_i32, [_vp, _i32, _ip, ctypes.POINTER(ctypes.c_int64), _ip]),
     "simp_gpu_set_state": (_i32, [_vp, _i32, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _i32, _dp, _dp,
                                   ctypes.c_double, ctypes.c_double]),
     "simp_gpu_get_state": (_i32, [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),

@@ -1,5 +1,6 @@
-// C ABI of the SIMP hot path (include/simp_gpu.h): context lifecycle, state
-// transfer in the reference's Fortran layouts, and the per-step driver.
+// C ABI of the SIMP hot path (include/simp_gpu.h): context lifecycle, basin
+// (instance) admission and removal, state transfer in the reference's
+// Fortran layouts, and the per-step driver.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -23,8 +24,14 @@ int simp_cuda_check(simp_ctx *c, cudaError_t e, const char *what) {
 namespace {
 
 constexpr int kB = 256;
-constexpr int kSnapRing = 3;
+constexpr int kIdShift = 21;   // batch particle ids: slot << 21 | local index
 inline int nblk(long long n, int b) { return (int)((n + b - 1) / b); }
+
+#define TRY(expr)                       \
+    do {                                \
+        int _rc = (expr);               \
+        if (_rc != SIMP_OK) return _rc; \
+    } while (0)
 
 __global__ void k_deinterleave(int n, const double *__restrict__ in, double *__restrict__ a,
                                double *__restrict__ b) {
@@ -34,7 +41,44 @@ __global__ void k_deinterleave(int n, const double *__restrict__ in, double *__r
     b[i] = in[2 * i + 1];
 }
 
-// out (original order) <- cell-order arrays
+// New particles [off, off + n): ids, instance, sort positions, m / rho.
+__global__ void k_init_new(int n, int off, int id_base, int slot, int *id, int *pinst, const double *x,
+                           const double *y, double *xr, double *yr, const double *m, const double *rho,
+                           double *mor) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int i = off + k;
+    id[i] = id_base + k;
+    pinst[i] = slot;
+    xr[i] = x[i];
+    yr[i] = y[i];
+    mor[i] = m[i] / rho[i];
+}
+
+__global__ void k_mark_removed(int n, int slot, int *pinst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && pinst[i] == slot) pinst[i] = -1;
+}
+
+// One instance's state to its own particle order: stage = [x,y interleaved |
+// vx,vy interleaved | mass | rho | hsml | A | h], 9 n_k doubles.
+__global__ void k_pack_state(int n, int slot, int id_base, int nk, const int *__restrict__ pinst,
+                             const int *__restrict__ id, State s, double *__restrict__ stage) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n || pinst[k] != slot) return;
+    const size_t o = (size_t)(id[k] - id_base), N = (size_t)nk;
+    stage[2 * o] = s.x[k];
+    stage[2 * o + 1] = s.y[k];
+    stage[2 * N + 2 * o] = s.vx[k];
+    stage[2 * N + 2 * o + 1] = s.vy[k];
+    stage[4 * N + o] = s.m[k];
+    stage[5 * N + o] = s.rho[k];
+    stage[6 * N + o] = s.hs[k];
+    stage[7 * N + o] = s.A[k];
+    stage[8 * N + o] = s.h[k];
+}
+
+// Cell-order arrays of instance 0 to its particle order (single basin).
 __global__ void k_to_orig2(int n, const int *__restrict__ id, const double *__restrict__ a,
                            const double *__restrict__ b, double *__restrict__ out) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -51,31 +95,14 @@ __global__ void k_to_orig1(int n, const int *__restrict__ id, const double *__re
     out[id[k]] = a[k];
 }
 
-// Whole state to original order in one pass: stage = [x,y interleaved | vx,vy
-// interleaved | mass | rho | hsml | A | h], 9 n doubles.
-__global__ void k_pack_state(int n, const int *__restrict__ id, State s, double *__restrict__ stage) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    const size_t o = (size_t)id[k], N = (size_t)n;
-    stage[2 * o] = s.x[k];
-    stage[2 * o + 1] = s.y[k];
-    stage[2 * N + 2 * o] = s.vx[k];
-    stage[2 * N + 2 * o + 1] = s.vy[k];
-    stage[4 * N + o] = s.m[k];
-    stage[5 * N + o] = s.rho[k];
-    stage[6 * N + o] = s.hs[k];
-    stage[7 * N + o] = s.A[k];
-    stage[8 * N + o] = s.h[k];
+__global__ void k_set_time0(Scalars *sc, Inst *inst, double t) {
+    sc->t = t;
+    inst[0].t = t;
 }
 
-__global__ void k_init_ids(int n, int *id, const double *m, const double *rho, double *mor) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    id[k] = k;
-    mor[k] = m[k] / rho[k];
+__global__ void k_grow_xabs(Scalars *sc, double xa) {
+    atomicMax(&sc->xabs_bits, (unsigned long long)__double_as_longlong(xa));
 }
-
-__global__ void k_set_time(Scalars *sc, double t) { sc->t = t; }
 
 Phys make_phys(const simp_params &p, double max_hsml) {
     Phys P{};
@@ -107,19 +134,13 @@ Phys make_phys(const simp_params &p, double max_hsml) {
     P.b_length = p.b_length;
     P.kappa_n = p.kappa_n;
     P.alpha = p.alpha;
-    P.wind_u = p.wind_u;
-    P.wind_v = p.wind_v;
     P.current_u = p.current_u;
     P.current_v = p.current_v;
-    P.vortex_x = p.vortex_x;
-    P.vortex_y = p.vortex_y;
-    P.vortex_umax = p.vortex_umax;
-    P.vortex_radius = p.vortex_radius;
     P.max_hsml = max_hsml;
     return P;
 }
 
-int check_params(simp_ctx *c, const simp_params &p) {
+int check_params(simp_ctx *c, const simp_params &p, bool batch) {
     auto bad = [&](const char *what) { return simp_fail(c, SIMP_ERR_BADARG, std::string("unsupported switch: ") + what); };
     if (p.int_algorithm != 2) return bad("int_algorithm (only 2, predictor-corrector, is on this path)");
     if (p.nnps_algorithm != 1 && p.nnps_algorithm != 2) return bad("nnps_algorithm (1 or 2)");
@@ -132,8 +153,9 @@ int check_params(simp_ctx *c, const simp_params &p) {
     if (p.den_alg != 3) return bad("den_alg (3 in the step; the summation density is simp_gpu_sum_density)");
     if (p.bfa != 1) return bad("bfa (only 1, Monaghan)");
     if (p.boundary_friction) return bad("boundary_friction");
-    if (p.precision != SIMP_PREC_FP64) return bad("precision (this context type is FP64)");
+    if (p.precision != SIMP_PREC_FP64 && p.precision != SIMP_PREC_MIXED) return bad("precision (0 FP64, 1 mixed)");
     if (!(p.e > 0.0) || !(p.rho_ice > 0.0) || !(p.b_length > 0.0)) return bad("material constants");
+    if (batch && (p.tse != 0 || p.sle == 2)) return bad("batches need a fixed dt (tse = 0) and fixed hsml (sle = 0)");
     return SIMP_OK;
 }
 
@@ -145,22 +167,16 @@ int dalloc(simp_ctx *c, T **p, size_t count) {
     return SIMP_OK;
 }
 
-#define TRY(expr)                       \
-    do {                                \
-        int _rc = (expr);               \
-        if (_rc != SIMP_OK) return _rc; \
-    } while (0)
-
 void free_all(simp_ctx *c) {
     void *ptrs[] = {c->s0.x, c->s0.y, c->s0.vx, c->s0.vy, c->s0.m, c->s0.rho, c->s0.mor, c->s0.h,
                     c->s0.A, c->s0.hs, c->s1.x, c->s1.y, c->s1.vx, c->s1.vy, c->s1.rho, c->s1.mor,
-                    c->s1.h, c->s1.A, c->mass1, c->xr, c->yr, c->xl, c->yl, c->cell, c->id, c->inv_id,
+                    c->s1.h, c->s1.A, c->mass1, c->xr, c->yr, c->xl, c->yl, c->cell, c->id, c->pinst,
                     c->tau11, c->tau12, c->tau22, c->div, c->diag, c->rates, c->bx, c->by, c->bm,
-                    c->bid, c->bcell, c->bcell_start, c->cell_start, c->cnt, c->perm, c->tmp,
+                    c->bid, c->binst, c->bcell, c->bcell_start, c->cell_start, c->cnt, c->perm, c->tmp,
                     c->itmp, c->scan_tmp, c->sc, c->pair_cnt, c->bpair_cnt, c->pair_buf_i,
                     c->pair_buf_j, c->pair_buf_r, c->pair_buf_h, c->nbr, c->nbr_count,
-                    c->pair_j, c->pair_count,
-                    c->s0.xf, c->s0.yf, c->s0.hsf, c->s1.xf, c->s1.yf};
+                    c->pair_j, c->pair_count, c->nbr_tmp, c->s0.xf, c->s0.yf, c->s0.hsf, c->s1.xf, c->s1.yf,
+                    c->inst_dev};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->sc_host) cudaFreeHost(c->sc_host);
@@ -170,42 +186,73 @@ void free_all(simp_ctx *c) {
     if (c->stream) cudaStreamDestroy(c->stream);
 }
 
+void invalidate_graph(simp_ctx *c) {
+    if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+    c->step_graph = nullptr;
+}
+
 // Verlet-list skin: the parameter when given, else 10% of max(hsml).
 double list_skin(const simp_ctx *c, double hmax) {
     return (c->prm.skin >= 0.0) ? c->prm.skin : 0.1 * hmax;
 }
 
-// Grid sizing from host-side extents.  Cell side = 1.15 (hsml + skin);
-// the grid covers the particles and walls with a margin; the cell count is
+// Grid of one instance from its extents: cell side 1.15 (hsml + skin) (the
+// Verlet-list reach plus room for motion between sorts); the cell count is
 // capped (a larger side only adds candidates, never drops pairs).
-int size_grid(simp_ctx *c, double xmin, double xmax, double ymin, double ymax, double hmax) {
-    // cell side: the Verlet-list reach (hsml + skin) plus 15% for motion
-    // between sorts
+void size_inst_grid(const simp_ctx *c, InstHost &h, double xmin, double xmax, double ymin, double ymax,
+                    double hmax) {
     double cs = (hmax + list_skin(c, hmax)) * 1.15;
     if (!(cs > 0.0)) cs = 1.0;
     const double ext = std::max(xmax - xmin, ymax - ymin);
     const double margin = std::max(2.0 * cs, 0.02 * ext);
-    const double x0 = xmin - margin, y0 = ymin - margin;
-    const double w = xmax - xmin + 2.0 * margin, h = ymax - ymin + 2.0 * margin;
-    const double cap = std::max(4.0 * (double)c->maxn, 65536.0);
-    while (std::ceil(w / cs) * std::ceil(h / cs) > cap) cs *= 1.25;
-    Grid &g = c->grid;
-    c->grid_hmax = hmax;
-    g.x0 = x0;
-    g.y0 = y0;
-    g.cs = cs;
-    g.inv_cs = 1.0 / cs;
-    g.ncx = std::max(1, (int)std::ceil(w / cs));
-    g.ncy = std::max(1, (int)std::ceil(h / cs));
-    const size_t ncells = (size_t)g.ncx * g.ncy;
-    if (ncells + 1 > c->cell_cap) {
-        if (c->cell_start) cudaFree(c->cell_start);
-        if (c->cnt) cudaFree(c->cnt);
-        if (c->bcell_start) cudaFree(c->bcell_start);
-        if (c->scan_tmp) cudaFree(c->scan_tmp);
+    const double w = xmax - xmin + 2.0 * margin, hh = ymax - ymin + 2.0 * margin;
+    const double cap = std::max(4.0 * (double)h.n, 65536.0);
+    while (std::ceil(w / cs) * std::ceil(hh / cs) > cap) cs *= 1.25;
+    Inst &I = h.I;
+    I.x0 = xmin - margin;
+    I.y0 = ymin - margin;
+    I.cs = cs;
+    I.inv_cs = 1.0 / cs;
+    I.ncx = std::max(1, (int)std::ceil(w / cs));
+    I.ncy = std::max(1, (int)std::ceil(hh / cs));
+    h.grid_hmax = hmax;
+}
+
+// Cell-key bases of the active instances, the device table, the cell-list
+// capacity and the wall cells.  Reads the device table first: current_time,
+// displacement bounds and flags evolve there.
+int layout(simp_ctx *c) {
+    cudaStream_t s = c->stream;
+    std::vector<Inst> cur(c->max_inst);
+    SIMP_CUDA(c, cudaMemcpyAsync(cur.data(), c->inst_dev, sizeof(Inst) * c->max_inst, cudaMemcpyDeviceToHost, s));
+    SIMP_CUDA(c, cudaStreamSynchronize(s));
+    int base = 0, top = 0;
+    for (int q = 0; q < c->max_inst; ++q) {
+        InstHost &h = c->insts[q];
+        if (!h.active) continue;
+        if (h.I.base >= 0) {   // already on the device: keep its evolving fields
+            h.I.t = cur[q].t;
+            h.I.dmax2_bits = cur[q].dmax2_bits;
+            h.I.flags = cur[q].flags;
+            h.I.hmin = cur[q].hmin;
+            h.I.hmax = cur[q].hmax;
+            h.I.bs = cur[q].bs;
+        }
+        h.I.base = base;
+        base += h.I.ncx * h.I.ncy;
+        top = q + 1;
+    }
+    c->total_cells = base;
+    c->ninst = std::max(top, 1);
+    const size_t need = (size_t)base + 2;
+    if (need > c->cell_cap) {
+        cudaFree(c->cell_start);
+        cudaFree(c->cnt);
+        cudaFree(c->bcell_start);
+        cudaFree(c->scan_tmp);
         c->cell_start = c->cnt = c->bcell_start = nullptr;
         c->scan_tmp = nullptr;
-        const size_t capn = ncells + 1;
+        const size_t capn = need + need / 4;
         TRY(dalloc(c, &c->cell_start, capn));
         TRY(dalloc(c, &c->cnt, capn));
         TRY(dalloc(c, &c->bcell_start, capn));
@@ -214,54 +261,175 @@ int size_grid(simp_ctx *c, double xmin, double xmax, double ymin, double ymax, d
         c->scan_tmp_bytes = sb;
         c->cell_cap = capn;
     }
-    g.cell_start = c->cell_start;
-    return SIMP_OK;
-}
-
-// Walls never move: bin them on the host (stable by wall index).
-int bin_walls(simp_ctx *c, int nb, const double *xb, const double *massb) {
-    const Grid &g = c->grid;
-    const size_t ncells = (size_t)g.ncx * g.ncy;
-    std::vector<int> key(nb), order(nb);
-    for (int b = 0; b < nb; ++b) {
-        const int cx = clampi((int)std::floor((xb[2 * b] - g.x0) * g.inv_cs), 0, g.ncx - 1);
-        const int cy = clampi((int)std::floor((xb[2 * b + 1] - g.y0) * g.inv_cs), 0, g.ncy - 1);
-        key[b] = cy * g.ncx + cx;
+    std::vector<Inst> table(c->max_inst);
+    for (int q = 0; q < c->max_inst; ++q) table[q] = c->insts[q].active ? c->insts[q].I : Inst{};
+    SIMP_CUDA(c, cudaMemcpyAsync(c->inst_dev, table.data(), sizeof(Inst) * c->max_inst, cudaMemcpyHostToDevice, s));
+    // walls of every active instance, sorted by cell key (stable)
+    struct W { int key, slot, local; double x, y, m; };
+    std::vector<W> ws;
+    for (int q = 0; q < c->max_inst; ++q) {
+        const InstHost &h = c->insts[q];
+        if (!h.active) continue;
+        const Inst &I = h.I;
+        for (int b = 0; b < h.nb; ++b) {
+            const double xb = h.xb[2 * b], yb = h.xb[2 * b + 1];
+            const int cx = clampi((int)std::floor((xb - I.x0) * I.inv_cs), 0, I.ncx - 1);
+            const int cy = clampi((int)std::floor((yb - I.y0) * I.inv_cs), 0, I.ncy - 1);
+            ws.push_back({I.base + cy * I.ncx + cx, q, b, xb, yb, h.massb[b]});
+        }
     }
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key[a] < key[b]; });
+    std::stable_sort(ws.begin(), ws.end(), [](const W &a, const W &b) { return a.key < b.key; });
+    const int nb = (int)ws.size();
     std::vector<double> hx(nb), hy(nb), hm(nb);
-    std::vector<int> hid(nb), hcell(nb);
-    std::vector<int> start(ncells + 1, 0);
+    std::vector<int> hid(nb), hinst(nb), hcell(nb), start((size_t)base + 1, 0);
     for (int k = 0; k < nb; ++k) {
-        const int b = order[k];
-        hx[k] = xb[2 * b];
-        hy[k] = xb[2 * b + 1];
-        hm[k] = massb[b];
-        hid[k] = b;
-        hcell[k] = key[b];
-        start[key[b] + 1] += 1;
+        hx[k] = ws[k].x;
+        hy[k] = ws[k].y;
+        hm[k] = ws[k].m;
+        hid[k] = ws[k].local;
+        hinst[k] = ws[k].slot;
+        hcell[k] = ws[k].key;
+        start[ws[k].key + 1] += 1;
     }
-    for (size_t k = 0; k < ncells; ++k) start[k + 1] += start[k];
-    cudaStream_t s = c->stream;
+    for (int k = 0; k < base; ++k) start[k + 1] += start[k];
     if (nb > 0) {
         SIMP_CUDA(c, cudaMemcpyAsync(c->bx, hx.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, s));
         SIMP_CUDA(c, cudaMemcpyAsync(c->by, hy.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, s));
         SIMP_CUDA(c, cudaMemcpyAsync(c->bm, hm.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, s));
         SIMP_CUDA(c, cudaMemcpyAsync(c->bid, hid.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, s));
+        SIMP_CUDA(c, cudaMemcpyAsync(c->binst, hinst.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, s));
         SIMP_CUDA(c, cudaMemcpyAsync(c->bcell, hcell.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, s));
     }
-    SIMP_CUDA(c, cudaMemcpyAsync(c->bcell_start, start.data(), sizeof(int) * (ncells + 1),
+    SIMP_CUDA(c, cudaMemcpyAsync(c->bcell_start, start.data(), sizeof(int) * ((size_t)base + 1),
                                  cudaMemcpyHostToDevice, s));
+    SIMP_CUDA(c, cudaStreamSynchronize(s));
+    c->nb = nb;
+    invalidate_graph(c);
+    return SIMP_OK;
+}
+
+DueMask mask_of(int slot) {
+    DueMask m{};
+    if (slot >= 0) m.w[slot >> 6] |= 1ull << (slot & 63);
+    return m;
+}
+
+// Appends one basin's particles after the current ones and sorts it in.
+int add_instance(simp_ctx *c, int slot, const simp_forcing &f, int n, const double *x, const double *vx,
+                 const double *mass, const double *rho, const double *hsml, const double *A,
+                 const double *h, int nb, const double *xb, const double *massb, double t0) {
+    if (n < 1 || nb < 0 || !x || !vx || !mass || !rho || !hsml || !A || !h || (nb > 0 && (!xb || !massb)))
+        return simp_fail(c, SIMP_ERR_BADARG, "bad sizes or null arrays");
+    if (c->n + n > c->maxn)
+        return simp_fail(c, SIMP_ERR_MAXN,
+                         "Resolution desired too high, the number of particles generated is higher "
+                         "than the maximum allowed. (initialize.f90:156-163)");
+    if (c->nb + nb > c->maxnb)
+        return simp_fail(c, SIMP_ERR_MAXN,
+                         "The number of boundary particles generated is higher than the maximum "
+                         "allowed. (boundaries.f90:296-303)");
+    if (c->id_stride && n >= c->id_stride)
+        return simp_fail(c, SIMP_ERR_BADARG, "a basin of a batch holds at most 2,097,151 particles");
+    double xmin = x[0], xmax = x[0], ymin = x[1], ymax = x[1], hmin = hsml[0], hmax = hsml[0];
+    for (int i = 0; i < n; ++i) {
+        xmin = std::min(xmin, x[2 * i]);
+        xmax = std::max(xmax, x[2 * i]);
+        ymin = std::min(ymin, x[2 * i + 1]);
+        ymax = std::max(ymax, x[2 * i + 1]);
+        hmin = std::min(hmin, hsml[i]);
+        hmax = std::max(hmax, hsml[i]);
+        if (!(hsml[i] > 0.0) || !(rho[i] > 0.0) || !(h[i] > 0.0))
+            return simp_fail(c, SIMP_ERR_BADARG, "hsml, rho and h must be positive");
+    }
+    const double pxa = std::max(std::max(std::fabs(xmin), std::fabs(xmax)), std::max(std::fabs(ymin), std::fabs(ymax)));
+    for (int b = 0; b < nb; ++b) {
+        xmin = std::min(xmin, xb[2 * b]);
+        xmax = std::max(xmax, xb[2 * b]);
+        ymin = std::min(ymin, xb[2 * b + 1]);
+        ymax = std::max(ymax, xb[2 * b + 1]);
+    }
+    if (!std::isfinite(xmin + xmax + ymin + ymax))
+        return simp_fail(c, SIMP_ERR_BADARG, "non-finite positions");
+    InstHost &ih = c->insts[slot];
+    ih = InstHost{};
+    ih.active = true;
+    ih.n = n;
+    ih.nb = nb;
+    ih.id_base = c->id_stride * slot;
+    ih.xb.assign(xb, xb + 2 * (size_t)nb);
+    ih.massb.assign(massb, massb + nb);
+    size_inst_grid(c, ih, xmin, xmax, ymin, ymax, hmax);
+    Inst &I = ih.I;
+    I.base = -1;   // not laid out yet
+    I.wind_kind = f.wind_kind;
+    I.wind_u = f.wind_u;
+    I.wind_v = f.wind_v;
+    I.vortex_x = f.vortex_x;
+    I.vortex_y = f.vortex_y;
+    I.vortex_umax = f.vortex_umax;
+    I.vortex_radius = f.vortex_radius;
+    I.b_length = c->prm.b_length;
+    I.t = t0;
+    I.hmin = hmin;
+    I.hmax = hmax;
+    I.bs = 2.0 * hmin;
+    I.dmax2_bits = 0ull;
+    I.flags = 0;
+    // particle arrays at [off, off + n)
+    cudaStream_t s = c->stream;
+    const int off = c->n;
+    const size_t N = (size_t)n;
+    double *stage = c->tmp;
+    SIMP_CUDA(c, cudaMemcpyAsync(stage, x, sizeof(double) * 2 * N, cudaMemcpyHostToDevice, s));
+    SIMP_CUDA(c, cudaMemcpyAsync(stage + 2 * N, vx, sizeof(double) * 2 * N, cudaMemcpyHostToDevice, s));
+    k_deinterleave<<<nblk(n, kB), kB, 0, s>>>(n, stage, c->s0.x + off, c->s0.y + off);
+    k_deinterleave<<<nblk(n, kB), kB, 0, s>>>(n, stage + 2 * N, c->s0.vx + off, c->s0.vy + off);
+    SIMP_CUDA(c, cudaMemcpyAsync(c->s0.m + off, mass, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    SIMP_CUDA(c, cudaMemcpyAsync(c->s0.rho + off, rho, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    SIMP_CUDA(c, cudaMemcpyAsync(c->s0.hs + off, hsml, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    SIMP_CUDA(c, cudaMemcpyAsync(c->s0.A + off, A, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    SIMP_CUDA(c, cudaMemcpyAsync(c->s0.h + off, h, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    k_init_new<<<nblk(n, kB), kB, 0, s>>>(n, off, ih.id_base, slot, c->id, c->pinst, c->s0.x, c->s0.y, c->xr,
+                                          c->yr, c->s0.m, c->s0.rho, c->s0.mor);
+    k_grow_xabs<<<1, 1, 0, s>>>(c->sc, pxa);
+    c->launches += 4;
+    SIMP_CUDA(c, cudaGetLastError());
+    c->n += n;
+    TRY(layout(c));
+    TRY(rebuild(c, mask_of(slot), true, true));
     SIMP_CUDA(c, cudaStreamSynchronize(s));
     return SIMP_OK;
 }
 
-int upload_interleaved(simp_ctx *c, const double *h2, double *a, double *b, int n, double *stage) {
-    SIMP_CUDA(c, cudaMemcpyAsync(stage, h2, sizeof(double) * 2 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
-    k_deinterleave<<<nblk(n, kB), kB, 0, c->stream>>>(n, stage, a, b);
+int remove_instance(simp_ctx *c, int slot) {
+    InstHost &h = c->insts[slot];
+    if (!h.active) return simp_fail(c, SIMP_ERR_BADARG, "slot is free");
+    cudaStream_t s = c->stream;
+    k_mark_removed<<<nblk(c->n, kB), kB, 0, s>>>(c->n, slot, c->pinst);
     c->launches += 1;
-    SIMP_CUDA(c, cudaGetLastError());
+    h = InstHost{};
+    TRY(layout(c));
+    TRY(rebuild(c, DueMask{}, true, false));
+    SIMP_CUDA(c, cudaStreamSynchronize(s));
+    return SIMP_OK;
+}
+
+int reset_all(simp_ctx *c) {
+    for (InstHost &h : c->insts) h = InstHost{};
+    c->n = 0;
+    c->nb = 0;
+    return SIMP_OK;
+}
+
+int read_scalars(simp_ctx *c) {
+    SIMP_CUDA(c, cudaMemcpyAsync(c->sc_host, c->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, c->stream));
+    SIMP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return SIMP_OK;
+}
+
+int read_inst(simp_ctx *c, int slot, Inst *out) {
+    SIMP_CUDA(c, cudaMemcpyAsync(out, c->inst_dev + slot, sizeof(Inst), cudaMemcpyDeviceToHost, c->stream));
+    SIMP_CUDA(c, cudaStreamSynchronize(c->stream));
     return SIMP_OK;
 }
 
@@ -283,13 +451,29 @@ int download1(simp_ctx *c, const double *a, double *h1) {
     return SIMP_OK;
 }
 
-int read_scalars(simp_ctx *c) {
-    SIMP_CUDA(c, cudaMemcpyAsync(c->sc_host, c->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, c->stream));
-    SIMP_CUDA(c, cudaStreamSynchronize(c->stream));
+int get_instance_state(simp_ctx *c, int slot, double *x, double *vx, double *mass, double *rho, double *hsml,
+                       double *A, double *h, double *t) {
+    const InstHost &ih = c->insts[slot];
+    const int nk = ih.n;
+    const size_t N = (size_t)nk;
+    cudaStream_t s = c->stream;
+    double *stage = c->tmp;  // 9 n_k doubles
+    k_pack_state<<<nblk(c->n, kB), kB, 0, s>>>(c->n, slot, ih.id_base, nk, c->pinst, c->id, c->s0, stage);
+    c->launches += 1;
+    SIMP_CUDA(c, cudaGetLastError());
+    struct Out { double *dst; size_t off, len; } outs[] = {
+        {x, 0, 2 * N}, {vx, 2 * N, 2 * N}, {mass, 4 * N, N}, {rho, 5 * N, N},
+        {hsml, 6 * N, N}, {A, 7 * N, N}, {h, 8 * N, N}};
+    for (const Out &o : outs)
+        if (o.dst)
+            SIMP_CUDA(c, cudaMemcpyAsync(o.dst, stage + o.off, sizeof(double) * o.len, cudaMemcpyDeviceToHost, s));
+    Inst I{};
+    SIMP_CUDA(c, cudaMemcpyAsync(&I, c->inst_dev + slot, sizeof(Inst), cudaMemcpyDeviceToHost, s));
+    SIMP_CUDA(c, cudaStreamSynchronize(s));
+    if (t) *t = I.t;
     return SIMP_OK;
 }
 
-// One predictor-corrector step (time_integration.f90:263-390).
 // One predictor-corrector step (time_integration.f90:263-390).  With
 // profiling on, external event records between the kernels time each one.
 void enqueue_step(simp_ctx *c, bool diag, bool prof) {
@@ -312,10 +496,7 @@ void enqueue_step(simp_ctx *c, bool diag, bool prof) {
 int ensure_graph(simp_ctx *c, bool diag) {
     const bool prof = c->profile;
     if (c->step_graph && c->graph_diag == diag && c->graph_profiled == prof) return SIMP_OK;
-    if (c->step_graph) {
-        cudaGraphExecDestroy(c->step_graph);
-        c->step_graph = nullptr;
-    }
+    invalidate_graph(c);
     if (prof && !c->prof_ev[0])
         for (auto &e : c->prof_ev) SIMP_CUDA(c, cudaEventCreate(&e));
     cudaGraph_t g = nullptr;
@@ -334,34 +515,16 @@ int ensure_graph(simp_ctx *c, bool diag) {
     return SIMP_OK;
 }
 
-void invalidate_graph(simp_ctx *c) {
-    if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
-    c->step_graph = nullptr;
-}
-
-double disp_of(const Scalars &s) {
-    double d2;
-    std::memcpy(&d2, &s.dmax2_bits, sizeof(double));
-    return std::sqrt(std::max(0.0, d2));
-}
-
-// Re-sort when the device-side stencil would grow past one cell ring.
-bool wants_rebuild(const simp_ctx *c, const Scalars &s) {
-    return (s.hmax + s.skin + 2.0 * disp_of(s)) * c->grid.inv_cs > 0.98;
-}
-
-// Resize the grid when hsml grew 5% past the bound the grid was sized for
-// (sle = 2); until then the device-side stencil radius covers the growth.
-bool wants_regrid(const simp_ctx *c, const Scalars &s) { return s.hmax > 1.05 * c->grid_hmax; }
-
-int size_grid(simp_ctx *c, double xmin, double xmax, double ymin, double ymax, double hmax);
-int bin_walls(simp_ctx *c, int nb, const double *xb, const double *massb);
-int download2(simp_ctx *c, const double *a, const double *b, double *h2);
-
-// New grid from the current extents and hsml bound, then a full re-sort.
-int regrid(simp_ctx *c) {
-    TRY(read_scalars(c));
-    const double hmax = c->sc_host->hmax;
+// A single basin whose hsml grew 5% past the size its grid was built for
+// (sle = 2) gets a new grid; until then the stencil radius covers it.
+int maybe_regrid(simp_ctx *c, bool *done) {
+    *done = false;
+    if (c->max_inst != 1 || !c->insts[0].active || c->prm.sle != 2) return SIMP_OK;
+    InstHost &h = c->insts[0];
+    Inst I{};
+    TRY(read_inst(c, 0, &I));
+    if (!(I.hmax > 1.05 * h.grid_hmax)) return SIMP_OK;
+    *done = true;
     std::vector<double> xy(2 * (size_t)c->n);
     TRY(download2(c, c->s0.x, c->s0.y, xy.data()));
     double xmin = xy[0], xmax = xy[0], ymin = xy[1], ymax = xy[1];
@@ -371,21 +534,22 @@ int regrid(simp_ctx *c) {
         ymin = std::min(ymin, xy[2 * i + 1]);
         ymax = std::max(ymax, xy[2 * i + 1]);
     }
-    for (int b = 0; b < c->nb; ++b) {
-        xmin = std::min(xmin, c->host_xb[2 * b]);
-        xmax = std::max(xmax, c->host_xb[2 * b]);
-        ymin = std::min(ymin, c->host_xb[2 * b + 1]);
-        ymax = std::max(ymax, c->host_xb[2 * b + 1]);
+    for (int b = 0; b < h.nb; ++b) {
+        xmin = std::min(xmin, h.xb[2 * b]);
+        xmax = std::max(xmax, h.xb[2 * b]);
+        ymin = std::min(ymin, h.xb[2 * b + 1]);
+        ymax = std::max(ymax, h.xb[2 * b + 1]);
     }
-    invalidate_graph(c);
-    TRY(size_grid(c, xmin, xmax, ymin, ymax, hmax));
-    TRY(bin_walls(c, c->nb, c->host_xb.data(), c->host_massb.data()));
-    return rebuild(c);
+    size_inst_grid(c, h, xmin, xmax, ymin, ymax, I.hmax);
+    TRY(layout(c));
+    TRY(rebuild(c, mask_of(0), false, false));
+    h.steps_since_sort = 0;
+    return SIMP_OK;
 }
 
 int check_after(simp_ctx *c) {
     const Scalars &s = *c->sc_host;
-    if (s.flags & FLAG_NONFINITE)
+    if ((s.flags & FLAG_NONFINITE) && c->max_inst == 1)   // batches flag the basin instead
         return simp_fail(c, SIMP_ERR_NONFINITE, "non-finite particle state after a step");
     if (s.maxip > c->prm.max_ind_int)
         return simp_fail(c, SIMP_ERR_IND_INT,
@@ -395,11 +559,95 @@ int check_after(simp_ctx *c) {
     return SIMP_OK;
 }
 
+int create(const simp_params *params, int32_t maxn, int32_t maxnb, int32_t max_inst, simp_ctx **out) {
+    if (!out) return SIMP_ERR_BADARG;
+    *out = nullptr;
+    if (!params || maxn < 1 || maxnb < 0 || max_inst < 1 || max_inst > kMaxSlots) return SIMP_ERR_BADARG;
+    simp_ctx *c = new simp_ctx();
+    *out = c;   // on failure the caller can read last_error, then destroy
+    c->prm = *params;
+    TRY(check_params(c, c->prm, max_inst > 1));
+    c->maxn = maxn;
+    c->maxnb = std::max(maxnb, 1);
+    c->max_inst = max_inst;
+    c->id_stride = (max_inst > 1) ? (1 << kIdShift) : 0;
+    c->insts.assign(max_inst, InstHost{});
+    cudaGetDevice(&c->device);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return simp_fail(c, SIMP_ERR_CUDA, "cudaStreamCreate failed (no usable CUDA device?)");
+    const size_t M = (size_t)maxn, MB = (size_t)c->maxnb, MX = std::max(M, MB);
+    double **d1[] = {&c->s0.x, &c->s0.y, &c->s0.vx, &c->s0.vy, &c->s0.m, &c->s0.rho, &c->s0.mor, &c->s0.h,
+                     &c->s0.A, &c->s0.hs, &c->s1.x, &c->s1.y, &c->s1.vx, &c->s1.vy, &c->s1.rho,
+                     &c->s1.mor, &c->s1.h, &c->s1.A, &c->xr, &c->yr, &c->xl, &c->yl,
+                     &c->tau11, &c->tau12, &c->tau22, &c->div};
+    for (double **p : d1) TRY(dalloc(c, p, M));
+    if (c->prm.mass_from_area && c->prm.sle != 2) {
+        TRY(dalloc(c, &c->mass1, M));
+        c->s1.m = c->mass1;
+    } else {
+        c->s1.m = c->s0.m;
+    }
+    c->s1.hs = c->s0.hs;
+    float **f1[] = {&c->s0.xf, &c->s0.yf, &c->s0.hsf, &c->s1.xf, &c->s1.yf};
+    for (float **p : f1) TRY(dalloc(c, p, M));
+    c->s1.hsf = c->s0.hsf;
+    TRY(dalloc(c, &c->nbr, (size_t)kMaxNbr * M));
+    TRY(dalloc(c, &c->nbr_count, M));
+    TRY(dalloc(c, &c->nbr_tmp, (size_t)kMaxNbr * M));
+    TRY(dalloc(c, &c->pair_j, (size_t)kMaxPairs * M));
+    TRY(dalloc(c, &c->pair_count, M));
+    TRY(dalloc(c, &c->diag, 9 * M));
+    TRY(dalloc(c, &c->rates, 4 * M));
+    TRY(dalloc(c, &c->cell, M));
+    TRY(dalloc(c, &c->id, M));
+    TRY(dalloc(c, &c->pinst, M));
+    TRY(dalloc(c, &c->perm, M));
+    TRY(dalloc(c, &c->tmp, 14 * MX));
+    TRY(dalloc(c, &c->itmp, 5 * MX));
+    TRY(dalloc(c, &c->bx, MB));
+    TRY(dalloc(c, &c->by, MB));
+    TRY(dalloc(c, &c->bm, MB));
+    TRY(dalloc(c, &c->bid, MB));
+    TRY(dalloc(c, &c->binst, MB));
+    TRY(dalloc(c, &c->bcell, MB));
+    TRY(dalloc(c, &c->sc, 1));
+    TRY(dalloc(c, &c->pair_cnt, M + 1));
+    TRY(dalloc(c, &c->bpair_cnt, MB + 1));
+    TRY(dalloc(c, &c->inst_dev, (size_t)max_inst));
+    if (cudaMallocHost((void **)&c->sc_host, sizeof(Scalars)) != cudaSuccess)
+        return simp_fail(c, SIMP_ERR_NOMEM, "pinned host allocation failed");
+    std::memset(c->sc_host, 0, sizeof(Scalars));
+    SIMP_CUDA(c, cudaMemsetAsync(c->inst_dev, 0, sizeof(Inst) * (size_t)max_inst, c->stream));
+    // scalars of an empty context
+    Scalars &sc = *c->sc_host;
+    sc.dt = c->prm.dt;
+    const double inf = INFINITY;
+    std::memcpy(&sc.acc_hmin, &inf, sizeof(double));
+    std::memcpy(&sc.acc_dt, &inf, sizeof(double));
+    sc.minip = 0x7fffffff;
+    sc.list_scan = 1;
+    SIMP_CUDA(c, cudaMemcpyAsync(c->sc, c->sc_host, sizeof(Scalars), cudaMemcpyHostToDevice, c->stream));
+    TRY(layout(c));
+    return SIMP_OK;
+}
+
+simp_forcing forcing_of(const simp_params &p) {
+    simp_forcing f{};
+    f.wind_kind = p.wind_kind;
+    f.wind_u = p.wind_u;
+    f.wind_v = p.wind_v;
+    f.vortex_x = p.vortex_x;
+    f.vortex_y = p.vortex_y;
+    f.vortex_umax = p.vortex_umax;
+    f.vortex_radius = p.vortex_radius;
+    return f;
+}
+
 }  // namespace
 
 extern "C" {
 
-const char *simp_gpu_version(void) { return "simp_b200 0.1 (sm_100a)"; }
+const char *simp_gpu_version(void) { return "simp_b200 0.2 (sm_100a)"; }
 
 void simp_params_reference_default(simp_params *p) {
     if (!p) return;
@@ -449,66 +697,12 @@ void simp_params_reference_default(simp_params *p) {
 }
 
 int32_t simp_gpu_create(const simp_params *params, int32_t maxn, int32_t maxnb, simp_ctx **out) {
-    if (!out) return SIMP_ERR_BADARG;
-    *out = nullptr;
-    if (!params || maxn < 1 || maxnb < 0) return SIMP_ERR_BADARG;
-    simp_ctx *c = new simp_ctx();
-    c->prm = *params;
-    int rc = check_params(c, c->prm);
-    if (rc != SIMP_OK) {
-        *out = c;  // caller can read last_error, then destroy
-        return rc;
-    }
-    c->maxn = maxn;
-    c->maxnb = std::max(maxnb, 1);
-    cudaGetDevice(&c->device);
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
-        *out = c;
-        return simp_fail(c, SIMP_ERR_CUDA, "cudaStreamCreate failed (no usable CUDA device?)");
-    }
-    const size_t M = (size_t)maxn, MB = (size_t)c->maxnb, MX = std::max(M, MB);
-    double **d1[] = {&c->s0.x, &c->s0.y, &c->s0.vx, &c->s0.vy, &c->s0.m, &c->s0.rho, &c->s0.mor, &c->s0.h,
-                     &c->s0.A, &c->s0.hs, &c->s1.x, &c->s1.y, &c->s1.vx, &c->s1.vy, &c->s1.rho,
-                     &c->s1.mor, &c->s1.h, &c->s1.A, &c->xr, &c->yr, &c->xl, &c->yl,
-                     &c->tau11, &c->tau12, &c->tau22,
-                     &c->div};
-    for (double **p : d1) {
-        rc = dalloc(c, p, M);
-        if (rc) { *out = c; return rc; }
-    }
-    if (c->prm.mass_from_area && c->prm.sle != 2) {
-        rc = dalloc(c, &c->mass1, M);
-        if (rc) { *out = c; return rc; }
-        c->s1.m = c->mass1;
-    } else {
-        c->s1.m = c->s0.m;
-    }
-    c->s1.hs = c->s0.hs;
-    float **f1[] = {&c->s0.xf, &c->s0.yf, &c->s0.hsf, &c->s1.xf, &c->s1.yf};
-    for (float **p : f1) {
-        rc = dalloc(c, p, M);
-        if (rc) { *out = c; return rc; }
-    }
-    c->s1.hsf = c->s0.hsf;
-    if ((rc = dalloc(c, &c->nbr, (size_t)kMaxNbr * M)) || (rc = dalloc(c, &c->nbr_count, M)) ||
-        (rc = dalloc(c, &c->pair_j, (size_t)kMaxPairs * M)) || (rc = dalloc(c, &c->pair_count, M)) ||
-        (rc = dalloc(c, &c->diag, 9 * M)) || (rc = dalloc(c, &c->rates, 4 * M)) ||
-        (rc = dalloc(c, &c->cell, M)) || (rc = dalloc(c, &c->id, M)) || (rc = dalloc(c, &c->inv_id, M)) ||
-        (rc = dalloc(c, &c->perm, M)) || (rc = dalloc(c, &c->tmp, 12 * MX)) ||
-        (rc = dalloc(c, &c->itmp, 3 * MX)) || (rc = dalloc(c, &c->bx, MB)) || (rc = dalloc(c, &c->by, MB)) ||
-        (rc = dalloc(c, &c->bm, MB)) || (rc = dalloc(c, &c->bid, MB)) || (rc = dalloc(c, &c->bcell, MB)) ||
-        (rc = dalloc(c, &c->sc, 1)) || (rc = dalloc(c, &c->pair_cnt, M + 1)) ||
-        (rc = dalloc(c, &c->bpair_cnt, MB + 1))) {
-        *out = c;
-        return rc;
-    }
-    if (cudaMallocHost((void **)&c->sc_host, sizeof(Scalars) * (1 + kSnapRing)) != cudaSuccess) {
-        *out = c;
-        return simp_fail(c, SIMP_ERR_NOMEM, "pinned host allocation failed");
-    }
-    std::memset(c->sc_host, 0, sizeof(Scalars) * (1 + kSnapRing));
-    *out = c;
-    return SIMP_OK;
+    return create(params, maxn, maxnb, 1, out);
+}
+
+int32_t simp_gpu_create_batch(const simp_params *params, int32_t maxn, int32_t maxnb, int32_t max_instances,
+                              simp_ctx **out) {
+    return create(params, maxn, maxnb, max_instances, out);
 }
 
 int32_t simp_gpu_destroy(simp_ctx *c) {
@@ -525,9 +719,7 @@ int32_t simp_gpu_set_state(simp_ctx *c, int32_t ntotal, const double *x, const d
                            const double *massb, double dt, double current_time) {
     if (!c) return SIMP_ERR_BADARG;
     if (!c->stream) return simp_fail(c, SIMP_ERR_STATE, "context was not created successfully");
-    if (ntotal < 1 || ntotalb < 0 || !x || !vx || !mass || !rho || !hsml || !A || !h ||
-        (ntotalb > 0 && (!xb || !massb)))
-        return simp_fail(c, SIMP_ERR_BADARG, "set_state: bad sizes or null arrays");
+    if (c->max_inst != 1) return simp_fail(c, SIMP_ERR_BADARG, "set_state is for single-basin contexts; use simp_gpu_batch_add");
     if (ntotal > c->maxn)
         return simp_fail(c, SIMP_ERR_MAXN,
                          "Resolution desired too high, the number of particles generated is higher "
@@ -536,101 +728,97 @@ int32_t simp_gpu_set_state(simp_ctx *c, int32_t ntotal, const double *x, const d
         return simp_fail(c, SIMP_ERR_MAXN,
                          "The number of boundary particles generated is higher than the maximum "
                          "allowed. (boundaries.f90:296-303)");
-    invalidate_graph(c);
-    const int n = ntotal;
-    c->n = n;
-    c->nb = ntotalb;
-    cudaStream_t s = c->stream;
-    // extents and hsml bounds (host)
-    double xmin = x[0], xmax = x[0], ymin = x[1], ymax = x[1], hmin = hsml[0], hmax = hsml[0];
-    for (int i = 0; i < n; ++i) {
-        xmin = std::min(xmin, x[2 * i]);
-        xmax = std::max(xmax, x[2 * i]);
-        ymin = std::min(ymin, x[2 * i + 1]);
-        ymax = std::max(ymax, x[2 * i + 1]);
-        hmin = std::min(hmin, hsml[i]);
-        hmax = std::max(hmax, hsml[i]);
-        if (!(hsml[i] > 0.0) || !(rho[i] > 0.0) || !(h[i] > 0.0))
-            return simp_fail(c, SIMP_ERR_BADARG, "set_state: hsml, rho and h must be positive");
-    }
-    for (int b = 0; b < ntotalb; ++b) {
-        xmin = std::min(xmin, xb[2 * b]);
-        xmax = std::max(xmax, xb[2 * b]);
-        ymin = std::min(ymin, xb[2 * b + 1]);
-        ymax = std::max(ymax, xb[2 * b + 1]);
-    }
-    if (!std::isfinite(xmin + xmax + ymin + ymax))
-        return simp_fail(c, SIMP_ERR_BADARG, "set_state: non-finite positions");
+    if (ntotal < 1) return simp_fail(c, SIMP_ERR_BADARG, "set_state: bad sizes or null arrays");
+    double hmax = hsml[0];
+    for (int i = 0; i < ntotal; ++i) hmax = std::max(hmax, hsml[i]);
     const double max_hsml = (c->prm.max_hsml > 0.0) ? c->prm.max_hsml : hmax * 10.0;  // initialize.f90:191
     c->phys = make_phys(c->prm, max_hsml);
-    TRY(size_grid(c, xmin, xmax, ymin, ymax, hmax));
-    // particle arrays (original order)
-    TRY(upload_interleaved(c, x, c->s0.x, c->s0.y, n, c->tmp));
-    TRY(upload_interleaved(c, vx, c->s0.vx, c->s0.vy, n, c->tmp + 2 * (size_t)n));
-    SIMP_CUDA(c, cudaMemcpyAsync(c->s0.m, mass, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-    SIMP_CUDA(c, cudaMemcpyAsync(c->s0.rho, rho, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-    SIMP_CUDA(c, cudaMemcpyAsync(c->s0.hs, hsml, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-    SIMP_CUDA(c, cudaMemcpyAsync(c->s0.A, A, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-    SIMP_CUDA(c, cudaMemcpyAsync(c->s0.h, h, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-    k_init_ids<<<nblk(n, kB), kB, 0, s>>>(n, c->id, c->s0.m, c->s0.rho, c->s0.mor);
-    c->launches += 1;
-    SIMP_CUDA(c, cudaGetLastError());
-    c->host_xb.assign(xb, xb + 2 * (size_t)ntotalb);
-    c->host_massb.assign(massb, massb + ntotalb);
-    TRY(bin_walls(c, ntotalb, xb, massb));
-    // scalars
-    Scalars sc{};
+    reset_all(c);
+    // global scalars of the run
+    Scalars &sc = *c->sc_host;
+    std::memset(&sc, 0, sizeof(Scalars));
     sc.dt = dt;
     sc.t = current_time;
+    double hmin = hsml[0];
+    for (int i = 0; i < ntotal; ++i) hmin = std::min(hmin, hsml[i]);
     sc.hmin = hmin;
     sc.hmax = hmax;
     sc.bs = 2.0 * hmin;
-    sc.dmax2_bits = 0ull;
-    {
-        // bound on |coordinate| for the FP32 prefilter (grows on the device)
-        const double xa = std::max(std::max(std::fabs(xmin), std::fabs(xmax)),
-                                   std::max(std::fabs(ymin), std::fabs(ymax)));
-        std::memcpy(&sc.xabs_bits, &xa, sizeof(double));
-    }
-    {
-        const double inf = INFINITY;
-        std::memcpy(&sc.acc_hmin, &inf, sizeof(double));
-        std::memcpy(&sc.acc_dt, &inf, sizeof(double));
-    }
-    sc.acc_hmax = 0ull;
+    const double inf = INFINITY;
+    std::memcpy(&sc.acc_hmin, &inf, sizeof(double));
+    std::memcpy(&sc.acc_dt, &inf, sizeof(double));
     sc.minip = 0x7fffffff;
     sc.skin = list_skin(c, hmax);
-    sc.dlist2_bits = 0ull;
     sc.list_scan = 1;
-    sc.blocks_done = 0u;
-    *c->sc_host = sc;
-    SIMP_CUDA(c, cudaMemcpyAsync(c->sc, c->sc_host, sizeof(Scalars), cudaMemcpyHostToDevice, s));
-    TRY(rebuild(c));
-    SIMP_CUDA(c, cudaStreamSynchronize(s));
+    SIMP_CUDA(c, cudaMemcpyAsync(c->sc, c->sc_host, sizeof(Scalars), cudaMemcpyHostToDevice, c->stream));
+    SIMP_CUDA(c, cudaMemsetAsync(c->inst_dev, 0, sizeof(Inst), c->stream));
+    c->have_state = false;
+    TRY(add_instance(c, 0, forcing_of(c->prm), ntotal, x, vx, mass, rho, hsml, A, h, ntotalb, xb, massb,
+                     current_time));
     c->have_state = true;
+    return SIMP_OK;
+}
+
+int32_t simp_gpu_batch_add(simp_ctx *c, const simp_forcing *forcing, int32_t ntotal, const double *x,
+                           const double *vx, const double *mass, const double *rho, const double *hsml,
+                           const double *A, const double *h, int32_t ntotalb, const double *xb,
+                           const double *massb, int32_t *slot) {
+    if (!c || !forcing || !slot) return SIMP_ERR_BADARG;
+    if (!c->stream) return simp_fail(c, SIMP_ERR_STATE, "context was not created successfully");
+    int q = -1;
+    for (int k = 0; k < c->max_inst; ++k)
+        if (!c->insts[k].active) { q = k; break; }
+    if (q < 0) return simp_fail(c, SIMP_ERR_MAXN, "no free slot in the batch");
+    if (!c->have_state) {
+        // first basin: physics constants and the list skin
+        double hmax = 0.0;
+        for (int i = 0; i < ntotal && hsml; ++i) hmax = std::max(hmax, hsml[i]);
+        c->phys = make_phys(c->prm, c->prm.max_hsml > 0.0 ? c->prm.max_hsml : 10.0 * hmax);
+        TRY(read_scalars(c));
+        c->sc_host->skin = list_skin(c, hmax);
+        c->sc_host->dt = c->prm.dt;
+        SIMP_CUDA(c, cudaMemcpyAsync(c->sc, c->sc_host, sizeof(Scalars), cudaMemcpyHostToDevice, c->stream));
+    }
+    TRY(add_instance(c, q, *forcing, ntotal, x, vx, mass, rho, hsml, A, h, ntotalb, xb, massb, 0.0));
+    c->have_state = true;
+    *slot = q;
+    return SIMP_OK;
+}
+
+int32_t simp_gpu_batch_remove(simp_ctx *c, int32_t slot) {
+    if (!c || slot < 0 || slot >= c->max_inst) return SIMP_ERR_BADARG;
+    return remove_instance(c, slot);
+}
+
+int32_t simp_gpu_batch_get_state(simp_ctx *c, int32_t slot, double *x, double *vx, double *mass, double *rho,
+                                 double *hsml, double *A, double *h, double *current_time) {
+    if (!c || slot < 0 || slot >= c->max_inst) return SIMP_ERR_BADARG;
+    if (!c->insts[slot].active) return simp_fail(c, SIMP_ERR_BADARG, "slot is free");
+    return get_instance_state(c, slot, x, vx, mass, rho, hsml, A, h, current_time);
+}
+
+int32_t simp_gpu_batch_info(simp_ctx *c, int32_t slot, int32_t *ntotal, int64_t *steps, int32_t *flags) {
+    if (!c || slot < 0 || slot >= c->max_inst) return SIMP_ERR_BADARG;
+    const InstHost &h = c->insts[slot];
+    if (ntotal) *ntotal = h.active ? h.n : 0;
+    if (steps) *steps = h.steps_done;
+    if (flags) {
+        *flags = 0;
+        if (h.active) {
+            Inst I{};
+            TRY(read_inst(c, slot, &I));
+            *flags = I.flags;
+        }
+    }
     return SIMP_OK;
 }
 
 int32_t simp_gpu_get_state(simp_ctx *c, double *x, double *vx, double *mass, double *rho,
                            double *hsml, double *A, double *h, double *dt, double *current_time) {
     if (!c) return SIMP_ERR_BADARG;
-    if (!c->have_state) return simp_fail(c, SIMP_ERR_STATE, "get_state before set_state");
-    const int n = c->n;
-    const size_t N = (size_t)n;
-    cudaStream_t s = c->stream;
-    double *stage = c->tmp;  // 9 n doubles
-    k_pack_state<<<nblk(n, kB), kB, 0, s>>>(n, c->id, c->s0, stage);
-    c->launches += 1;
-    SIMP_CUDA(c, cudaGetLastError());
-    struct Out { double *dst; size_t off, len; } outs[] = {
-        {x, 0, 2 * N}, {vx, 2 * N, 2 * N}, {mass, 4 * N, N}, {rho, 5 * N, N},
-        {hsml, 6 * N, N}, {A, 7 * N, N}, {h, 8 * N, N}};
-    for (const Out &o : outs)
-        if (o.dst)
-            SIMP_CUDA(c, cudaMemcpyAsync(o.dst, stage + o.off, sizeof(double) * o.len,
-                                         cudaMemcpyDeviceToHost, s));
-    SIMP_CUDA(c, cudaMemcpyAsync(c->sc_host, c->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, s));
-    SIMP_CUDA(c, cudaStreamSynchronize(s));
+    if (!c->have_state || !c->insts[0].active) return simp_fail(c, SIMP_ERR_STATE, "get_state before set_state");
+    TRY(get_instance_state(c, 0, x, vx, mass, rho, hsml, A, h, nullptr));
+    TRY(read_scalars(c));
     if (dt) *dt = c->sc_host->dt;
     if (current_time) *current_time = c->sc_host->t;
     return SIMP_OK;
@@ -645,7 +833,7 @@ int32_t simp_gpu_keep_diag(simp_ctx *c, int32_t keep) {
 int32_t simp_gpu_get_diag(simp_ctx *c, double *eps11, double *eps12, double *eps22, double *zeta,
                           double *eta, double *p, double *sig11, double *sig12, double *sig22) {
     if (!c) return SIMP_ERR_BADARG;
-    if (!c->have_state) return simp_fail(c, SIMP_ERR_STATE, "get_diag before set_state");
+    if (!c->have_state || c->max_inst != 1) return simp_fail(c, SIMP_ERR_STATE, "get_diag needs a single basin with state");
     double *outs[9] = {eps11, eps12, eps22, zeta, eta, p, sig11, sig12, sig22};
     for (int k = 0; k < 9; ++k)
         if (outs[k]) TRY(download1(c, c->diag + (size_t)k * c->maxn, outs[k]));
@@ -656,7 +844,7 @@ int32_t simp_gpu_nnps(simp_ctx *c, int32_t *nip, int32_t *p_i, int32_t *p_j, dou
                       double *hsml_ij, int32_t cap, int32_t *bnip, int32_t *bp_i, int32_t *bp_j,
                       double *br_ij, int32_t bcap) {
     if (!c) return SIMP_ERR_BADARG;
-    if (!c->have_state) return simp_fail(c, SIMP_ERR_STATE, "nnps before set_state");
+    if (!c->have_state || c->max_inst != 1) return simp_fail(c, SIMP_ERR_STATE, "nnps needs a single basin with state");
     return export_pairs(c, nip, p_i, p_j, r_ij, hsml_ij, cap, bnip, bp_i, bp_j, br_ij, bcap);
 }
 
@@ -675,14 +863,15 @@ int32_t simp_gpu_interaction_stats(simp_ctx *c, int32_t *maxip, int32_t *minip, 
 int32_t simp_gpu_single_step(simp_ctx *c, double current_time, double *dxdt, double *dvxdt,
                              double *dhdt, double *dAdt) {
     if (!c) return SIMP_ERR_BADARG;
-    if (!c->have_state) return simp_fail(c, SIMP_ERR_STATE, "single_step before set_state");
+    if (!c->have_state || c->max_inst != 1) return simp_fail(c, SIMP_ERR_STATE, "single_step needs a single basin with state");
     cudaStream_t s = c->stream;
-    k_set_time<<<1, 1, 0, s>>>(c->sc, current_time);
+    k_set_time0<<<1, 1, 0, s>>>(c->sc, c->inst_dev, current_time);
     c->launches += 1;
     launch_reset_stats(c);
     launch_kinematic(c, c->s0, true);
     launch_stress(c, c->s0, c->s0, EPI_RATES);
     SIMP_CUDA(c, cudaGetLastError());
+    c->lists_valid = true;
     const size_t M = (size_t)c->maxn;
     if (dxdt) TRY(download2(c, c->s0.vx, c->s0.vy, dxdt));
     if (dvxdt) TRY(download2(c, c->rates, c->rates + M, dvxdt));
@@ -694,7 +883,7 @@ int32_t simp_gpu_single_step(simp_ctx *c, double current_time, double *dxdt, dou
 
 int32_t simp_gpu_sum_density(simp_ctx *c, double *rho_out) {
     if (!c || !rho_out) return SIMP_ERR_BADARG;
-    if (!c->have_state) return simp_fail(c, SIMP_ERR_STATE, "sum_density before set_state");
+    if (!c->have_state || c->max_inst != 1) return simp_fail(c, SIMP_ERR_STATE, "sum_density needs a single basin with state");
     double *stage = c->tmp;
     TRY(sum_density(c, stage));
     SIMP_CUDA(c, cudaMemcpyAsync(rho_out, stage, sizeof(double) * c->n, cudaMemcpyDeviceToHost, c->stream));
@@ -702,52 +891,51 @@ int32_t simp_gpu_sum_density(simp_ctx *c, double *rho_out) {
     return SIMP_OK;
 }
 
+// time_integration.f90:146-181 for nsteps iterations of every basin.  Each
+// basin is re-sorted into its grid every kSortEvery of its own steps; in
+// between the device-side stencil radius keeps the cell list exact.
 int32_t simp_gpu_step(simp_ctx *c, int32_t nsteps, double *current_time, double *dt) {
     if (!c || nsteps < 0) return SIMP_ERR_BADARG;
     if (!c->have_state) return simp_fail(c, SIMP_ERR_STATE, "step before set_state");
     cudaStream_t s = c->stream;
-    // bounds read at the end of the previous call (or by set_state)
-    if (wants_regrid(c, *c->sc_host)) TRY(regrid(c));
-    else if (wants_rebuild(c, *c->sc_host)) TRY(rebuild(c));
+    if (c->n == 0) {   // an empty batch
+        if (current_time) *current_time = 0.0;
+        if (dt) *dt = c->prm.dt;
+        return SIMP_OK;
+    }
+    bool regridded = false;
+    TRY(maybe_regrid(c, &regridded));
     launch_reset_stats(c);
     TRY(ensure_graph(c, c->keep_diag));
-    // The cell list stays exact between sorts (the stencil radius adapts on
-    // the device); the host re-sorts when a recent snapshot of the bounds says
-    // the stencil would outgrow one ring of cells.  Snapshots are read without
-    // stalling the device: the host runs at most kLag steps ahead.
-    constexpr int kLag = kSnapRing - 1;
-    cudaEvent_t ev[kSnapRing];
-    for (int k = 0; k < kSnapRing; ++k) cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming);
-    int rc = SIMP_OK;
-    int quiet = 0;  // steps to skip checks after a sort (older snapshots predate it)
-    for (int st = 0; st < nsteps && rc == SIMP_OK; ++st) {
-        if (st >= kLag) {
-            const int slot = (st - kLag) % kSnapRing;
-            cudaEventSynchronize(ev[slot]);
-            if (quiet > 0) {
-                --quiet;
-            } else if (wants_regrid(c, c->sc_host[1 + slot])) {
-                rc = regrid(c);
-                if (rc != SIMP_OK) break;
-                rc = ensure_graph(c, c->keep_diag);
-                if (rc != SIMP_OK) break;
-                quiet = kLag;
-            } else if (wants_rebuild(c, c->sc_host[1 + slot])) {
-                rc = rebuild(c);
-                if (rc != SIMP_OK) break;
-                quiet = kLag;
+    for (int st = 0; st < nsteps; ++st) {
+        DueMask due{};
+        bool any = false;
+        for (int q = 0; q < c->max_inst; ++q) {
+            InstHost &h = c->insts[q];
+            if (h.active && h.steps_since_sort >= kSortEvery) {
+                due.w[q >> 6] |= 1ull << (q & 63);
+                h.steps_since_sort = 0;
+                any = true;
             }
         }
+        if (any) {
+            TRY(maybe_regrid(c, &regridded));   // hsml grew past the grid (sle = 2)
+            if (regridded) TRY(ensure_graph(c, c->keep_diag));
+            else TRY(rebuild(c, due, false, false));
+        }
         cudaError_t e = cudaGraphLaunch(c->step_graph, s);
-        if (e != cudaSuccess) { rc = simp_cuda_check(c, e, "cudaGraphLaunch"); break; }
+        if (e != cudaSuccess) return simp_cuda_check(c, e, "cudaGraphLaunch");
         c->launches += c->graph_kernels;
-        cudaMemcpyAsync(&c->sc_host[1 + st % kSnapRing], c->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, s);
-        cudaEventRecord(ev[st % kSnapRing], s);
-        c->steps_since_rebuild++;
+        c->lists_valid = true;
+        for (InstHost &h : c->insts)
+            if (h.active) {
+                ++h.steps_since_sort;
+                ++h.steps_done;
+            }
         if (c->graph_profiled) {
             // timing mode: wait for this step and add up its kernel times
             e = cudaEventSynchronize(c->prof_ev[simp_ctx::kProfKernels]);
-            if (e != cudaSuccess) { rc = simp_cuda_check(c, e, "profile event"); break; }
+            if (e != cudaSuccess) return simp_cuda_check(c, e, "profile event");
             for (int k = 0; k < simp_ctx::kProfKernels; ++k) {
                 float ms = 0.0f;
                 cudaEventElapsedTime(&ms, c->prof_ev[k], c->prof_ev[k + 1]);
@@ -756,10 +944,7 @@ int32_t simp_gpu_step(simp_ctx *c, int32_t nsteps, double *current_time, double 
             c->prof_steps += 1;
         }
     }
-    cudaError_t e = cudaStreamSynchronize(s);
-    for (int k = 0; k < kSnapRing; ++k) cudaEventDestroy(ev[k]);
-    if (rc != SIMP_OK) return rc;
-    if (e != cudaSuccess) return simp_cuda_check(c, e, "simp_gpu_step");
+    SIMP_CUDA(c, cudaStreamSynchronize(s));
     TRY(read_scalars(c));
     if (current_time) *current_time = c->sc_host->t;
     if (dt) *dt = c->sc_host->dt;

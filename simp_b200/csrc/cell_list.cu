@@ -121,15 +121,43 @@ __global__ void scan_total(const int *__restrict__ in, int n, int *__restrict__ 
     out[n] = (n > 0) ? out[n - 1] + in[n - 1] : 0;
 }
 
-__global__ void k_keys(int n, const double *__restrict__ x, const double *__restrict__ y,
-                       Grid g, int *__restrict__ key, int *__restrict__ cnt) {
+// Cell key of each particle from its sort position and its instance's grid;
+// particles being removed (instance -1) go to the dump key after all cells.
+__global__ void k_keys(int n, const double *__restrict__ xr, const double *__restrict__ yr,
+                       const int *__restrict__ pinst, const Inst *__restrict__ inst, int dump_key,
+                       int *__restrict__ key, int *__restrict__ cnt) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const int cx = clampi((int)floor((x[i] - g.x0) * g.inv_cs), 0, g.ncx - 1);
-    const int cy = clampi((int)floor((y[i] - g.y0) * g.inv_cs), 0, g.ncy - 1);
-    const int k = cy * g.ncx + cx;
+    const int q = pinst[i];
+    int k = dump_key;
+    if (q >= 0) {
+        const Inst &I = inst[q];
+        const int cx = clampi((int)floor((xr[i] - I.x0) * I.inv_cs), 0, I.ncx - 1);
+        const int cy = clampi((int)floor((yr[i] - I.y0) * I.inv_cs), 0, I.ncy - 1);
+        k = I.base + cy * I.ncx + cx;
+    }
     key[i] = k;
     atomicAdd(&cnt[k], 1);
+}
+
+// Instances due for a re-sort take their current positions as sort
+// positions; a basin flagged non-finite keeps its old (finite) ones.
+__global__ void k_refresh_sortpos(int n, const int *__restrict__ pinst, DueMask due, const Inst *__restrict__ inst,
+                                  const double *__restrict__ x, const double *__restrict__ y,
+                                  double *__restrict__ xr, double *__restrict__ yr) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int q = pinst[i];
+    if (q < 0 || !((due.w[q >> 6] >> (q & 63)) & 1ull)) return;
+    if (inst[q].flags & FLAG_NONFINITE) return;
+    xr[i] = x[i];
+    yr[i] = y[i];
+}
+
+__global__ void k_reset_inst_disp(Inst *inst, int ninst, DueMask due) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= ninst) return;
+    if ((due.w[q >> 6] >> (q & 63)) & 1ull) inst[q].dmax2_bits = 0ull;
 }
 
 __global__ void k_scatter(int n, const int *__restrict__ key, const int *__restrict__ start,
@@ -157,41 +185,113 @@ __global__ void k_cell_sort(int ncells, const int *__restrict__ start, int *__re
     }
 }
 
+constexpr int kGathered = 12;
 struct Gather {
-    const double *src[10];
-    double *dst[10];
+    const double *src[kGathered];
+    double *dst[kGathered];
 };
 
-__global__ void k_gather(int n, const int *__restrict__ perm, Gather gd, int narr,
-                         const int *__restrict__ key, int *__restrict__ cell_out,
-                         const int *__restrict__ id_in, int *__restrict__ id_out) {
+__device__ __forceinline__ bool is_due(const DueMask &m, int q) {
+    return q >= 0 && ((m.w[q >> 6] >> (q & 63)) & 1ull);
+}
+
+// Positions of the new order whose particle may differ from the old one: all
+// of them after an admission or a removal (instance ranges shift), else only
+// those of the due instances (every instance keeps its range of positions,
+// and the others keep their order).
+__device__ __forceinline__ bool moves(int all, const DueMask &due, const int *pinst, int k) {
+    return all || is_due(due, pinst[k]);
+}
+
+// New order into scratch; inv[old] = new for every moved particle.
+__global__ void k_gather(int kept, int all, DueMask due, const int *__restrict__ perm, Gather gd,
+                         const int *__restrict__ key, int *__restrict__ cell_out, const int *__restrict__ id_in,
+                         int *__restrict__ id_out, const int *__restrict__ pinst_in, int *__restrict__ pinst_out,
+                         int *__restrict__ inv) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
+    if (k >= kept || !moves(all, due, pinst_in, k)) return;
     const int o = perm[k];
-    for (int a = 0; a < narr; ++a) gd.dst[a][k] = gd.src[a][o];
+#pragma unroll
+    for (int a = 0; a < kGathered; ++a) gd.dst[a][k] = gd.src[a][o];
     cell_out[k] = key[o];
     id_out[k] = id_in[o];
+    pinst_out[k] = pinst_in[o];
+    inv[o] = k;
 }
 
-// Rebuild-time positions, inverse index and the FP32 copies of the sorted state.
-__global__ void k_finish_rebuild(int n, State s, double *__restrict__ xr, double *__restrict__ yr,
-                                 const int *__restrict__ id, int *__restrict__ inv_id) {
+// Verlet-list rows of the moved particles: each entry renamed to the new
+// index and the row re-sorted, so a row lists its members in increasing
+// index order exactly as a fresh scan of the cell stencil would.  An entry
+// whose new index cannot be confirmed (perm[inv[v]] != v) turns the row into
+// an overflowed one, which the kinematic pass answers by a stencil scan.
+__global__ void k_remap_lists(int kept, int all, DueMask due, const int *__restrict__ pinst,
+                              const int *__restrict__ perm, const int *__restrict__ inv, int n_old,
+                              NbrList nl, int *__restrict__ nbr_out, int *__restrict__ cnt_out,
+                              double *__restrict__ xl_out, double *__restrict__ yl_out) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    const double x = s.x[k], y = s.y[k];
-    xr[k] = x;
-    yr[k] = y;
-    s.xf[k] = (float)x;
-    s.yf[k] = (float)y;
-    s.hsf[k] = (float)s.hs[k];
-    inv_id[id[k]] = k;
+    if (k >= kept || !moves(all, due, pinst, k)) return;
+    const int o = perm[k];
+    int cnt = nl.count[o];
+    xl_out[k] = nl.xl[o];
+    yl_out[k] = nl.yl[o];
+    if (cnt >= 0 && cnt <= kMaxNbr) {
+        int row[kMaxNbr];
+        for (int e = 0; e < cnt; ++e) {
+            const int v = nl.nbr[(size_t)e * nl.stride + o];
+            int w = -1;
+            if (v >= 0 && v < n_old) {
+                w = inv[v];
+                if (w < 0 || w >= kept || perm[w] != v) w = -1;
+            }
+            if (w < 0) { cnt = kMaxNbr + 1; break; }
+            int j = e - 1;
+            while (j >= 0 && row[j] > w) { row[j + 1] = row[j]; --j; }
+            row[j + 1] = w;
+        }
+        if (cnt <= kMaxNbr)
+            for (int e = 0; e < cnt; ++e) nbr_out[(size_t)e * nl.stride + k] = row[e];
+    } else {
+        cnt = kMaxNbr + 1;
+    }
+    cnt_out[k] = cnt;
 }
 
-// After a sort the cell-order indices in the Verlet lists are stale.
-__global__ void k_reset_disp(Scalars *sc) {
+__global__ void k_put_back_lists(int kept, int all, DueMask due, const int *__restrict__ pinst, NbrList nl,
+                                 const int *__restrict__ nbr_in, const int *__restrict__ cnt_in,
+                                 const double *__restrict__ xl_in, const double *__restrict__ yl_in) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= kept || !moves(all, due, pinst, k)) return;
+    const int cnt = cnt_in[k];
+    nl.count[k] = cnt;
+    nl.xl[k] = xl_in[k];
+    nl.yl[k] = yl_in[k];
+    if (cnt <= kMaxNbr)
+        for (int e = 0; e < cnt; ++e) nl.nbr[(size_t)e * nl.stride + k] = nbr_in[(size_t)e * nl.stride + k];
+}
+
+// Scratch back into the state arrays (pointers stay fixed so the captured
+// step graph remains valid), with the FP32 copies of the moved particles.
+__global__ void k_put_back(int kept, int all, DueMask due, Gather gd, State s, const int *__restrict__ id_new,
+                           int *__restrict__ id, const int *__restrict__ pinst_new, int *__restrict__ pinst) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= kept || !moves(all, due, pinst, k)) return;
+#pragma unroll
+    for (int a = 0; a < kGathered; ++a) const_cast<double *>(gd.src[a])[k] = gd.dst[a][k];
+    id[k] = id_new[k];
+    pinst[k] = pinst_new[k];
+    s.xf[k] = (float)s.x[k];
+    s.yf[k] = (float)s.y[k];
+    s.hsf[k] = (float)s.hs[k];
+}
+
+// After a sort: displacement since the sort restarts; the Verlet lists are
+// rebuilt by the next kinematic pass unless they were renamed.
+__global__ void k_reset_disp(Scalars *sc, int lists_kept) {
     sc->dmax2_bits = 0ull;
-    sc->dlist2_bits = 0ull;
-    sc->list_scan = 1;
+    if (!lists_kept) {
+        sc->dlist2_bits = 0ull;
+        sc->list_scan = 1;
+    }
 }
 
 inline int nblk(long long n, int b) { return (int)((n + b - 1) / b); }
@@ -213,35 +313,73 @@ void launch_scan_i32(const int *in, int *out, int n, void *tmp, cudaStream_t s) 
     scan_total<<<1, 1, 0, s>>>(in, n, out);
 }
 
-int rebuild(simp_ctx *c) {
+// Sorts the particles into cell order (instance-major keys, within a cell by
+// global id).  Instances in `due` re-bin at their current positions; the
+// others keep their sort positions, so their order does not change.  With
+// `full` (after an admission or a removal) every position is rewritten;
+// otherwise only the due instances' ranges move.  Particles of removed
+// instances (instance -1) end up after all others and are dropped: c->n
+// shrinks to the kept count.  The Verlet lists follow the particles unless
+// `new_lists` (or no list was built yet), in which case the next kinematic
+// pass rebuilds them.
+int rebuild(simp_ctx *c, const DueMask &due, bool full, bool new_lists) {
     const int n = c->n;
-    const Grid &g = c->grid;
-    const int ncells = g.ncx * g.ncy;
     cudaStream_t s = c->stream;
     const int B = 256;
-    int *key = c->itmp;                 // n ints
-    int *id_new = c->itmp + c->maxn;    // n ints
-    SIMP_CUDA(c, cudaMemsetAsync(c->cnt, 0, sizeof(int) * (size_t)ncells, s));
-    k_keys<<<nblk(n, B), B, 0, s>>>(n, c->s0.x, c->s0.y, g, key, c->cnt);
-    launch_scan_i32(c->cnt, c->cell_start, ncells, c->scan_tmp, s);
-    k_scatter<<<nblk(n, B), B, 0, s>>>(n, key, c->cell_start, c->cnt, c->perm);
-    k_cell_sort<<<nblk(ncells, 128), 128, 0, s>>>(ncells, c->cell_start, c->perm, c->id);
-    // gather state into scratch, then copy back (pointers stay fixed so the
-    // captured step graph remains valid)
-    double *srcs[10] = {c->s0.x, c->s0.y, c->s0.vx, c->s0.vy, c->s0.m,
-                        c->s0.rho, c->s0.mor, c->s0.h, c->s0.A, c->s0.hs};
-    Gather gd;
-    for (int a = 0; a < 10; ++a) { gd.src[a] = srcs[a]; gd.dst[a] = c->tmp + (size_t)a * c->maxn; }
-    k_gather<<<nblk(n, B), B, 0, s>>>(n, c->perm, gd, 10, key, c->cell, c->id, id_new);
-    for (int a = 0; a < 10; ++a)
-        SIMP_CUDA(c, cudaMemcpyAsync(srcs[a], gd.dst[a], sizeof(double) * (size_t)n,
-                                     cudaMemcpyDeviceToDevice, s));
-    SIMP_CUDA(c, cudaMemcpyAsync(c->id, id_new, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, s));
-    k_finish_rebuild<<<nblk(n, B), B, 0, s>>>(n, c->s0, c->xr, c->yr, c->id, c->inv_id);
-    k_reset_disp<<<1, 1, 0, s>>>(c->sc);
-    c->launches += 7 + kScanKernels;
+    const int nkeys = c->total_cells + 1;   // + the dump key
+    const size_t MX = (size_t)std::max(c->maxn, c->maxnb);
+    int *key = c->itmp;
+    int *id_new = c->itmp + MX;
+    int *pinst_new = c->itmp + 2 * MX;
+    int *inv = c->itmp + 3 * MX;
+    int *cnt_new = c->itmp + 4 * MX;
+    int kept = 0;
+    for (const InstHost &h : c->insts)
+        if (h.active) kept += h.n;
+    const bool keep_lists = c->lists_valid && !new_lists;
+    const int all = full ? 1 : 0;
+    if (n > 0) {
+        k_refresh_sortpos<<<nblk(n, B), B, 0, s>>>(n, c->pinst, due, c->inst_dev, c->s0.x, c->s0.y, c->xr, c->yr);
+        k_reset_inst_disp<<<nblk(c->ninst, 128), 128, 0, s>>>(c->inst_dev, c->ninst, due);
+        SIMP_CUDA(c, cudaMemsetAsync(c->cnt, 0, sizeof(int) * (size_t)nkeys, s));
+        k_keys<<<nblk(n, B), B, 0, s>>>(n, c->xr, c->yr, c->pinst, c->inst_dev, c->total_cells, key, c->cnt);
+        launch_scan_i32(c->cnt, c->cell_start, nkeys, c->scan_tmp, s);
+        k_scatter<<<nblk(n, B), B, 0, s>>>(n, key, c->cell_start, c->cnt, c->perm);
+        // (the dump key is not ordered: its particles are dropped)
+        if (c->total_cells > 0)
+            k_cell_sort<<<nblk(c->total_cells, 128), 128, 0, s>>>(c->total_cells, c->cell_start, c->perm, c->id);
+        double *srcs[kGathered] = {c->s0.x, c->s0.y, c->s0.vx, c->s0.vy, c->s0.m, c->s0.rho,
+                                   c->s0.mor, c->s0.h, c->s0.A, c->s0.hs, c->xr, c->yr};
+        Gather gd;
+        for (int a = 0; a < kGathered; ++a) {
+            gd.src[a] = srcs[a];
+            gd.dst[a] = c->tmp + (size_t)a * MX;
+        }
+        c->launches += 7 + kScanKernels;
+        if (kept > 0) {
+            k_gather<<<nblk(kept, B), B, 0, s>>>(kept, all, due, c->perm, gd, key, c->cell, c->id, id_new,
+                                                 c->pinst, pinst_new, inv);
+            c->launches += 1;
+            if (keep_lists) {
+                NbrList nl{c->nbr, c->nbr_count, c->xl, c->yl, c->maxn};
+                double *xl_new = c->tmp + 12 * MX, *yl_new = c->tmp + 13 * MX;
+                k_remap_lists<<<nblk(kept, 128), 128, 0, s>>>(kept, all, due, c->pinst, c->perm, inv, n, nl,
+                                                              c->nbr_tmp, cnt_new, xl_new, yl_new);
+                k_put_back_lists<<<nblk(kept, B), B, 0, s>>>(kept, all, due, c->pinst, nl, c->nbr_tmp, cnt_new,
+                                                             xl_new, yl_new);
+                c->launches += 2;
+            }
+            k_put_back<<<nblk(kept, B), B, 0, s>>>(kept, all, due, gd, c->s0, id_new, c->id, pinst_new, c->pinst);
+            c->launches += 1;
+        }
+    } else {
+        SIMP_CUDA(c, cudaMemsetAsync(c->cell_start, 0, sizeof(int) * (size_t)(nkeys + 1), s));
+    }
+    k_reset_disp<<<1, 1, 0, s>>>(c->sc, keep_lists ? 1 : 0);
+    c->launches += 1;
     SIMP_CUDA(c, cudaGetLastError());
-    c->steps_since_rebuild = 0;
+    if (!keep_lists) c->lists_valid = false;
+    c->n = kept;
     c->rebuilds += 1;
     return SIMP_OK;
 }

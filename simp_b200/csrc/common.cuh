@@ -47,12 +47,42 @@ struct PairList {
     int stride;
 };
 
-// Uniform cell grid.  cell = clamp(floor((x - x0) * inv_cs)); rows are y.
+// Uniform cell grid of one basin.  cell = clamp(floor((x - x0) * inv_cs));
+// rows are y.  A batch gives every basin (instance) its own grid in one
+// shared cell-key space: key = base + row * ncx + col, so instances never
+// share a cell and never interact.
 struct Grid {
     double x0, y0, cs, inv_cs;
-    int ncx, ncy;
-    const int *cell_start;  // ncx * ncy + 1 entries, cell-ordered ranges
+    int ncx, ncy, base;
+    const int *cell_start;  // global: total cells + 1 entries, cell-ordered ranges
 };
+
+// Per-instance data of a batch (device table, indexed by instance id).
+struct Inst {
+    double x0, y0, cs, inv_cs;   // grid of this instance
+    int ncx, ncy, base;
+    int wind_kind;
+    double wind_u, wind_v, vortex_x, vortex_y, vortex_umax, vortex_radius;
+    double b_length;
+    double t;                    // this instance's current_time
+    double hmin, hmax, bs;       // hsml bounds and reference bucket size
+    unsigned long long dmax2_bits;  // max squared displacement since its last sort
+    int flags;                   // FLAG_* seen in this instance
+    int pad;
+};
+
+__host__ __device__ __forceinline__ Grid inst_grid(const Inst &I, const int *cell_start) {
+    Grid g;
+    g.x0 = I.x0;
+    g.y0 = I.y0;
+    g.cs = I.cs;
+    g.inv_cs = I.inv_cs;
+    g.ncx = I.ncx;
+    g.ncy = I.ncy;
+    g.base = I.base;
+    g.cell_start = cell_start;
+    return g;
+}
 
 // Device-resident integrator scalars and per-step reductions.
 struct Scalars {
@@ -209,20 +239,21 @@ __device__ __forceinline__ double boundary_w(const Phys &P, double br, double hs
     return 0.0;
 }
 
-// Wind at a particle: uniform (wind_forcing.f90:36-37) or a cyclonic vortex
+// Wind at a particle of an instance: uniform (the reference hard-codes one,
+// wind_forcing.f90:36-37) or a cyclonic vortex
 // U(r) = Umax (r/R) exp((1 - r^2/R^2)/2), counter-clockwise.
-__device__ __forceinline__ void wind_at(const Phys &P, double x, double y, double *wu, double *wv) {
-    if (P.wind_kind == SIMP_WIND_VORTEX) {
-        const double rx = x - P.vortex_x, ry = y - P.vortex_y;
+__device__ __forceinline__ void wind_at(const Inst &I, double x, double y, double *wu, double *wv) {
+    if (I.wind_kind == SIMP_WIND_VORTEX) {
+        const double rx = x - I.vortex_x, ry = y - I.vortex_y;
         const double r = sqrt(rx * rx + ry * ry);
         if (r == 0.0) { *wu = 0.0; *wv = 0.0; return; }
-        const double s = r / P.vortex_radius;
-        const double U = P.vortex_umax * s * exp(0.5 * (1.0 - s * s));
+        const double s = r / I.vortex_radius;
+        const double U = I.vortex_umax * s * exp(0.5 * (1.0 - s * s));
         *wu = -U * ry / r;
         *wv = U * rx / r;
     } else {
-        *wu = P.wind_u;
-        *wv = P.wind_v;
+        *wu = I.wind_u;
+        *wv = I.wind_v;
     }
 }
 
@@ -238,9 +269,10 @@ __device__ __forceinline__ int clamp_radius(double Rd, const Grid &g) {
     return (int)Rd;
 }
 
-__device__ __forceinline__ int stencil_radius(const Scalars *sc, const Grid &g, double extra) {
-    const double dm = sqrt(bitsd(sc->dmax2_bits));
-    const double reach = fmax(sc->hmax, extra) + 2.0 * dm;
+__device__ __forceinline__ int stencil_radius(double hmax, unsigned long long dmax2_bits, const Grid &g,
+                                              double extra) {
+    const double dm = sqrt(bitsd(dmax2_bits));
+    const double reach = fmax(hmax, extra) + 2.0 * dm;
     return clamp_radius(ceil(reach * g.inv_cs * (1.0 + 1e-12) + 1e-9), g);
 }
 

@@ -1,4 +1,5 @@
-// Host-side context of one resident basin (the C ABI's opaque simp_ctx).
+// Host-side context (the C ABI's opaque simp_ctx): one batch of resident
+// basins ("instances").  A single-basin context is a batch of one.
 #pragma once
 
 #include <cstdint>
@@ -8,58 +9,76 @@
 
 #include "common.cuh"
 
+// Host bookkeeping of one instance slot.
+struct InstHost {
+    bool active = false;
+    simp::Inst I{};                // host copy of the device table entry
+    int n = 0, nb = 0;             // particles and wall particles
+    int id_base = 0;               // global particle id = id_base + local index
+    double grid_hmax = 0.0;        // max(hsml) its grid was sized for
+    long long steps_since_sort = 0;
+    long long steps_done = 0;
+    std::vector<double> xb, massb; // its walls (re-binned when the layout changes)
+};
+
 struct simp_ctx {
     simp_params prm{};
     simp::Phys phys{};
-    int maxn = 0, maxnb = 0;
-    int n = 0, nb = 0;
+    int maxn = 0, maxnb = 0;       // capacities over all instances
+    int max_inst = 1;
+    int n = 0, nb = 0;             // particles and walls over all instances
     bool have_state = false;
     bool keep_diag = false;
     std::string err;
     cudaStream_t stream = nullptr;
     int device = 0;
 
+    // instances
+    std::vector<InstHost> insts;   // max_inst slots
+    simp::Inst *inst_dev = nullptr;
+    int ninst = 0;                 // table entries in use (highest active slot + 1)
+    int id_stride = 0;             // 0 for a single basin, 1 << 21 for batches
+    int total_cells = 0;           // cell keys over all instances
+
     // particle state sets (device, cell order)
     simp::State s0{}, s1{};
     double *mass1 = nullptr;       // half-step mass when the mass update is on
-    double *xr = nullptr, *yr = nullptr;  // positions at the last rebuild
+    double *xr = nullptr, *yr = nullptr;  // sort positions (updated when the instance is re-sorted)
     double *xl = nullptr, *yl = nullptr;  // positions where each Verlet list was built
-    int *cell = nullptr;           // rebuild-time cell id per particle
-    int *id = nullptr;             // original index per particle
-    int *inv_id = nullptr;         // cell-order position of original index
+    int *cell = nullptr;           // sort-time cell key per particle
+    int *id = nullptr;             // global particle id
+    int *pinst = nullptr;          // instance slot of each particle (-1: being removed)
     // per-RHS intermediates from the kinematic pass
     double *tau11 = nullptr, *tau12 = nullptr, *tau22 = nullptr, *div = nullptr;
     int *nbr = nullptr;            // kMaxNbr * maxn neighbour indices (column-major)
     int *nbr_count = nullptr;      // maxn
+    int *nbr_tmp = nullptr;        // kMaxNbr * maxn: lists being renamed by a sort
+    bool lists_valid = false;      // every particle's list was built by a kinematic pass
     int *pair_j = nullptr;         // kMaxPairs * maxn exact pairs of the current RHS
     int *pair_count = nullptr;     // maxn
     // diagnostics (epsilon_11.. sigma_22, zeta, eta, p)
     double *diag = nullptr;        // 9 * maxn
     // rates of the last single_step (cell order): ax, ay, dhdt, dAdt
     double *rates = nullptr;       // 4 * maxn
-    // boundary particles (cell order in the same grid)
+    // wall particles, sorted by cell key
     double *bx = nullptr, *by = nullptr, *bm = nullptr;
-    int *bid = nullptr;            // original wall index per wall slot
-    int *bcell = nullptr;          // cell id per wall slot
+    int *bid = nullptr;            // local wall index within its instance
+    int *binst = nullptr;          // instance slot of each wall particle
+    int *bcell = nullptr;          // cell key per wall slot
     int *bcell_start = nullptr;
-    // cell grid
-    simp::Grid grid{};
-    double grid_hmax = 0.0;        // max(hsml) the grid was sized for
+    // cell lists
     int *cell_start = nullptr;
     size_t cell_cap = 0;
     // rebuild scratch
     int *cnt = nullptr;            // per-cell counters (cell_cap)
     int *perm = nullptr;           // maxn
-    double *tmp = nullptr;         // maxn * 12 doubles reorder scratch
-    int *itmp = nullptr;           // maxn * 3 ints
+    double *tmp = nullptr;         // 14 * max(maxn, maxnb) doubles reorder scratch
+    int *itmp = nullptr;           // 5 * max(maxn, maxnb) ints
     void *scan_tmp = nullptr;
     size_t scan_tmp_bytes = 0;
     // scalars
     simp::Scalars *sc = nullptr;
-    simp::Scalars *sc_host = nullptr;  // pinned mirror: [0] synchronous reads,
-                                       // [1..kSnapRing] per-step snapshots
-    // host copies of the walls (re-binned when the grid is resized)
-    std::vector<double> host_xb, host_massb;
+    simp::Scalars *sc_host = nullptr;  // pinned mirror
     // NNPS export scratch
     int *pair_cnt = nullptr;       // maxn + 1
     int *bpair_cnt = nullptr;      // maxnb + 1
@@ -78,15 +97,22 @@ struct simp_ctx {
     cudaEvent_t prof_ev[kProfKernels + 1] = {};
     double prof_ms[kProfKernels] = {};
     long long prof_steps = 0;
-    // rebuild policy
-    int steps_since_rebuild = 0;
     long long rebuilds = 0;
 };
 
 namespace simp {
 
+// Steps between the re-sorts of an instance into its cell grid.  A fixed
+// schedule per instance (not a displacement test over the whole batch)
+// keeps each instance's summation order independent of the other instances.
+constexpr int kSortEvery = 16;
+constexpr int kMaxSlots = 1024;
+
 // cell_list.cu
-int rebuild(simp_ctx *c);               // sort particles into cell order
+struct DueMask {
+    unsigned long long w[kMaxSlots / 64];
+};
+int rebuild(simp_ctx *c, const DueMask &due, bool full, bool new_lists);   // sort into cell order
 void launch_scan_i32(const int *in, int *out, int n, void *tmp, cudaStream_t s);
 constexpr int kScanKernels = 4;         // kernels per launch_scan_i32
 size_t scan_tmp_bytes(int n);
@@ -98,7 +124,7 @@ void launch_stress(simp_ctx *c, const State &nb, const State &own, EpiMode mode)
 void launch_step_finish(simp_ctx *c);
 void launch_reset_stats(simp_ctx *c);
 
-// nnps_export.cu
+// nnps_export.cu (instance 0 of the context)
 int export_pairs(simp_ctx *c, int32_t *nip, int32_t *p_i, int32_t *p_j, double *r_ij,
                  double *hsml_ij, int32_t cap, int32_t *bnip, int32_t *bp_i, int32_t *bp_j,
                  double *br_ij, int32_t bcap);

@@ -19,10 +19,10 @@ struct BinRule {
     long long bx, by;
 };
 
-__device__ __forceinline__ BinRule make_bin_rule(const Scalars *sc, double xi, double yi, double reach) {
+__device__ __forceinline__ BinRule make_bin_rule(double bs, double xi, double yi, double reach) {
     BinRule b;
-    b.on = reach >= sc->bs * (1.0 - 1e-6);
-    b.bs = sc->bs;
+    b.on = reach >= bs * (1.0 - 1e-6);
+    b.bs = bs;
     b.bx = b.on ? ref_bin(xi, b.bs) : 0;
     b.by = b.on ? ref_bin(yi, b.bs) : 0;
     return b;
@@ -34,19 +34,28 @@ __device__ __forceinline__ bool bin_rule_ok(const BinRule &b, double xj, double 
     return dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1;
 }
 
+// Visits the stencil rows of cell ci (a global key of grid g) within radius
+// R: f(j0, j1) for each row's contiguous index range.
+template <class F>
+__device__ __forceinline__ void for_stencil_rows(const Grid &g, int ci, int R, F &&f) {
+    const int local = ci - g.base;
+    const int cx = local % g.ncx, cy = local / g.ncx;
+    const int r0 = max(cy - R, 0), r1 = min(cy + R, g.ncy - 1);
+    const int c0 = max(cx - R, 0), c1 = min(cx + R, g.ncx - 1);
+    for (int row = r0; row <= r1; ++row) {
+        const int k = g.base + row * g.ncx;
+        f(g.cell_start[k + c0], g.cell_start[k + c1 + 1]);
+    }
+}
+
 // f(j, dx, dy, r, mh): dx = x_i - x_j, r = reference distance, mh = hsml_ij.
 template <class F>
 __device__ __forceinline__ int for_each_pair(const double *__restrict__ X, const double *__restrict__ Y,
                                              const double *__restrict__ HS, const Grid &g, int i, int ci,
                                              int R, const BinRule &br, double xi, double yi, double hi,
                                              F &&f) {
-    const int cx = ci % g.ncx, cy = ci / g.ncx;
-    const int r0 = max(cy - R, 0), r1 = min(cy + R, g.ncy - 1);
-    const int c0 = max(cx - R, 0), c1 = min(cx + R, g.ncx - 1);
     int count = 0;
-    for (int row = r0; row <= r1; ++row) {
-        const int j0 = g.cell_start[row * g.ncx + c0];
-        const int j1 = g.cell_start[row * g.ncx + c1 + 1];
+    for_stencil_rows(g, ci, R, [&](int j0, int j1) {
         for (int j = j0; j < j1; ++j) {
             if (j == i) continue;
             const double xj = X[j], yj = Y[j];
@@ -58,7 +67,7 @@ __device__ __forceinline__ int for_each_pair(const double *__restrict__ X, const
             ++count;
             f(j, dx, dy, r, mh);
         }
-    }
+    });
     return count;
 }
 
@@ -70,13 +79,10 @@ __device__ __forceinline__ int for_each_wall(const double *__restrict__ BX, cons
                                              const int *__restrict__ bstart, const Grid &g, int ci, int Rb,
                                              const BinRule &br, double xi, double yi, double b_length,
                                              F &&f) {
-    const int cx = ci % g.ncx, cy = ci / g.ncx;
-    const int r0 = max(cy - Rb, 0), r1 = min(cy + Rb, g.ncy - 1);
-    const int c0 = max(cx - Rb, 0), c1 = min(cx + Rb, g.ncx - 1);
+    Grid gb = g;
+    gb.cell_start = bstart;
     int count = 0;
-    for (int row = r0; row <= r1; ++row) {
-        const int b0 = bstart[row * g.ncx + c0];
-        const int b1 = bstart[row * g.ncx + c1 + 1];
+    for_stencil_rows(gb, ci, Rb, [&](int b0, int b1) {
         for (int b = b0; b < b1; ++b) {
             const double xb = BX[b], yb = BY[b];
             const double bdx = __dsub_rn(xb, xi), bdy = __dsub_rn(yb, yi);
@@ -86,7 +92,7 @@ __device__ __forceinline__ int for_each_wall(const double *__restrict__ BX, cons
             ++count;
             f(b, bdx, bdy, d);
         }
-    }
+    });
     return count;
 }
 
@@ -97,9 +103,8 @@ __device__ __forceinline__ int for_each_wall(const double *__restrict__ BX, cons
 // (5.7 X / hmin + 12) 2^-24 relative near the decision boundary (where
 // mhsml >= hmin).  The returned margin doubles that bound; a candidate is
 // decided in FP32 only outside the margin, otherwise by the exact FP64 test.
-__device__ __forceinline__ float prefilter_margin(const Scalars *sc) {
-    const double X = bitsd(sc->xabs_bits);
-    return (float)((12.0 * X / sc->hmin + 40.0) * 0x1p-24);
+__device__ __forceinline__ float prefilter_margin(double xabs, double hmin) {
+    return (float)((12.0 * xabs / hmin + 40.0) * 0x1p-24);
 }
 
 // 0: not a pair, 1: a pair, 2: undecided (use the FP64 test)
@@ -113,8 +118,8 @@ __device__ __forceinline__ int prefilter(float dxf, float dyf, float mf, float m
 
 // Stencil radius for wall pairs: walls are static, the particle moved at
 // most sqrt(dmax2) since it was binned.
-__device__ __forceinline__ int wall_radius(const Scalars *sc, const Grid &g, double b_length) {
-    const double dm = sqrt(bitsd(sc->dmax2_bits));
+__device__ __forceinline__ int wall_radius(unsigned long long dmax2_bits, const Grid &g, double b_length) {
+    const double dm = sqrt(bitsd(dmax2_bits));
     return clamp_radius(ceil((b_length + dm) * g.inv_cs * (1.0 + 1e-12) + 1e-9), g);
 }
 

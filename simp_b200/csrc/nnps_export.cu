@@ -1,4 +1,5 @@
-// Pair-list export of the NNPS entry point and the density pair sum.
+// Pair-list export of the NNPS entry point and the density pair sum, for
+// the context's single basin (instance 0).
 //
 // The reference's NNPS writes p_i, p_j, r_ij, hsml_ij (nnps.f90:284-288) and
 // bp_i, bp_j, br_ij (:479-482) into global arrays, in an order that depends on
@@ -22,7 +23,8 @@ inline int nblk(long long n, int b) { return (int)((n + b - 1) / b); }
 
 struct ExpArgs {
     State s;
-    Grid g;
+    const Inst *inst;          // instance 0 (the basin)
+    const int *cell_start;
     const int *cell;
     const int *id;
     const double *bx, *by;
@@ -41,18 +43,20 @@ __global__ void __launch_bounds__(kBlock) k_count(ExpArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const State &s = a.s;
+    const Inst &I = a.inst[0];
+    const Grid g = inst_grid(I, a.cell_start);
     const double xi = s.x[i], yi = s.y[i], hi = s.hs[i];
     const int ci = a.cell[i];
-    const int R = stencil_radius(a.sc, a.g, 0.0);
-    const BinRule br = make_bin_rule(a.sc, xi, yi, a.sc->hmax);
+    const int R = stencil_radius(I.hmax, I.dmax2_bits, g, 0.0);
+    const BinRule br = make_bin_rule(I.bs, xi, yi, I.hmax);
     const int idi = a.id[i];
     int up = 0;
-    int cnt = for_each_pair(s.x, s.y, s.hs, a.g, i, ci, R, br, xi, yi, hi,
+    int cnt = for_each_pair(s.x, s.y, s.hs, g, i, ci, R, br, xi, yi, hi,
                             [&](int j, double, double, double, double) { up += (a.id[j] > idi); });
     if (a.P.boundary_pressure && a.nb > 0) {
-        const int Rb = wall_radius(a.sc, a.g, a.P.b_length);
-        const BinRule bb = make_bin_rule(a.sc, xi, yi, a.P.b_length);
-        cnt += for_each_wall(a.bx, a.by, a.bstart, a.g, ci, Rb, bb, xi, yi, a.P.b_length,
+        const int Rb = wall_radius(I.dmax2_bits, g, I.b_length);
+        const BinRule bb = make_bin_rule(I.bs, xi, yi, I.b_length);
+        cnt += for_each_wall(a.bx, a.by, a.bstart, g, ci, Rb, bb, xi, yi, I.b_length,
                              [&](int, double, double, double) {});
     }
     a.up_cnt[idi] = up;
@@ -66,13 +70,15 @@ __global__ void __launch_bounds__(kBlock) k_emit(ExpArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const State &s = a.s;
+    const Inst &I = a.inst[0];
+    const Grid g = inst_grid(I, a.cell_start);
     const double xi = s.x[i], yi = s.y[i], hi = s.hs[i];
-    const int R = stencil_radius(a.sc, a.g, 0.0);
-    const BinRule br = make_bin_rule(a.sc, xi, yi, a.sc->hmax);
+    const int R = stencil_radius(I.hmax, I.dmax2_bits, g, 0.0);
+    const BinRule br = make_bin_rule(I.bs, xi, yi, I.hmax);
     const int idi = a.id[i];
     const int base = a.up_off[idi];
     int k = 0;
-    for_each_pair(s.x, s.y, s.hs, a.g, i, a.cell[i], R, br, xi, yi, hi,
+    for_each_pair(s.x, s.y, s.hs, g, i, a.cell[i], R, br, xi, yi, hi,
                   [&](int j, double, double, double r, double mh) {
                       const int idj = a.id[j];
                       if (idj <= idi) return;
@@ -102,13 +108,12 @@ __global__ void __launch_bounds__(kBlock) k_emit(ExpArgs a) {
 // Wall pairs from the wall side: fluid particles binned within the stencil.
 struct WallArgs {
     State s;
-    Grid g;
+    const Inst *inst;
+    const int *cell_start;
     const int *id;
     const double *bx, *by;
     const int *bcell, *bid;
     int nb;
-    double b_length;
-    Scalars *sc;
     int *cnt;        // by original wall index
     const int *off;
     int *oi, *oj;
@@ -119,22 +124,19 @@ struct WallArgs {
 __global__ void __launch_bounds__(kBlock) k_wall(WallArgs a) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= a.nb) return;
+    const Inst &I = a.inst[0];
+    const Grid g = inst_grid(I, a.cell_start);
     const double xb = a.bx[b], yb = a.by[b];
-    const int cb = a.bcell[b];
-    const int Rb = wall_radius(a.sc, a.g, a.b_length);
-    const BinRule bb = make_bin_rule(a.sc, xb, yb, a.b_length);
-    const int cx = cb % a.g.ncx, cy = cb / a.g.ncx;
-    const int r0 = max(cy - Rb, 0), r1 = min(cy + Rb, a.g.ncy - 1);
-    const int c0 = max(cx - Rb, 0), c1 = min(cx + Rb, a.g.ncx - 1);
+    const int Rb = wall_radius(I.dmax2_bits, g, I.b_length);
+    const BinRule bb = make_bin_rule(I.bs, xb, yb, I.b_length);
     const int idb = a.bid[b];
     const int base = a.emit ? a.off[idb] : 0;
     int k = 0;
-    for (int row = r0; row <= r1; ++row) {
-        const int j0 = a.g.cell_start[row * a.g.ncx + c0], j1 = a.g.cell_start[row * a.g.ncx + c1 + 1];
+    for_stencil_rows(g, a.bcell[b], Rb, [&](int j0, int j1) {
         for (int j = j0; j < j1; ++j) {
             const double xj = a.s.x[j], yj = a.s.y[j];
             const double d = ref_distance(__dsub_rn(xb, xj), __dsub_rn(yb, yj));
-            if (!(d <= a.b_length)) continue;
+            if (!(d <= I.b_length)) continue;
             if (!bin_rule_ok(bb, xj, yj)) continue;
             if (a.emit) {
                 a.oi[base + k] = idb + 1;
@@ -143,7 +145,7 @@ __global__ void __launch_bounds__(kBlock) k_wall(WallArgs a) {
             }
             ++k;
         }
-    }
+    });
     if (!a.emit) {
         a.cnt[idb] = k;
         return;
@@ -164,11 +166,11 @@ __global__ void __launch_bounds__(kBlock) k_wall(WallArgs a) {
 
 struct DenArgs {
     State s;
-    Grid g;
+    const Inst *inst;
+    const int *cell_start;
     const int *cell;
     const int *id;
     Phys P;
-    Scalars *sc;
     int n;
     double *out;   // original order
 };
@@ -179,13 +181,15 @@ __global__ void __launch_bounds__(kBlock) k_sum_density(DenArgs a) {
     if (i >= a.n) return;
     const State &s = a.s;
     const Phys &P = a.P;
+    const Inst &I = a.inst[0];
+    const Grid g = inst_grid(I, a.cell_start);
     const double xi = s.x[i], yi = s.y[i], hi = s.hs[i];
-    const int R = stencil_radius(a.sc, a.g, 0.0);
-    const BinRule br = make_bin_rule(a.sc, xi, yi, a.sc->hmax);
+    const int R = stencil_radius(I.hmax, I.dmax2_bits, g, 0.0);
+    const BinRule br = make_bin_rule(I.bs, xi, yi, I.hmax);
     const double k0 = kernel_zero(P, hi);
     const double mi = s.m[i], rhoi = s.rho[i];
     double num = k0 * mi, den = k0 * mi / rhoi;
-    for_each_pair(s.x, s.y, s.hs, a.g, i, a.cell[i], R, br, xi, yi, hi,
+    for_each_pair(s.x, s.y, s.hs, g, i, a.cell[i], R, br, xi, yi, hi,
                   [&](int j, double, double, double r, double mh) {
                       double w, gf;
                       pair_kernel<true>(P, r, mh, &w, &gf);
@@ -205,7 +209,8 @@ int export_pairs(simp_ctx *c, int32_t *nip, int32_t *p_i, int32_t *p_j, double *
     const int n = c->n;
     ExpArgs a{};
     a.s = c->s0;
-    a.g = c->grid;
+    a.inst = c->inst_dev;
+    a.cell_start = c->cell_start;
     a.cell = c->cell;
     a.id = c->id;
     a.bx = c->bx;
@@ -227,15 +232,14 @@ int export_pairs(simp_ctx *c, int32_t *nip, int32_t *p_i, int32_t *p_j, double *
     int btotal = 0;
     WallArgs w{};
     w.s = c->s0;
-    w.g = c->grid;
+    w.inst = c->inst_dev;
+    w.cell_start = c->cell_start;
     w.id = c->id;
     w.bx = c->bx;
     w.by = c->by;
     w.bcell = c->bcell;
     w.bid = c->bid;
     w.nb = c->nb;
-    w.b_length = c->prm.b_length;
-    w.sc = c->sc;
     const bool walls = c->prm.boundary_pressure && c->nb > 0;
     if (walls) {
         w.cnt = c->itmp + (size_t)std::max(c->maxn, c->maxnb);
@@ -308,11 +312,11 @@ int export_pairs(simp_ctx *c, int32_t *nip, int32_t *p_i, int32_t *p_j, double *
 int sum_density(simp_ctx *c, double *rho_out_dev) {
     DenArgs a{};
     a.s = c->s0;
-    a.g = c->grid;
+    a.inst = c->inst_dev;
+    a.cell_start = c->cell_start;
     a.cell = c->cell;
     a.id = c->id;
     a.P = c->phys;
-    a.sc = c->sc;
     a.n = c->n;
     a.out = rho_out_dev;
     k_sum_density<<<nblk(c->n, kBlock), kBlock, 0, c->stream>>>(a);

@@ -116,6 +116,7 @@ __global__ void k_grid(unsigned char *base) {
     g.inv_cs = 1.0 / cs;
     g.ncx = min(kMaxCells, max(1, (int)ceil(w / cs)));
     g.ncy = min(kMaxCells / g.ncx, max(1, (int)ceil(hh / cs)));
+    g.base = 0;
     g.cell_start = at<int>(base, kOffStart);
     h->grid = g;
     Scalars s{};
@@ -185,7 +186,7 @@ __global__ void __launch_bounds__(kB) k_density(unsigned char *base, int n, Phys
     const double *HS = at<double>(base, kOffHs), *M = at<double>(base, kOffM);
     const double *RHO = at<double>(base, kOffRho);
     const double xi = X[i], yi = Y[i], hi = HS[i];
-    const BinRule br = make_bin_rule(&hd->sc, xi, yi, hd->sc.hmax);
+    const BinRule br = make_bin_rule(hd->sc.bs, xi, yi, hd->sc.hmax);
     const double k0 = kernel_zero(P, hi);
     const double mi = M[i];
     double num = k0 * mi, den = k0 * mi / RHO[i];

@@ -41,43 +41,74 @@ constexpr int kBlock = 128;
 // per-thread shared-memory list: the whole pair list of a particle with up
 // to kMaxPairs pairs (then written out row by row), flushed when full
 constexpr int kListSlots = kMaxPairs + 1;
+// minimum resident blocks per SM (register caps 73 and 64): more warps in
+// flight to hide the latency of the neighbour gathers
+constexpr int kMinBlocksKin = 7;
+constexpr int kMinBlocksStress = 8;
 
-// Per-pair FP64 geometry and kernel gradient: dw = gfac * (dx, dy).
-// r = s * rsqrt(s) and 1/hsml_ij from the particle's own 1/hsml when the two
-// smoothing lengths are equal (then hsml_ij = hsml_i exactly).
-struct PairGeom {
-    double dx, dy, gfac, w;
+// Pair arithmetic type T: double for the plain form, float for the mixed
+// form.  Positions and velocities stay FP64; their differences are formed in
+// FP64 and rounded to T, after which the kernel gradient and the pair sums
+// run in T (compensated when T is float).
+__device__ __forceinline__ double rsq(double v) { return rsqrt(v); }
+__device__ __forceinline__ float rsq(float v) { return rsqrtf(v); }
+
+// Sum of pair terms: plain FP64, or FP32 with Kahan compensation.
+template <class T>
+struct Sum {
+    double s = 0.0;
+    __device__ __forceinline__ void add(double v) { s += v; }
+    __device__ __forceinline__ double get() const { return s; }
+};
+template <>
+struct Sum<float> {
+    float s = 0.0f, c = 0.0f;
+    __device__ __forceinline__ void add(float v) {
+        const float y = v - c;
+        const float t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+    __device__ __forceinline__ double get() const { return (double)s - (double)c; }
 };
 
-template <bool WANT_W>
-__device__ __forceinline__ PairGeom pair_geom(const Phys &P, double xi, double yi, double hi, double inv_hi,
-                                              double xj, double yj, double hj) {
-    PairGeom g;
-    g.dx = xi - xj;
-    g.dy = yi - yj;
-    const double s = g.dx * g.dx + g.dy * g.dy;
-    const double rs = rsqrt(s);
-    const double r = s * rs;
-    const double inv_h = (hj == hi) ? inv_hi : 2.0 / (hi + hj);
-    const double sh = (double)P.scale_h;
-    const double shh = sh * inv_h;
-    const double q = r * shh;
-    double gq;
+// Per-pair geometry and kernel gradient: dw = gfac * (dx, dy).
+// r = s * rsqrt(s) and 1/hsml_ij from the particle's own 1/hsml when the two
+// smoothing lengths are equal (then hsml_ij = hsml_i exactly).
+template <class T>
+struct PairGeom {
+    T dx, dy, gfac, w;
+};
+
+template <class T, bool WANT_W>
+__device__ __forceinline__ PairGeom<T> pair_geom(const Phys &P, double xi, double yi, double hi, double inv_hi,
+                                                 double xj, double yj, double hj) {
+    PairGeom<T> g;
+    g.dx = (T)(xi - xj);
+    g.dy = (T)(yi - yj);
+    const T s = g.dx * g.dx + g.dy * g.dy;
+    const T rs = rsq(s);
+    const T r = s * rs;
+    const T inv_h = (T)((hj == hi) ? inv_hi : 2.0 / (hi + hj));
+    const T sh = (T)P.scale_h;
+    const T shh = sh * inv_h;
+    const T q = r * shh;
+    T gq;
     if (P.skf == SIMP_SKF_WENDLAND_C6) {
-        const double factor = (78.0 / (7.0 * kPi)) * (shh * shh);
-        const double om = 1.0 - q;
-        const double om2 = om * om, om4 = om2 * om2;
-        if (WANT_W) g.w = factor * (om4 * om4) * (((32.0 * q + 25.0) * q + 8.0) * q + 1.0);
-        gq = factor * (-22.0 * q * (om4 * om2 * om) * ((16.0 * q + 7.0) * q + 1.0));
+        const T factor = (T)(78.0 / (7.0 * kPi)) * (shh * shh);
+        const T om = T(1) - q;
+        const T om2 = om * om, om4 = om2 * om2;
+        if (WANT_W) g.w = factor * (om4 * om4) * (((T(32) * q + T(25)) * q + T(8)) * q + T(1));
+        gq = factor * (T(-22) * q * (om4 * om2 * om) * ((T(16) * q + T(7)) * q + T(1)));
     } else {
-        const double factor = (15.0 / (7.0 * kPi)) * (shh * shh);
-        if (q <= 1.0) {
-            if (WANT_W) g.w = factor * ((double)(2.0f / 3.0f) - q * q + 0.5 * q * q * q);
-            gq = factor * (-2.0 * q + 1.5 * q * q);
+        const T factor = (T)(15.0 / (7.0 * kPi)) * (shh * shh);
+        if (q <= T(1)) {
+            if (WANT_W) g.w = factor * ((T)(2.0f / 3.0f) - q * q + T(0.5) * q * q * q);
+            gq = factor * (T(-2) * q + T(1.5) * q * q);
         } else {
-            const double u = 2.0 - q;
-            if (WANT_W) g.w = factor * ((double)(1.0f / 6.0f) * u * u * u);
-            gq = factor * (-0.5 * u * u);
+            const T u = T(2) - q;
+            if (WANT_W) g.w = factor * ((T)(1.0f / 6.0f) * u * u * u);
+            gq = factor * (T(-0.5) * u * u);
         }
     }
     g.gfac = gq * shh * rs;
@@ -91,9 +122,13 @@ struct PairCtx {
     float margin;
     bool use_f32;
     BinRule br;
+    Grid g;                     // the particle's instance grid
+    double hmax;                // instance bounds for the stencil radius
+    unsigned long long dmax2_bits;
 };
 
-__device__ __forceinline__ PairCtx pair_ctx(const State &s, const Scalars *sc, int i) {
+__device__ __forceinline__ PairCtx pair_ctx(const State &s, const Scalars *sc, const Inst &I,
+                                            const int *cell_start, int i) {
     PairCtx p;
     p.xi = s.x[i];
     p.yi = s.y[i];
@@ -101,9 +136,12 @@ __device__ __forceinline__ PairCtx pair_ctx(const State &s, const Scalars *sc, i
     p.xif = s.xf[i];
     p.yif = s.yf[i];
     p.hif = s.hsf[i];
-    p.margin = prefilter_margin(sc);
+    p.margin = prefilter_margin(bitsd(sc->xabs_bits), I.hmin);
     p.use_f32 = p.margin < 0.25f;
-    p.br = make_bin_rule(sc, p.xi, p.yi, sc->hmax);
+    p.br = make_bin_rule(I.bs, p.xi, p.yi, I.hmax);
+    p.g = inst_grid(I, cell_start);
+    p.hmax = I.hmax;
+    p.dmax2_bits = I.dmax2_bits;
     return p;
 }
 
@@ -128,15 +166,10 @@ __device__ __forceinline__ bool is_pair(const State &s, const PairCtx &p, int j)
 // Visits the cell-stencil candidates of particle i (cell order).
 template <class F>
 __device__ __forceinline__ void for_stencil(const Grid &g, int i, int ci, int R, F &&f) {
-    const int cx = ci % g.ncx, cy = ci / g.ncx;
-    const int r0 = max(cy - R, 0), r1 = min(cy + R, g.ncy - 1);
-    const int c0 = max(cx - R, 0), c1 = min(cx + R, g.ncx - 1);
-    for (int row = r0; row <= r1; ++row) {
-        const int j0 = g.cell_start[row * g.ncx + c0];
-        const int j1 = g.cell_start[row * g.ncx + c1 + 1];
+    for_stencil_rows(g, ci, R, [&](int j0, int j1) {
         for (int j = j0; j < j1; ++j)
             if (j != i) f(j);
-    }
+    });
 }
 
 // Every current pair of particle i: from its Verlet list when that list
@@ -145,9 +178,8 @@ __device__ __forceinline__ void for_stencil(const Grid &g, int i, int ci, int R,
 // current pair (i, j) was then at most mhsml + |dx_i| + |dx_j| apart, so i's
 // list is complete while |dx_i| + max_j |dx_j| < skin.
 template <class F>
-__device__ __forceinline__ void for_each_current_pair(const State &s, const Grid &g, const NbrList &nl,
-                                                      const Scalars *sc, int i, int ci, const PairCtx &p,
-                                                      F &&on_pair) {
+__device__ __forceinline__ void for_each_current_pair(const State &s, const NbrList &nl, const Scalars *sc,
+                                                      int i, int ci, const PairCtx &p, F &&on_pair) {
     const int cnt = nl.count[i];
     const double dxl = p.xi - nl.xl[i], dyl = p.yi - nl.yl[i];
     const double own = sqrt(dxl * dxl + dyl * dyl);
@@ -159,7 +191,7 @@ __device__ __forceinline__ void for_each_current_pair(const State &s, const Grid
             if (is_pair(s, p, j)) on_pair(j);
         }
     } else {
-        for_stencil(g, i, ci, stencil_radius(sc, g, 0.0), [&](int j) {
+        for_stencil(p.g, i, ci, stencil_radius(p.hmax, p.dmax2_bits, p.g, 0.0), [&](int j) {
             if (is_pair(s, p, j)) on_pair(j);
         });
     }
@@ -167,7 +199,9 @@ __device__ __forceinline__ void for_each_current_pair(const State &s, const Grid
 
 struct KinArgs {
     State s;
-    Grid g;
+    const int *cell_start;
+    const Inst *inst;
+    const int *pinst;      // instance of each particle
     const int *cell;
     Phys P;
     Scalars *sc;
@@ -178,33 +212,39 @@ struct KinArgs {
     int n, maxn;
 };
 
-__global__ void __launch_bounds__(kBlock) k_kinematic(KinArgs a) {
+template <class T>
+__global__ void __launch_bounds__(kBlock, kMinBlocksKin) k_kinematic(KinArgs a) {
     __shared__ int s_list[kListSlots * kBlock];
     const int t = threadIdx.x;
     const int i = blockIdx.x * blockDim.x + t;
     if (i >= a.n) return;
     const State &s = a.s;
     const Phys &P = a.P;
-    const PairCtx pc = pair_ctx(s, a.sc, i);
+    const Inst &I = a.inst[a.pinst[i]];
+    // a basin whose state turned non-finite is not searched any more (its
+    // stencil would span its whole grid); it is only carried until retired
+    const bool dead = (I.flags & FLAG_NONFINITE) != 0;
+    const PairCtx pc = pair_ctx(s, a.sc, I, a.cell_start, i);
     const double xi = pc.xi, yi = pc.yi, hi = pc.hi;
     const double vxi = s.vx[i], vyi = s.vy[i];
     const double inv_hi = 1.0 / hi;
-    double dv = 0.0, g1 = 0.0, g2 = 0.0, g3 = 0.0, g4 = 0.0;
+    Sum<T> dvs, g1s, g2s, g3s, g4s;   // -div and the velocity gradient, negated
     int cnt = 0;       // entries in this thread's shared-memory list
     int npairs = 0;    // exact pairs found so far
     auto flush = [&]() {
+#pragma unroll 4
         for (int k = 0; k < cnt; ++k) {
             const int j = s_list[k * kBlock + t];
-            const PairGeom pg = pair_geom<false>(P, xi, yi, hi, inv_hi, s.x[j], s.y[j], s.hs[j]);
-            const double dwx = pg.gfac * pg.dx, dwy = pg.gfac * pg.dy;
-            const double dvx = vxi - s.vx[j], dvy = vyi - s.vy[j];
-            const double w1 = dvx * dwx, w2 = dvy * dwx, w3 = dvx * dwy, w4 = dvy * dwy;
-            const double mj = s.m[j], mrj = s.mor[j];
-            dv -= mj * (w1 + w4);
-            g1 -= mrj * w1;
-            g2 -= mrj * w2;
-            g3 -= mrj * w3;
-            g4 -= mrj * w4;
+            const PairGeom<T> pg = pair_geom<T, false>(P, xi, yi, hi, inv_hi, s.x[j], s.y[j], s.hs[j]);
+            const T dwx = pg.gfac * pg.dx, dwy = pg.gfac * pg.dy;
+            const T dvx = (T)(vxi - s.vx[j]), dvy = (T)(vyi - s.vy[j]);
+            const T w1 = dvx * dwx, w2 = dvy * dwx, w3 = dvx * dwy, w4 = dvy * dwy;
+            const T mj = (T)s.m[j], mrj = (T)s.mor[j];
+            dvs.add(mj * (w1 + w4));
+            g1s.add(mrj * w1);
+            g2s.add(mrj * w2);
+            g3s.add(mrj * w3);
+            g4s.add(mrj * w4);
         }
         cnt = 0;
     };
@@ -213,13 +253,20 @@ __global__ void __launch_bounds__(kBlock) k_kinematic(KinArgs a) {
         ++npairs;
         if (++cnt == kListSlots) flush();   // more than kMaxPairs pairs: no pair list
     };
-    if (a.sc->list_scan) {
+    if (a.sc->list_scan && i == 0) atomicExch(&a.sc->dlist2_bits, 0ull);
+    if (dead) {
+        if (a.sc->list_scan) {
+            a.nl.count[i] = 0;
+            a.nl.xl[i] = xi;
+            a.nl.yl[i] = yi;
+        }
+    } else if (a.sc->list_scan) {
         // rebuild the Verlet list from the cell stencil: members are the
         // candidates not certainly beyond mhsml + skin (FP32, with margin)
         const double skin = a.sc->skin;
         const float skinf = (float)skin, grow = 1.0f + pc.margin;
         int total = 0;
-        for_stencil(a.g, i, a.cell[i], stencil_radius(a.sc, a.g, a.sc->hmax + skin), [&](int j) {
+        for_stencil(pc.g, i, a.cell[i], stencil_radius(pc.hmax, pc.dmax2_bits, pc.g, pc.hmax + skin), [&](int j) {
             const float dxf = pc.xif - s.xf[j], dyf = pc.yif - s.yf[j];
             const float lim = 0.5f * (pc.hif + s.hsf[j]) + skinf;
             if (dxf * dxf + dyf * dyf > lim * lim * grow) return;
@@ -230,15 +277,16 @@ __global__ void __launch_bounds__(kBlock) k_kinematic(KinArgs a) {
         a.nl.count[i] = total;
         a.nl.xl[i] = xi;
         a.nl.yl[i] = yi;
-        if (i == 0) atomicExch(&a.sc->dlist2_bits, 0ull);
     } else {
-        for_each_current_pair(s, a.g, a.nl, a.sc, i, a.cell[i], pc, on_pair);
+        for_each_current_pair(s, a.nl, a.sc, i, a.cell[i], pc, on_pair);
     }
     // the stress pass's pair list, one coalesced row per k
     if (npairs <= kMaxPairs)
         for (int k = 0; k < cnt; ++k) a.pl.pj[(size_t)k * a.pl.stride + i] = s_list[k * kBlock + t];
     a.pl.count[i] = npairs;
     flush();
+    const double dv = -dvs.get();
+    const double g1 = -g1s.get(), g2 = -g2s.get(), g3 = -g3s.get(), g4 = -g4s.get();
     // strain rates, single_step.f90:80-84
     const double e11 = g1, e22 = g4, e12 = 0.5 * (g2 + g3);
     // rheology, internal_stress.f90:20-42
@@ -283,7 +331,9 @@ struct StressArgs {
     State rhs;     // state the right-hand side is evaluated at
     State base;    // step-start state (own values for the integrator)
     State out;     // state written by the epilogue
-    Grid g;
+    const int *cell_start;
+    Inst *inst;
+    const int *pinst;
     const int *cell;
     const double *bx, *by, *bm;
     const int *bstart;
@@ -298,6 +348,21 @@ struct StressArgs {
     double *hs_next;
     int n, maxn, mode;
 };
+
+// Max of a per-instance 64-bit field over the lanes of a warp: one atomic per
+// warp when the warp holds a single instance (the common case: instances are
+// contiguous in cell order), one per lane otherwise.
+__device__ __forceinline__ void inst_max_u64(Inst *inst, int k, size_t field, unsigned long long v) {
+    const unsigned mask = __match_any_sync(0xffffffffu, k);
+    if (mask == 0xffffffffu) {
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long t = __shfl_xor_sync(0xffffffffu, v, o);
+            v = (t > v) ? t : v;
+        }
+        if ((threadIdx.x & 31) != 0) return;
+    }
+    atomicMax(reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(&inst[k]) + field), v);
+}
 
 // Block-wide max / min folded into one device atomic per block (the
 // same-address atomics of every warp would serialise in L2).  Called by all
@@ -335,7 +400,8 @@ __device__ __forceinline__ void warp_max_i32(int *dst, int v) {
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(kBlock) k_stress(StressArgs a) {
+template <class T>
+__global__ void __launch_bounds__(kBlock, kMinBlocksStress) k_stress(StressArgs a) {
     const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
     const bool live = i0 < a.n;
     const int i = live ? i0 : a.n - 1;   // dead lanes mirror the last particle for warp reductions
@@ -344,39 +410,48 @@ __global__ void __launch_bounds__(kBlock) k_stress(StressArgs a) {
     const double xi = s.x[i], yi = s.y[i], hi = s.hs[i];
     const double inv_hi = 1.0 / hi;
     const int ci = a.cell[i];
-    double Sx = 0.0, Sy = 0.0, Tx = 0.0, Ty = 0.0;
+    const int ki = a.pinst[i];
+    const Inst &I = a.inst[ki];
+    const bool dead = (I.flags & FLAG_NONFINITE) != 0;   // see k_kinematic
+    Sum<T> Sxs, Sys, Txs, Tys;
     auto accumulate = [&](int j) {
-        const PairGeom pg = pair_geom<false>(P, xi, yi, hi, inv_hi, s.x[j], s.y[j], s.hs[j]);
-        const double dwx = pg.gfac * pg.dx, dwy = pg.gfac * pg.dy;
-        const double mj = s.m[j];
-        const double t11 = a.tau11[j], t12 = a.tau12[j], t22 = a.tau22[j];
-        Sx += mj * dwx;
-        Sy += mj * dwy;
-        Tx += mj * (t11 * dwx + t12 * dwy);
-        Ty += mj * (t12 * dwx + t22 * dwy);
+        const PairGeom<T> pg = pair_geom<T, false>(P, xi, yi, hi, inv_hi, s.x[j], s.y[j], s.hs[j]);
+        const T dwx = pg.gfac * pg.dx, dwy = pg.gfac * pg.dy;
+        const T mj = (T)s.m[j];
+        const T t11 = (T)a.tau11[j], t12 = (T)a.tau12[j], t22 = (T)a.tau22[j];
+        Sxs.add(mj * dwx);
+        Sys.add(mj * dwy);
+        Txs.add(mj * (t11 * dwx + t12 * dwy));
+        Tys.add(mj * (t12 * dwx + t22 * dwy));
     };
     int cnt = a.pl.count[i];
     if (cnt <= kMaxPairs) {
         // the kinematic pass of this right-hand side found the pairs
+#pragma unroll 4
         for (int k = 0; k < cnt; ++k) accumulate(a.pl.pj[(size_t)k * a.pl.stride + i]);
+    } else if (dead) {
+        cnt = 0;
     } else {
         cnt = 0;
-        const PairCtx pc = pair_ctx(s, a.sc, i);
-        for_each_current_pair(s, a.g, a.nl, a.sc, i, ci, pc, [&](int j) {
+        const PairCtx pc = pair_ctx(s, a.sc, I, a.cell_start, i);
+        for_each_current_pair(s, a.nl, a.sc, i, ci, pc, [&](int j) {
             accumulate(j);
             ++cnt;
         });
     }
+    const double Sx = Sxs.get(), Sy = Sys.get(), Tx = Txs.get(), Ty = Tys.get();
     const double rho = s.rho[i], hh = s.h[i], AA = s.A[i], mi = s.m[i];
     const double fi = rho / P.rho_ice / hh;
     double ax = fi * (a.tau11[i] * Sx + a.tau12[i] * Sy + Tx);
     double ay = fi * (a.tau12[i] * Sx + a.tau22[i] * Sy + Ty);
     // boundary force (bf_Monaghan normal component, boundary_force.f90:78-82)
-    if (P.boundary_pressure && a.nb > 0) {
-        const int Rb = wall_radius(a.sc, a.g, P.b_length);
-        const BinRule bb = make_bin_rule(a.sc, xi, yi, P.b_length);
+    if (P.boundary_pressure && a.nb > 0 && !dead) {
+        const Grid g = inst_grid(I, a.cell_start);
+        const double bl = I.b_length;
+        const int Rb = wall_radius(I.dmax2_bits, g, bl);
+        const BinRule bb = make_bin_rule(I.bs, xi, yi, bl);
         double fx = 0.0, fy = 0.0;
-        cnt += for_each_wall(a.bx, a.by, a.bstart, a.g, ci, Rb, bb, xi, yi, P.b_length,
+        cnt += for_each_wall(a.bx, a.by, a.bstart, g, ci, Rb, bb, xi, yi, bl,
                              [&](int b, double bdx, double bdy, double d) {
                                  const double bw = boundary_w(P, d, hi);
                                  const double mb = a.bm[b];
@@ -389,10 +464,10 @@ __global__ void __launch_bounds__(kBlock) k_stress(StressArgs a) {
     }
     // drag, wind_forcing.f90:35-51 and water_drag.f90:35-53 (off at t <= 0)
     const double vxi = s.vx[i], vyi = s.vy[i];
-    const double tnow = a.sc->t;
+    const double tnow = I.t;
     if (P.wind_force && tnow > 0.0) {
         double wu, wv;
-        wind_at(P, xi, yi, &wu, &wv);
+        wind_at(I, xi, yi, &wu, &wv);
         const double ru = wu - vxi, rv = wv - vyi;
         const double k = P.c_wind * P.rho_air / (hh * P.rho_ice);
         ax += k * ru * fabs(ru);
@@ -457,12 +532,25 @@ __global__ void __launch_bounds__(kBlock) k_stress(StressArgs a) {
         hsn = sqrt(mn / rhon) * (double)P.hsml_multiplicity;
         if (hsn > P.max_hsml) hsn = P.max_hsml;
     }
+    // displacement since the instance's last sort, max per instance
     const double dxr = xn - a.xr[i], dyr = yn - a.yr[i];
-    const double d2 = live ? dxr * dxr + dyr * dyr : 0.0;
-    warp_max_u64(&a.sc->dmax2_bits, dbits(d2));
+    // (non-finite values stay out of these bounds: the basin is flagged below)
+    double d2 = dxr * dxr + dyr * dyr;
+    if (!live || !isfinite(d2)) d2 = 0.0;
+    inst_max_u64(a.inst, ki, offsetof(Inst, dmax2_bits), dbits(d2));
     const double dxl = xn - a.nl.xl[i], dyl = yn - a.nl.yl[i];
-    warp_max_u64(&a.sc->dlist2_bits, dbits(live ? dxl * dxl + dyl * dyl : 0.0));
-    warp_max_u64(&a.sc->xabs_bits, dbits(fmax(fabs(xn), fabs(yn))));
+    double dl2 = dxl * dxl + dyl * dyl;
+    if (!live || !isfinite(dl2)) dl2 = 0.0;
+    warp_max_u64(&a.sc->dlist2_bits, dbits(dl2));
+    double xa = fmax(fabs(xn), fabs(yn));
+    if (!isfinite(xa)) xa = 0.0;
+    warp_max_u64(&a.sc->xabs_bits, dbits(xa));
+    const bool bad = !(isfinite(xn) && isfinite(yn) && isfinite(vxn) && isfinite(vyn) &&
+                       isfinite(hn) && isfinite(An));
+    if (live && bad) {
+        atomicOr(&a.sc->flags, FLAG_NONFINITE);
+        atomicOr(&a.inst[ki].flags, FLAG_NONFINITE);
+    }
     if (live) {
         const State &o = a.out;
         o.x[i] = xn;
@@ -487,9 +575,6 @@ __global__ void __launch_bounds__(kBlock) k_stress(StressArgs a) {
             const double v = P.rho_ice * (hsn * hsn) * P.delta_min / (P.P_star * (1.0 + P.k_t));
             warp_min_u64(&a.sc->acc_dt, dbits(v));
         }
-        const bool bad = !(isfinite(xn) && isfinite(yn) && isfinite(vxn) && isfinite(vyn) &&
-                           isfinite(hn) && isfinite(An));
-        if (live && bad) atomicOr(&a.sc->flags, FLAG_NONFINITE);
     }
     // The last block to finish decides whether the next kinematic pass
     // rebuilds the Verlet lists: when the fastest particle moved 3/4 of the
@@ -525,19 +610,32 @@ __global__ void k_commit_hsml(int n, const double *__restrict__ hs_next, double 
 // End of a predictor-corrector step: time_step's new dt, current_time += dt
 // (time_integration.f90:179, using the dt computed at the end of the step),
 // and the new hsml bounds.
-__global__ void k_step_finish(Scalars *sc, int tse, int sle) {
-    if (tse == 2) {
-        sc->dt = bitsd(sc->acc_dt);
-        sc->acc_dt = dbits(INFINITY);
+// (One basin per context when tse = 2 or sle = 2: instance 0 carries its
+// hsml bounds.)  Every instance's current_time advances by the same dt.
+constexpr int kFinishThreads = 256;
+__global__ void __launch_bounds__(kFinishThreads) k_step_finish(Scalars *sc, Inst *inst, int ninst, int tse,
+                                                                int sle) {
+    __shared__ double dt;
+    if (threadIdx.x == 0) {
+        if (tse == 2) {
+            sc->dt = bitsd(sc->acc_dt);
+            sc->acc_dt = dbits(INFINITY);
+        }
+        dt = sc->dt;
+        sc->t = sc->t + dt;
+        if (sle == 2) {
+            sc->hmin = bitsd(sc->acc_hmin);
+            sc->hmax = fmax(sc->hmax, bitsd(sc->acc_hmax));
+            sc->bs = 2.0 * sc->hmin;
+            sc->acc_hmin = dbits(INFINITY);
+            sc->acc_hmax = 0ull;
+            inst[0].hmin = sc->hmin;
+            inst[0].hmax = sc->hmax;
+            inst[0].bs = sc->bs;
+        }
     }
-    sc->t = sc->t + sc->dt;
-    if (sle == 2) {
-        sc->hmin = bitsd(sc->acc_hmin);
-        sc->hmax = fmax(sc->hmax, bitsd(sc->acc_hmax));
-        sc->bs = 2.0 * sc->hmin;
-        sc->acc_hmin = dbits(INFINITY);
-        sc->acc_hmax = 0ull;
-    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < ninst; k += kFinishThreads) inst[k].t = inst[k].t + dt;
 }
 
 __global__ void k_reset_stats(Scalars *sc) {
@@ -573,7 +671,9 @@ PairList pair_list(simp_ctx *c) {
 void launch_kinematic(simp_ctx *c, const State &s, bool diag) {
     KinArgs a;
     a.s = s;
-    a.g = c->grid;
+    a.cell_start = c->cell_start;
+    a.inst = c->inst_dev;
+    a.pinst = c->pinst;
     a.cell = c->cell;
     a.P = c->phys;
     a.sc = c->sc;
@@ -586,7 +686,10 @@ void launch_kinematic(simp_ctx *c, const State &s, bool diag) {
     a.pl = pair_list(c);
     a.n = c->n;
     a.maxn = c->maxn;
-    k_kinematic<<<nblk(c->n, kBlock), kBlock, 0, c->stream>>>(a);
+    if (c->prm.precision == SIMP_PREC_MIXED)
+        k_kinematic<float><<<nblk(c->n, kBlock), kBlock, 0, c->stream>>>(a);
+    else
+        k_kinematic<double><<<nblk(c->n, kBlock), kBlock, 0, c->stream>>>(a);
     c->launches += 1;
 }
 
@@ -595,7 +698,9 @@ void launch_stress(simp_ctx *c, const State &rhs, const State &base, EpiMode mod
     a.rhs = rhs;
     a.base = base;
     a.out = (mode == EPI_PREDICT) ? c->s1 : c->s0;
-    a.g = c->grid;
+    a.cell_start = c->cell_start;
+    a.inst = c->inst_dev;
+    a.pinst = c->pinst;
     a.cell = c->cell;
     a.bx = c->bx;
     a.by = c->by;
@@ -617,7 +722,10 @@ void launch_stress(simp_ctx *c, const State &rhs, const State &base, EpiMode mod
     a.n = c->n;
     a.maxn = c->maxn;
     a.mode = mode;
-    k_stress<<<nblk(c->n, kBlock), kBlock, 0, c->stream>>>(a);
+    if (c->prm.precision == SIMP_PREC_MIXED)
+        k_stress<float><<<nblk(c->n, kBlock), kBlock, 0, c->stream>>>(a);
+    else
+        k_stress<double><<<nblk(c->n, kBlock), kBlock, 0, c->stream>>>(a);
     c->launches += 1;
 }
 
@@ -626,7 +734,7 @@ void launch_step_finish(simp_ctx *c) {
         k_commit_hsml<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->n, c->tmp, c->s0.hs, c->s0.hsf);
         c->launches += 1;
     }
-    k_step_finish<<<1, 1, 0, c->stream>>>(c->sc, c->prm.tse, c->prm.sle);
+    k_step_finish<<<1, kFinishThreads, 0, c->stream>>>(c->sc, c->inst_dev, c->ninst, c->prm.tse, c->prm.sle);
     c->launches += 1;
 }
 

@@ -49,6 +49,23 @@ class SimpParams(ctypes.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class SimpForcing(ctypes.Structure):
+    """Per-basin forcing of a batch (``simp_forcing`` in include/simp_gpu.h)."""
+    _fields_ = [("wind_kind", ctypes.c_int32), ("reserved0", ctypes.c_int32),
+                ("wind_u", ctypes.c_double), ("wind_v", ctypes.c_double),
+                ("vortex_x", ctypes.c_double), ("vortex_y", ctypes.c_double),
+                ("vortex_umax", ctypes.c_double), ("vortex_radius", ctypes.c_double)]
+
+    @classmethod
+    def of(cls, p: "SimpParams") -> "SimpForcing":
+        """The forcing a parameter set describes (its wind fields)."""
+        f = cls()
+        for name, _ in cls._fields_:
+            if name != "reserved0":
+                setattr(f, name, getattr(p, name))
+        return f
+
+
 def _real4(v: float) -> float:
     """Value of a Fortran default-real (single precision) literal."""
     return struct.unpack("f", struct.pack("f", v))[0]

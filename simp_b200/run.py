@@ -33,9 +33,14 @@ def main():
     ap.add_argument("--workload", default="cfg2")
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--chunk", type=int, default=0, help="steps per call (0: all in one call)")
+    ap.add_argument("--precision", choices=("fp64", "mixed"), default=None,
+                    help="override the workload's precision")
     args = ap.parse_args()
     b = workload(args.workload)
-    sim = Simp.from_basin(b)
+    prm = b.params.copy()
+    if args.precision:
+        prm.precision = 1 if args.precision == "mixed" else 0
+    sim = Simp.from_basin(b, prm)
     t0 = time.perf_counter()
     done = 0
     chunk = args.chunk or args.steps

@@ -15,7 +15,7 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from .params import SimpParams
+from .params import SimpForcing, SimpParams
 
 SIMP_OK = 0
 SIMP_ERR_BADARG = 1
@@ -169,6 +169,97 @@ class Simp:
 
     def predictor_corrector(self):
         return self.time_integration(1)
+
+
+class Batch:
+    """A batch of resident basins stepped together (one launch per kernel per
+    sub-step for the whole batch).
+
+    Every basin keeps its own grid, forcing, current_time and re-sort
+    schedule, so its trajectory is bitwise the same alone or in any mix.
+    Basins join with ``add`` (returns a slot) and leave with ``remove``.
+    The batch shares one parameter set with a fixed time step (tse = 0) and
+    fixed smoothing lengths (sle = 0).
+    """
+
+    def __init__(self, params: SimpParams, maxn: int, maxnb: int, max_instances: int):
+        self.lib = _lib.load()
+        self.params = params.copy()
+        h = ctypes.c_void_p()
+        rc = self.lib.simp_gpu_create_batch(ctypes.byref(self.params), int(maxn), int(maxnb),
+                                            int(max_instances), ctypes.byref(h))
+        self.h = h.value
+        if rc != SIMP_OK:
+            msg = self.lib.simp_gpu_last_error(self.h).decode() if self.h else "create failed"
+            self.close()
+            raise SimpError(rc, msg)
+        self.sizes: dict[int, int] = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.simp_gpu_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, rc: int):
+        if rc != SIMP_OK:
+            raise SimpError(rc, self.lib.simp_gpu_last_error(self.h).decode())
+
+    def add(self, b, forcing: SimpForcing | None = None) -> int:
+        """Admit basin ``b`` (a ``Basin``); returns its slot."""
+        f = SimpForcing.of(b.params) if forcing is None else forcing
+        n, nb = b.n, b.nb
+        arrs = (_f64(b.x, (n, 2)), _f64(b.vx, (n, 2)), _f64(b.mass), _f64(b.rho), _f64(b.hsml),
+                _f64(b.A), _f64(b.h), _f64(b.xb, (nb, 2)) if nb else np.zeros((1, 2)),
+                _f64(b.massb) if nb else np.zeros(1))
+        p = [_lib.dptr(a) for a in arrs]
+        slot = ctypes.c_int32()
+        self._chk(self.lib.simp_gpu_batch_add(self.h, ctypes.byref(f), n, *p[:7], nb, p[7], p[8],
+                                              ctypes.byref(slot)))
+        self.sizes[slot.value] = n
+        return slot.value
+
+    def remove(self, slot: int):
+        self._chk(self.lib.simp_gpu_batch_remove(self.h, int(slot)))
+        self.sizes.pop(int(slot), None)
+
+    def get_state(self, slot: int) -> dict:
+        n = self.sizes[int(slot)]
+        out = {"x": np.zeros((n, 2)), "vx": np.zeros((n, 2))}
+        for k in ("mass", "rho", "hsml", "A", "h"):
+            out[k] = np.zeros(n)
+        t = ctypes.c_double()
+        self._chk(self.lib.simp_gpu_batch_get_state(self.h, int(slot), *[_lib.dptr(out[k]) for k in
+                                                                        ("x", "vx", "mass", "rho", "hsml",
+                                                                         "A", "h")], ctypes.byref(t)))
+        out["current_time"] = t.value
+        return out
+
+    def info(self, slot: int) -> dict:
+        n, fl = ctypes.c_int32(), ctypes.c_int32()
+        st = ctypes.c_int64()
+        self._chk(self.lib.simp_gpu_batch_info(self.h, int(slot), ctypes.byref(n), ctypes.byref(st),
+                                               ctypes.byref(fl)))
+        return dict(ntotal=n.value, steps=st.value, flags=fl.value)
+
+    def step(self, nsteps: int = 1):
+        """nsteps predictor-corrector steps of every basin in the batch."""
+        t, dt = ctypes.c_double(), ctypes.c_double()
+        self._chk(self.lib.simp_gpu_step(self.h, int(nsteps), ctypes.byref(t), ctypes.byref(dt)))
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.simp_gpu_kernel_launches(self.h))
 
 
 def version() -> str:
