@@ -43,6 +43,10 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="target CPU time of the oracle baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--forms", default="mixed,batched,served",
+                    help="comma list of the other forms to measure on rank 0 ('' for none)")
+    ap.add_argument("--served-requests", type=int, default=32)
+    ap.add_argument("--served-steps-scale", type=float, default=0.25)
     return ap.parse_args()
 
 
@@ -207,13 +211,15 @@ def run_ours(args):
         dist.barrier()
     clk = clocks.stop()
     launches = lib.simp_gpu_kernel_launches(sim.h) - launches0
-    kms = (ctypes.c_double * 5)()
+    kms = (ctypes.c_double * 6)()
     nst = ctypes.c_int64()
-    lib.simp_gpu_kernel_times(sim.h, kms, 5, ctypes.byref(nst))
+    lib.simp_gpu_kernel_times(sim.h, kms, 6, ctypes.byref(nst))
     lib.simp_gpu_profile(sim.h, 0)
-    kernel_ms = list(kms)
-    # device time of the K steps: sum of in-graph kernel times per step
-    dev_ms = sum(kernel_ms)
+    kernel_ms = list(kms)[:5]
+    sort_ms = kms[5]
+    # device time of the K steps: the in-graph kernel times of every step
+    # plus the re-sorts between steps
+    dev_ms = sum(kernel_ms) + sort_ms
     outer_ms = sum(a.elapsed_time(z) for a, z in zip(ev0, ev1))
     dev_ms_max = job_time_ms(dist, dev_ms)
     value = job_value(world, b.n, args.steps, dev_ms_max)
@@ -238,6 +244,9 @@ def run_ours(args):
                "sample": f"first {steps} predictor-corrector steps of the same 262,144-particle basin "
                          f"({el:.1f} s), C++ FP64 restatement of the reference, OpenMP threads={threads}"}
     sim.close()
+    forms = None
+    if rank == 0 and args.forms:
+        forms = run_forms(args, [f for f in args.forms.split(",") if f])
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -252,17 +261,119 @@ def run_ours(args):
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "alg_bytes_per_launch": alg, "avg_launch_ms": avg_ms,
                          "step_alg_bytes_per_particle": roofline.STEP_BYTES_PER_PARTICLE,
-                         "kernel_ms_per_step": {n: kernel_ms[k] / max(1, nst.value) for k, n in enumerate(names)}},
+                         "kernel_ms_per_step": {**{n: kernel_ms[k] / max(1, nst.value) for k, n in enumerate(names)},
+                                                "sort": sort_ms / max(1, nst.value)}},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(launches),
             "clocks": clk,
+            "forms": forms,
         }
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+# --- the other forms: mixed single instance, batched ensemble, served stream -
+
+def _device_steps(sim_step, stream, nsteps):
+    """Device time (ms) of nsteps steps issued by sim_step(k) in one call."""
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    sim_step(nsteps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def run_forms(args, which):
+    import numpy as np
+    import torch
+    from simp_b200 import basins, serve
+    from simp_b200.params import PREC_FP64, PREC_MIXED
+    from simp_b200.simp import Batch, Simp
+    out = {}
+    if "mixed" in which:
+        # 1,048,576-particle vortex basin, mixed precision, against FP64 on
+        # the same seed: one right-hand side and a 3-step trajectory
+        b = basins.cfg3()
+        b.vx = basins.smooth_velocity(b.x, b.L, amp=0.3, seed=14)   # not at rest: the rheology is live
+        p64 = b.params.copy()
+        p64.precision = PREC_FP64
+        g32 = Simp.from_basin(b)
+        g64 = Simp.from_basin(b, p64)
+        r32, r64 = g32.single_step(600.0), g64.single_step(600.0)
+        rel = lambda a, c: float(np.linalg.norm(a - c) / max(np.linalg.norm(c), 1e-300))
+        err_rhs = {k: rel(r32[k], r64[k]) for k in ("dvxdt", "dhdt")}
+        res = {}
+        for name, g in (("mixed", g32), ("fp64", g64)):
+            g.set_state(b.x, b.vx, b.mass, b.rho, b.hsml, b.A, b.h, b.xb, b.massb, b.params.dt, 0.0)
+            g.time_integration(args.warmup)
+            st = torch.cuda.ExternalStream(g.lib.simp_gpu_stream(g.h))
+            ms = _device_steps(g.time_integration, st, args.steps)
+            res[name] = {"value": b.n * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps}
+        g32.set_state(b.x, b.vx, b.mass, b.rho, b.hsml, b.A, b.h, b.xb, b.massb, b.params.dt, 0.0)
+        g64.set_state(b.x, b.vx, b.mass, b.rho, b.hsml, b.A, b.h, b.xb, b.massb, b.params.dt, 0.0)
+        g32.time_integration(50)
+        g64.time_integration(50)
+        s32, s64 = g32.get_state(), g64.get_state()
+        g32.close()
+        g64.close()
+        out["mixed_single_instance"] = {
+            "workload": "1,048,576 particles (1024x1024, dx=250 m), 4 walls, vortex 15 m/s, smoothed h/A, dt=1e-5 s",
+            "metric": METRIC, "value": res["mixed"]["value"], "ms_per_step": res["mixed"]["ms_per_step"],
+            "fp64_same_basin": res["fp64"], "steps": args.steps,
+            "l2": "not flushed: one call of K steps; per-step working set > 126 MB L2",
+            "err_vs_fp64": {"rhs_rel_l2": err_rhs,
+                            "traj50_rel_l2": {k: rel(s32[k], s64[k]) for k in ("vx", "h")}}}
+    if "batched" in which:
+        # 64 uneven basins (log-uniform 4,096..262,144 particles), mixed
+        bs = basins.cfg4(64, steps=500)
+        ntot = sum(x.n for x in bs)
+        with Batch(bs[0].params, ntot, sum(x.nb for x in bs), 64) as bt:
+            for x in bs:
+                bt.add(x)
+            bt.step(args.warmup)
+            st = torch.cuda.ExternalStream(bt.lib.simp_gpu_stream(bt.h))
+            l0 = bt.kernel_launches()
+            ms = _device_steps(bt.step, st, args.steps)
+            launches = bt.kernel_launches() - l0
+        out["batched_ensemble"] = {
+            "workload": f"64 basins, {ntot} particles (log-uniform 4,096..262,144), dx=1 km, mixed, dt=1e-4 s",
+            "metric": METRIC, "value": ntot * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
+            "steps": args.steps, "launches_per_step": launches / args.steps,
+            "l2": "not flushed: one call of K steps; working set > 126 MB L2"}
+    if "served" in which:
+        reqs = serve.sample_stream(args.served_requests, seed=5, rate_hz=20.0,
+                                   steps_scale=args.served_steps_scale)
+        big = max(r.basin.n for r in reqs)
+        with serve.Server(reqs[0].basin.params, 150e9, max_instances=256, max_request_particles=big,
+                          quantum_steps=16, spot_every=8) as srv:
+            ids = [srv.submit(r) for r in reqs]
+            srv.run()
+            sst = srv.stats()
+            per = [srv.request(i) for i in ids]
+        lat = [q["completed_s"] - q["arrival_s"] for q in per]
+        spots = [{"n": q["ntotal"], "steps": q["steps"], "err_v": q["err_v"], "err_h": q["err_h"]}
+                 for q in per if q["spot_checked"]]
+        ser = serve.serial_fp64(reqs)
+        served_value = sst["particle_steps"] / sst["makespan_s"]
+        out["served_stream"] = {
+            "workload": (f"{len(reqs)} requests, Poisson 20/s, particles log-uniform 1,024..1,048,576, "
+                         f"steps U(100, 2000) x {args.served_steps_scale}, dx=1 km, dt=1e-4 s, mixed, "
+                         "HBM budget 150 GB, FP64 replica of every 8th request"),
+            "metric": METRIC, "value": served_value, "p50_s": float(np.percentile(lat, 50)),
+            "p99_s": float(np.percentile(lat, 99)), "makespan_s": sst["makespan_s"],
+            "particle_steps": sst["particle_steps"], "peak_resident_requests": sst["peak_resident_requests"],
+            "peak_resident_particles": sst["peak_resident_particles"],
+            "serial_fp64": ser, "speedup_vs_serial_fp64": served_value / ser["value"],
+            "spot_checks": spots}
+    return out
 
 
 def profile_traffic(kernel: str):

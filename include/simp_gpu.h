@@ -202,6 +202,11 @@ typedef struct simp_forcing {
     double vortex_x, vortex_y, vortex_umax, vortex_radius;
 } simp_forcing;
 
+/* Forcing of a single-basin context (the wind fields of its simp_params),
+ * used from the next simp_gpu_set_state on and by the basin already set.
+ * The reference hard-codes its wind (wind_forcing.f90:36-37). */
+SIMP_API int32_t simp_gpu_set_forcing(simp_ctx *ctx, const simp_forcing *forcing);
+
 /* maxn / maxnb: particle and wall capacities over all instances; at most
  * 2,097,151 particles per instance; max_instances <= 1024. */
 SIMP_API int32_t simp_gpu_create_batch(const simp_params *params, int32_t maxn, int32_t maxnb,
@@ -261,8 +266,9 @@ SIMP_API int64_t simp_gpu_kernel_launches(const simp_ctx *ctx);
 /* Per-kernel timing of simp_gpu_step: when on, CUDA events recorded inside
  * the step graph time each kernel of every step; simp_gpu_kernel_times then
  * returns, for the n_kernels kernels of a step (kinematic, stress-predict,
- * kinematic, stress-correct, step-finish), the summed milliseconds and the
- * number of steps timed.  No reference counterpart. */
+ * kinematic, stress-correct, step-finish) and, as a sixth entry, the
+ * re-sorts between steps, the summed milliseconds and the number of steps
+ * timed.  No reference counterpart. */
 SIMP_API int32_t simp_gpu_profile(simp_ctx *ctx, int32_t on);
 SIMP_API int32_t simp_gpu_kernel_times(simp_ctx *ctx, double *ms, int32_t n_kernels,
                                        int64_t *steps_timed);

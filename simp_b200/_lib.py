@@ -8,7 +8,7 @@ from __future__ import annotations
 import ctypes
 import os
 
-from .params import SimpForcing, SimpParams
+from .params import RequestStats, ServerConfig, ServerStats, SimpForcing, SimpParams
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsimp_gpu.so")
@@ -27,6 +27,7 @@ SIGNATURES = {
     "simp_gpu_batch_add": (_i32, [_vp, ctypes.POINTER(SimpForcing), _i32, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
                                   _i32, _dp, _dp, _ip]),
     "simp_gpu_batch_remove": (_i32, [_vp, _i32]),
+    "simp_gpu_set_forcing": (_i32, [_vp, ctypes.POINTER(SimpForcing)]),
     "simp_gpu_batch_get_state": (_i32, [_vp, _i32, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
     "simp_gpu_batch_info": (_i32, [_vp, _i32, _ip, ctypes.POINTER(ctypes.c_int64), _ip]),
     "simp_gpu_set_state": (_i32, [_vp, _i32, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _i32, _dp, _dp,
@@ -46,6 +47,16 @@ SIGNATURES = {
     "simp_gpu_kernel_times": (_i32, [_vp, _dp, _i32, ctypes.POINTER(ctypes.c_int64)]),
     "simp_gpu_last_error": (ctypes.c_char_p, [_vp]),
     "simp_gpu_version": (ctypes.c_char_p, []),
+    # include/simp_serve.h
+    "simp_server_create": (_i32, [ctypes.POINTER(SimpParams), ctypes.POINTER(ServerConfig), ctypes.POINTER(_vp)]),
+    "simp_server_destroy": (_i32, [_vp]),
+    "simp_server_submit": (_i32, [_vp, ctypes.POINTER(SimpForcing), _i32, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
+                                  _i32, _dp, _dp, ctypes.c_int64, ctypes.c_double, _dp, _dp, _dp, _dp,
+                                  ctypes.POINTER(ctypes.c_int64)]),
+    "simp_server_run": (_i32, [_vp]),
+    "simp_server_request": (_i32, [_vp, ctypes.c_int64, ctypes.POINTER(RequestStats)]),
+    "simp_server_stats_get": (_i32, [_vp, ctypes.POINTER(ServerStats)]),
+    "simp_server_last_error": (ctypes.c_char_p, [_vp]),
 }
 
 _lib = None

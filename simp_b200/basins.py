@@ -118,6 +118,17 @@ def make_basin(nside: int, dx: float, seed: int, *, name: str = "basin",
                  params=prm, steps=steps, meta={"seed": seed, "nside": nside})
 
 
+def smooth_velocity(x: np.ndarray, L: float, amp: float = 0.3, seed: int = 0) -> np.ndarray:
+    """A smooth, non-trivial velocity field (shear + divergence + rotation)
+    for exercising the rheology from a state not at rest."""
+    rng = np.random.default_rng(seed)
+    k = 2.0 * np.pi / L
+    p = rng.uniform(0, 2 * np.pi, size=4)
+    u = amp * (np.sin(k * x[:, 0] + p[0]) * np.cos(2 * k * x[:, 1] + p[1]) + 0.3)
+    v = amp * (np.cos(3 * k * x[:, 0] + p[2]) * np.sin(k * x[:, 1] + p[3]) - 0.2)
+    return np.ascontiguousarray(np.stack([u, v], axis=1))
+
+
 def _gauss_smooth(field2d: np.ndarray, sigma_cells: float) -> np.ndarray:
     from scipy.ndimage import gaussian_filter
     return gaussian_filter(field2d, sigma=sigma_cells, mode="nearest")
@@ -139,11 +150,21 @@ def cfg2(seed: int = 2) -> Basin:
                       wind=(10.0, 0.0), steps=1000)
 
 
-def cfg3(seed: int = 3, nside: int = 1024) -> Basin:
+# The reference's viscous-plastic time-step bound (time_step.f90:155):
+# dt <= rho_ice hsml^2 delta_min / (P_star (1 + k_t)), with hsml = 2.4 dx.
+# Above it the explicit scheme amplifies any rounding difference (a
+# reordered FP64 sum included) by a factor per step; below it mixed and FP64
+# trajectories stay close for thousands of steps.
+def vp_dt_bound(dx: float) -> float:
+    return RHO_ICE * (2.4 * dx) ** 2 * 2.0e-9 / 2.75e4
+
+
+def cfg3(seed: int = 3, nside: int = 1024, dt: float = 1.0e-5) -> Basin:
     """1,048,576 particles (1024x1024, dx = 250 m, 256 km), walls on four
     sides, cyclonic vortex wind of peak 15 m/s and radius 25 km centred in the
     middle 50% of the domain, h ~ U(0.5, 2), A ~ U(0.8, 1) smoothed with a
-    5 km Gaussian, 2,000 steps, mixed precision."""
+    5 km Gaussian, 2,000 steps, mixed precision.  dt = 1e-5 s, under the VP
+    bound (2.4e-5 s at dx = 250 m, halved for h up to 2)."""
     dx = 256000.0 / nside
     rng = np.random.default_rng(seed + 1000)
     L = nside * dx
@@ -155,15 +176,16 @@ def cfg3(seed: int = 3, nside: int = 1024) -> Basin:
     A = np.minimum(_gauss_smooth(A, sig).ravel(), 1.0)
     return make_basin(nside, dx, seed, name=f"cfg3_{nside * nside}", walls="+x-x+y-y",
                       vortex=(cx, cy, 15.0, 25000.0), h=h, A=A,
-                      precision=PREC_MIXED, steps=2000)
+                      precision=PREC_MIXED, steps=2000, dt=dt)
 
 
 def instance(k: int, n_target: int, dx: float = 1000.0, steps: int = 500,
-             precision: int = PREC_MIXED, seed_base: int = 4) -> Basin:
+             precision: int = PREC_MIXED, seed_base: int = 4, dt: float = 1.0e-4) -> Basin:
     """One basin of a batched ensemble or a served request: square lattice of
     about n_target particles, dx = 1 km, walls on four sides, uniform wind of
     speed U(5, 20) m/s and direction U(0, 2 pi), h ~ U(0.5, 2) m and
-    A ~ U(0.8, 1) drawn per instance."""
+    A ~ U(0.8, 1) drawn per instance.  dt = 1e-4 s, under the VP bound
+    (3.8e-4 s at dx = 1 km, halved for h up to 2)."""
     rng = np.random.default_rng(seed_base + k)
     nside = max(2, int(round(math.sqrt(n_target))))
     speed = rng.uniform(5.0, 20.0)
@@ -172,7 +194,7 @@ def instance(k: int, n_target: int, dx: float = 1000.0, steps: int = 500,
     Av = rng.uniform(0.8, 1.0)
     return make_basin(nside, dx, int(rng.integers(1 << 31)), name=f"inst{k}",
                       walls="+x-x+y-y", wind=(speed * math.cos(ang), speed * math.sin(ang)),
-                      h=hv, A=Av, precision=precision, steps=steps)
+                      h=hv, A=Av, precision=precision, steps=steps, dt=dt)
 
 
 def cfg4_sizes(count: int = 64, seed: int = 4, lo: int = 4096, hi: int = 262144):

@@ -183,6 +183,8 @@ void free_all(simp_ctx *c) {
     if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
     for (cudaEvent_t e : c->prof_ev)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : c->sort_ev)
+        if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -645,6 +647,90 @@ simp_forcing forcing_of(const simp_params &p) {
 
 }  // namespace
 
+namespace simp {
+
+// Enqueues nsteps steps of every basin of the context on its stream without
+// waiting for them (profiling mode waits step by step).
+int step_enqueue(simp_ctx *c, int nsteps) {
+    if (!c->have_state) return simp_fail(c, SIMP_ERR_STATE, "step before set_state");
+    cudaStream_t s = c->stream;
+    if (c->n == 0 || nsteps == 0) return SIMP_OK;   // (an empty batch)
+    bool regridded = false;
+    TRY(maybe_regrid(c, &regridded));
+    launch_reset_stats(c);
+    TRY(ensure_graph(c, c->keep_diag));
+    if (c->graph_profiled && !c->sort_ev[0])
+        for (auto &e : c->sort_ev) SIMP_CUDA(c, cudaEventCreate(&e));
+    for (int st = 0; st < nsteps; ++st) {
+        DueMask due{};
+        bool any = false;
+        for (int q = 0; q < c->max_inst; ++q) {
+            InstHost &h = c->insts[q];
+            if (h.active && h.steps_since_sort >= kSortEvery) {
+                due.w[q >> 6] |= 1ull << (q & 63);
+                h.steps_since_sort = 0;
+                any = true;
+            }
+        }
+        if (any) {
+            if (c->graph_profiled) SIMP_CUDA(c, cudaEventRecord(c->sort_ev[0], s));
+            TRY(maybe_regrid(c, &regridded));   // hsml grew past the grid (sle = 2)
+            if (regridded) TRY(ensure_graph(c, c->keep_diag));
+            else TRY(rebuild(c, due, false, false));
+            if (c->graph_profiled) {
+                SIMP_CUDA(c, cudaEventRecord(c->sort_ev[1], s));
+                SIMP_CUDA(c, cudaEventSynchronize(c->sort_ev[1]));
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, c->sort_ev[0], c->sort_ev[1]);
+                c->prof_ms[simp_ctx::kProfKernels] += ms;
+            }
+        }
+        cudaError_t e = cudaGraphLaunch(c->step_graph, s);
+        if (e != cudaSuccess) return simp_cuda_check(c, e, "cudaGraphLaunch");
+        c->launches += c->graph_kernels;
+        c->lists_valid = true;
+        for (InstHost &h : c->insts)
+            if (h.active) {
+                ++h.steps_since_sort;
+                ++h.steps_done;
+            }
+        if (c->graph_profiled) {
+            // timing mode: wait for this step and add up its kernel times
+            e = cudaEventSynchronize(c->prof_ev[simp_ctx::kProfKernels]);
+            if (e != cudaSuccess) return simp_cuda_check(c, e, "profile event");
+            for (int k = 0; k < simp_ctx::kProfKernels; ++k) {
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, c->prof_ev[k], c->prof_ev[k + 1]);
+                c->prof_ms[k] += ms;
+            }
+            c->prof_steps += 1;
+        }
+    }
+    return SIMP_OK;
+}
+
+// Waits for the enqueued steps and checks the step's status.
+int step_complete(simp_ctx *c, double *current_time, double *dt) {
+    if (!c->have_state) return simp_fail(c, SIMP_ERR_STATE, "step before set_state");
+    if (c->n == 0) {
+        if (current_time) *current_time = 0.0;
+        if (dt) *dt = c->prm.dt;
+        return SIMP_OK;
+    }
+    SIMP_CUDA(c, cudaStreamSynchronize(c->stream));
+    TRY(read_scalars(c));
+    if (current_time) *current_time = c->sc_host->t;
+    if (dt) *dt = c->sc_host->dt;
+    return check_after(c);
+}
+
+int batch_slot_state(simp_ctx *c, int slot, double *x, double *vx, double *mass, double *rho, double *hsml,
+                     double *A, double *h, double *t) {
+    return get_instance_state(c, slot, x, vx, mass, rho, hsml, A, h, t);
+}
+
+}  // namespace simp
+
 extern "C" {
 
 const char *simp_gpu_version(void) { return "simp_b200 0.2 (sm_100a)"; }
@@ -785,6 +871,33 @@ int32_t simp_gpu_batch_add(simp_ctx *c, const simp_forcing *forcing, int32_t nto
     return SIMP_OK;
 }
 
+int32_t simp_gpu_set_forcing(simp_ctx *c, const simp_forcing *f) {
+    if (!c || !f) return SIMP_ERR_BADARG;
+    if (c->max_inst != 1) return simp_fail(c, SIMP_ERR_BADARG, "set_forcing is for single-basin contexts");
+    if (f->wind_kind != SIMP_WIND_UNIFORM && f->wind_kind != SIMP_WIND_VORTEX)
+        return simp_fail(c, SIMP_ERR_BADARG, "unknown wind_kind");
+    c->prm.wind_kind = f->wind_kind;
+    c->prm.wind_u = f->wind_u;
+    c->prm.wind_v = f->wind_v;
+    c->prm.vortex_x = f->vortex_x;
+    c->prm.vortex_y = f->vortex_y;
+    c->prm.vortex_umax = f->vortex_umax;
+    c->prm.vortex_radius = f->vortex_radius;
+    InstHost &h = c->insts[0];
+    if (h.active) {
+        Inst &I = h.I;
+        I.wind_kind = f->wind_kind;
+        I.wind_u = f->wind_u;
+        I.wind_v = f->wind_v;
+        I.vortex_x = f->vortex_x;
+        I.vortex_y = f->vortex_y;
+        I.vortex_umax = f->vortex_umax;
+        I.vortex_radius = f->vortex_radius;
+        TRY(layout(c));
+    }
+    return SIMP_OK;
+}
+
 int32_t simp_gpu_batch_remove(simp_ctx *c, int32_t slot) {
     if (!c || slot < 0 || slot >= c->max_inst) return SIMP_ERR_BADARG;
     return remove_instance(c, slot);
@@ -896,59 +1009,8 @@ int32_t simp_gpu_sum_density(simp_ctx *c, double *rho_out) {
 // between the device-side stencil radius keeps the cell list exact.
 int32_t simp_gpu_step(simp_ctx *c, int32_t nsteps, double *current_time, double *dt) {
     if (!c || nsteps < 0) return SIMP_ERR_BADARG;
-    if (!c->have_state) return simp_fail(c, SIMP_ERR_STATE, "step before set_state");
-    cudaStream_t s = c->stream;
-    if (c->n == 0) {   // an empty batch
-        if (current_time) *current_time = 0.0;
-        if (dt) *dt = c->prm.dt;
-        return SIMP_OK;
-    }
-    bool regridded = false;
-    TRY(maybe_regrid(c, &regridded));
-    launch_reset_stats(c);
-    TRY(ensure_graph(c, c->keep_diag));
-    for (int st = 0; st < nsteps; ++st) {
-        DueMask due{};
-        bool any = false;
-        for (int q = 0; q < c->max_inst; ++q) {
-            InstHost &h = c->insts[q];
-            if (h.active && h.steps_since_sort >= kSortEvery) {
-                due.w[q >> 6] |= 1ull << (q & 63);
-                h.steps_since_sort = 0;
-                any = true;
-            }
-        }
-        if (any) {
-            TRY(maybe_regrid(c, &regridded));   // hsml grew past the grid (sle = 2)
-            if (regridded) TRY(ensure_graph(c, c->keep_diag));
-            else TRY(rebuild(c, due, false, false));
-        }
-        cudaError_t e = cudaGraphLaunch(c->step_graph, s);
-        if (e != cudaSuccess) return simp_cuda_check(c, e, "cudaGraphLaunch");
-        c->launches += c->graph_kernels;
-        c->lists_valid = true;
-        for (InstHost &h : c->insts)
-            if (h.active) {
-                ++h.steps_since_sort;
-                ++h.steps_done;
-            }
-        if (c->graph_profiled) {
-            // timing mode: wait for this step and add up its kernel times
-            e = cudaEventSynchronize(c->prof_ev[simp_ctx::kProfKernels]);
-            if (e != cudaSuccess) return simp_cuda_check(c, e, "profile event");
-            for (int k = 0; k < simp_ctx::kProfKernels; ++k) {
-                float ms = 0.0f;
-                cudaEventElapsedTime(&ms, c->prof_ev[k], c->prof_ev[k + 1]);
-                c->prof_ms[k] += ms;
-            }
-            c->prof_steps += 1;
-        }
-    }
-    SIMP_CUDA(c, cudaStreamSynchronize(s));
-    TRY(read_scalars(c));
-    if (current_time) *current_time = c->sc_host->t;
-    if (dt) *dt = c->sc_host->dt;
-    return check_after(c);
+    TRY(simp::step_enqueue(c, nsteps));
+    return simp::step_complete(c, current_time, dt);
 }
 
 void *simp_gpu_stream(simp_ctx *c) { return c ? (void *)c->stream : nullptr; }
@@ -965,7 +1027,7 @@ int32_t simp_gpu_profile(simp_ctx *c, int32_t on) {
 
 int32_t simp_gpu_kernel_times(simp_ctx *c, double *ms, int32_t n_kernels, int64_t *steps_timed) {
     if (!c || !ms || n_kernels < 0) return SIMP_ERR_BADARG;
-    for (int k = 0; k < n_kernels; ++k) ms[k] = (k < simp_ctx::kProfKernels) ? c->prof_ms[k] : 0.0;
+    for (int k = 0; k < n_kernels; ++k) ms[k] = (k <= simp_ctx::kProfKernels) ? c->prof_ms[k] : 0.0;
     if (steps_timed) *steps_timed = c->prof_steps;
     return SIMP_OK;
 }

@@ -92,10 +92,12 @@ struct simp_ctx {
     long long graph_kernels = 0;   // kernels per replay
     long long launches = 0;        // kernels launched by this context
     // per-kernel timing (events recorded inside the step graph)
+    // (entry kProfKernels of prof_ms: the re-sorts between steps)
     static constexpr int kProfKernels = 5;
     bool profile = false;
     cudaEvent_t prof_ev[kProfKernels + 1] = {};
-    double prof_ms[kProfKernels] = {};
+    cudaEvent_t sort_ev[2] = {};
+    double prof_ms[kProfKernels + 1] = {};
     long long prof_steps = 0;
     long long rebuilds = 0;
 };
@@ -123,6 +125,12 @@ void launch_kinematic(simp_ctx *c, const State &s, bool diag);
 void launch_stress(simp_ctx *c, const State &nb, const State &own, EpiMode mode);
 void launch_step_finish(simp_ctx *c);
 void launch_reset_stats(simp_ctx *c);
+
+// abi.cu: the step driver split for callers that overlap contexts
+int step_enqueue(simp_ctx *c, int nsteps);
+int step_complete(simp_ctx *c, double *current_time, double *dt);
+int batch_slot_state(simp_ctx *c, int slot, double *x, double *vx, double *mass, double *rho, double *hsml,
+                     double *A, double *h, double *t);
 
 // nnps_export.cu (instance 0 of the context)
 int export_pairs(simp_ctx *c, int32_t *nip, int32_t *p_i, int32_t *p_j, double *r_ij,

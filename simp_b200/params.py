@@ -66,6 +66,30 @@ class SimpForcing(ctypes.Structure):
         return f
 
 
+class ServerConfig(ctypes.Structure):
+    """``simp_server_config`` (include/simp_serve.h)."""
+    _fields_ = [("hbm_budget_bytes", ctypes.c_double), ("max_instances", ctypes.c_int32),
+                ("max_request_particles", ctypes.c_int32), ("quantum_steps", ctypes.c_int32),
+                ("spot_every", ctypes.c_int32)]
+
+
+class RequestStats(ctypes.Structure):
+    """``simp_request_stats`` (include/simp_serve.h)."""
+    _fields_ = [("arrival_s", ctypes.c_double), ("admitted_s", ctypes.c_double),
+                ("completed_s", ctypes.c_double), ("steps", ctypes.c_int64), ("ntotal", ctypes.c_int32),
+                ("status", ctypes.c_int32), ("spot_checked", ctypes.c_int32), ("reserved0", ctypes.c_int32),
+                ("err_v", ctypes.c_double), ("err_h", ctypes.c_double)]
+
+
+class ServerStats(ctypes.Structure):
+    """``simp_server_stats`` (include/simp_serve.h)."""
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
+                ("particle_steps", ctypes.c_int64), ("batch_steps", ctypes.c_int64),
+                ("peak_resident_particles", ctypes.c_int64), ("peak_resident_requests", ctypes.c_int32),
+                ("reserved0", ctypes.c_int32), ("makespan_s", ctypes.c_double),
+                ("capacity_particles", ctypes.c_double)]
+
+
 def _real4(v: float) -> float:
     """Value of a Fortran default-real (single precision) literal."""
     return struct.unpack("f", struct.pack("f", v))[0]

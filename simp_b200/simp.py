@@ -114,6 +114,13 @@ class Simp:
         out["dt"], out["current_time"] = dt.value, t.value
         return out
 
+    def set_forcing(self, forcing: SimpForcing):
+        """Wind of this basin (and of later set_state calls)."""
+        self._chk(self.lib.simp_gpu_set_forcing(self.h, ctypes.byref(forcing)))
+        for name, _ in SimpForcing._fields_:
+            if name != "reserved0":
+                setattr(self.params, name, getattr(forcing, name))
+
     def keep_diag(self, keep: bool = True):
         self._chk(self.lib.simp_gpu_keep_diag(self.h, 1 if keep else 0))
 

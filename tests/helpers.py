@@ -49,9 +49,5 @@ def rel_l2(a, b) -> float:
 
 def smooth_velocity(x: np.ndarray, L: float, amp: float = 0.3, seed: int = 0) -> np.ndarray:
     """A smooth, non-trivial velocity field (shear + divergence + rotation)."""
-    rng = np.random.default_rng(seed)
-    k = 2.0 * np.pi / L
-    p = rng.uniform(0, 2 * np.pi, size=4)
-    u = amp * (np.sin(k * x[:, 0] + p[0]) * np.cos(2 * k * x[:, 1] + p[1]) + 0.3)
-    v = amp * (np.cos(3 * k * x[:, 0] + p[2]) * np.sin(k * x[:, 1] + p[3]) - 0.2)
-    return np.ascontiguousarray(np.stack([u, v], axis=1))
+    from simp_b200.basins import smooth_velocity as sv
+    return sv(x, L, amp=amp, seed=seed)

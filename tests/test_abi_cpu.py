@@ -10,11 +10,11 @@ from simp_b200 import _lib, build
 from simp_b200.params import SimpParams, reference_default
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-HEADER = os.path.join(ROOT, "include", "simp_gpu.h")
+HEADERS = [os.path.join(ROOT, "include", h) for h in ("simp_gpu.h", "simp_serve.h")]
 
 
 def declared_symbols():
-    txt = open(HEADER).read()
+    txt = "".join(open(h).read() for h in HEADERS)
     return sorted(set(re.findall(r"SIMP_API\s+[\w\s\*]*?\b(simp_\w+)\s*\(", txt)))
 
 
@@ -46,6 +46,30 @@ def test_params_layout_matches_c(tmp_path):
     assert int(out["sizeof"]) == ctypes.sizeof(SimpParams)
     for f in fields:
         assert int(out[f]) == getattr(SimpParams, f).offset, f
+
+
+@pytest.mark.parametrize("cname,pyname,header", [
+    ("simp_forcing", "SimpForcing", "simp_gpu.h"),
+    ("simp_server_config", "ServerConfig", "simp_serve.h"),
+    ("simp_request_stats", "RequestStats", "simp_serve.h"),
+    ("simp_server_stats", "ServerStats", "simp_serve.h"),
+])
+def test_struct_layouts_match_c(tmp_path, cname, pyname, header):
+    from simp_b200 import params as P
+    cls = getattr(P, pyname)
+    fields = [f for f, _ in cls._fields_]
+    src = tmp_path / "layout.c"
+    body = "\n".join(f'    printf("%s %zu\\n", "{f}", offsetof({cname}, {f}));' for f in fields)
+    src.write_text(f'#include <stddef.h>\n#include <stdio.h>\n#include "{header}"\nint main(void){{\n'
+                   f'    printf("sizeof %zu\\n", sizeof({cname}));\n{body}\n    return 0;\n}}\n')
+    exe = tmp_path / "layout"
+    cc = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else "gcc"
+    subprocess.run([cc, "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                        check=True).stdout.splitlines())
+    assert int(out["sizeof"]) == ctypes.sizeof(cls)
+    for f in fields:
+        assert int(out[f]) == getattr(cls, f).offset, f
 
 
 def test_fortran_mirror_field_order():

@@ -5,6 +5,8 @@ Tolerances: one right-hand side on identical inputs within 2e-6 relative L2
 (FP32 rounding of the kernel gradient and of the pair terms, compensated
 sums); velocity and thickness within 1e-4 relative L2 after 20 steps.
 """
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -117,3 +119,54 @@ def test_mixed_short_trajectory_at_scale(gpu_lib):
         e = rel_l2(s32[k], s64[k])
         assert e < TOL_MIXED_TRAJ, (k, e)
     assert np.array_equal(s32["mass"], s64["mass"])
+
+
+def _permuted(b, seed):
+    """The same basin with its particles listed in another order (the pair
+    sums then run in another order; the physics is unchanged)."""
+    perm = np.random.default_rng(seed).permutation(b.n)
+    c = dataclasses.replace(b, **{k: np.ascontiguousarray(getattr(b, k)[perm])
+                                  for k in ("x", "vx", "mass", "rho", "hsml", "A", "h")})
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(b.n)
+    return c, inv
+
+
+def test_mixed_full_length_under_vp_bound(gpu_lib):
+    """A served-size basin for 2,000 steps at dt = 1e-4 s (under the
+    reference's viscous-plastic bound, time_step.f90:155): velocity and
+    thickness within 1e-4 of FP64 at every checkpoint."""
+    b = basins.instance(3, 16384)
+    assert b.params.dt < basins.vp_dt_bound(1000.0) / 2
+    p64 = b.params.copy()
+    p64.precision = 0
+    g32, g64 = Simp.from_basin(b), Simp.from_basin(b, p64)
+    done = 0
+    for mark in (50, 500, 2000):
+        g32.time_integration(mark - done)
+        g64.time_integration(mark - done)
+        done = mark
+        s32, s64 = g32.get_state(), g64.get_state()
+        for k in ("vx", "h"):
+            e = rel_l2(s32[k], s64[k])
+            assert e < TOL_MIXED_TRAJ, (mark, k, e)
+
+
+def test_mixed_error_at_fp64_reorder_floor_above_vp_bound(gpu_lib):
+    """dt = 1 s, 100 steps: FP64 against FP64 with the particles reordered
+    already differs by more than 1e-5 (the explicit scheme above the VP
+    bound amplifies rounding differences every step); the mixed form's
+    difference from FP64 is of the same size."""
+    b = basins.instance(3, 4096)
+    b.params.dt = 1.0
+    p64 = b.params.copy()
+    p64.precision = 0
+    bp, inv = _permuted(b, 7)
+    g64, gp, g32 = Simp.from_basin(b, p64), Simp.from_basin(bp, p64), Simp.from_basin(b)
+    for g in (g64, gp, g32):
+        g.time_integration(100)
+    s64, sp, s32 = g64.get_state(), gp.get_state(), g32.get_state()
+    floor = rel_l2(sp["vx"][inv], s64["vx"])
+    err = rel_l2(s32["vx"], s64["vx"])
+    assert floor > 1e-5, floor
+    assert err < 10 * floor, (err, floor)
