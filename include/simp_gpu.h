@@ -259,6 +259,21 @@ SIMP_API int32_t simp_gpu_sum_density_noalloc(const double *x, const double *hsm
  * device). */
 SIMP_API void *simp_gpu_stream(simp_ctx *ctx);
 
+/* Implementation of the two pair passes (no reference counterpart):
+ * SIMP_PASSES_TILED stages chunks of `threads` consecutive particles of a
+ * cell row with their cell halo (at most `cap` particles) in shared memory;
+ * SIMP_PASSES_GATHER gathers every particle's neighbours from HBM over
+ * Verlet lists.  Both give the same bits.  threads: 64..256, a multiple of
+ * 32; cap: a multiple of 4, within the shared memory of one block. */
+#define SIMP_PASSES_GATHER 0
+#define SIMP_PASSES_TILED 1
+SIMP_API int32_t simp_gpu_set_passes(simp_ctx *ctx, int32_t impl, int32_t threads, int32_t cap);
+SIMP_API int32_t simp_gpu_get_passes(const simp_ctx *ctx, int32_t *impl, int32_t *threads, int32_t *cap);
+/* Times one right-hand side (both passes, no state change) of the current
+ * state under a set of implementations and tile shapes, `reps` times each,
+ * and keeps the fastest.  *ms_best: its time per right-hand side. */
+SIMP_API int32_t simp_gpu_autotune(simp_ctx *ctx, int32_t reps, double *ms_best);
+
 /* Number of kernels this context has launched so far (graph replays count
  * each captured kernel).  No reference counterpart. */
 SIMP_API int64_t simp_gpu_kernel_launches(const simp_ctx *ctx);

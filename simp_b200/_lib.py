@@ -41,6 +41,9 @@ SIGNATURES = {
     "simp_gpu_step": (_i32, [_vp, _i32, _dp, _dp]),
     "simp_gpu_interaction_stats": (_i32, [_vp, _ip, _ip, ctypes.POINTER(ctypes.c_int64), _ip]),
     "simp_gpu_sum_density_noalloc": (_i32, [_vp, _vp, _vp, _vp, _i32, _i32, _vp, _vp]),
+    "simp_gpu_set_passes": (_i32, [_vp, _i32, _i32, _i32]),
+    "simp_gpu_get_passes": (_i32, [_vp, _ip, _ip, _ip]),
+    "simp_gpu_autotune": (_i32, [_vp, _i32, _dp]),
     "simp_gpu_stream": (_vp, [_vp]),
     "simp_gpu_kernel_launches": (ctypes.c_int64, [_vp]),
     "simp_gpu_profile": (_i32, [_vp, _i32]),

@@ -42,17 +42,20 @@ __global__ void k_deinterleave(int n, const double *__restrict__ in, double *__r
 }
 
 // New particles [off, off + n): ids, instance, sort positions, m / rho.
-__global__ void k_init_new(int n, int off, int id_base, int slot, int *id, int *pinst, const double *x,
-                           const double *y, double *xr, double *yr, const double *m, const double *rho,
-                           double *mor) {
+__global__ void k_init_new(int n, int off, int id_base, int slot, int *id, int *pinst, State s, double *xr,
+                           double *yr) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const int i = off + k;
     id[i] = id_base + k;
     pinst[i] = slot;
-    xr[i] = x[i];
-    yr[i] = y[i];
-    mor[i] = m[i] / rho[i];
+    xr[i] = s.x[i];
+    yr[i] = s.y[i];
+    s.mor[i] = s.m[i] / s.rho[i];
+    if (s.mf) {
+        s.mf[i] = (float)s.m[i];
+        s.morf[i] = (float)s.mor[i];
+    }
 }
 
 __global__ void k_mark_removed(int n, int slot, int *pinst) {
@@ -176,7 +179,8 @@ void free_all(simp_ctx *c) {
                     c->itmp, c->scan_tmp, c->sc, c->pair_cnt, c->bpair_cnt, c->pair_buf_i,
                     c->pair_buf_j, c->pair_buf_r, c->pair_buf_h, c->nbr, c->nbr_count,
                     c->pair_j, c->pair_count, c->nbr_tmp, c->s0.xf, c->s0.yf, c->s0.hsf, c->s1.xf, c->s1.yf,
-                    c->inst_dev};
+                    c->inst_dev, c->row_map, c->chunk_cnt, c->chunk_off, c->chunks, c->s0.mf, c->s0.morf,
+                    c->s1.morf, c->mass1f, c->tau11f, c->tau12f, c->tau22f};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->sc_host) cudaFreeHost(c->sc_host);
@@ -263,6 +267,32 @@ int layout(simp_ctx *c) {
         c->scan_tmp_bytes = sb;
         c->cell_cap = capn;
     }
+    // cell rows of all instances, for the chunks of the tiled passes
+    std::vector<int2> rows;
+    for (int q = 0; q < c->max_inst; ++q)
+        if (c->insts[q].active)
+            for (int r = 0; r < c->insts[q].I.ncy; ++r) rows.push_back(make_int2(q, r));
+    c->total_rows = (int)rows.size();
+    const size_t need_chunks = (size_t)c->maxn / kMinTileThreads + rows.size() + 2;
+    if (rows.size() + 2 > c->row_cap || need_chunks > c->chunk_cap) {
+        cudaFree(c->row_map);
+        cudaFree(c->chunk_cnt);
+        cudaFree(c->chunk_off);
+        cudaFree(c->chunks);
+        c->row_map = nullptr;
+        c->chunk_cnt = c->chunk_off = nullptr;
+        c->chunks = nullptr;
+        const size_t rcap = rows.size() + rows.size() / 4 + 2;
+        TRY(dalloc(c, &c->row_map, rcap));
+        TRY(dalloc(c, &c->chunk_cnt, rcap));
+        TRY(dalloc(c, &c->chunk_off, rcap));
+        const size_t ccap = (size_t)c->maxn / kMinTileThreads + rcap;
+        TRY(dalloc(c, &c->chunks, ccap));
+        c->row_cap = rcap;
+        c->chunk_cap = ccap;
+    }
+    if (!rows.empty())
+        SIMP_CUDA(c, cudaMemcpyAsync(c->row_map, rows.data(), sizeof(int2) * rows.size(), cudaMemcpyHostToDevice, s));
     std::vector<Inst> table(c->max_inst);
     for (int q = 0; q < c->max_inst; ++q) table[q] = c->insts[q].active ? c->insts[q].I : Inst{};
     SIMP_CUDA(c, cudaMemcpyAsync(c->inst_dev, table.data(), sizeof(Inst) * c->max_inst, cudaMemcpyHostToDevice, s));
@@ -391,8 +421,7 @@ int add_instance(simp_ctx *c, int slot, const simp_forcing &f, int n, const doub
     SIMP_CUDA(c, cudaMemcpyAsync(c->s0.hs + off, hsml, sizeof(double) * N, cudaMemcpyHostToDevice, s));
     SIMP_CUDA(c, cudaMemcpyAsync(c->s0.A + off, A, sizeof(double) * N, cudaMemcpyHostToDevice, s));
     SIMP_CUDA(c, cudaMemcpyAsync(c->s0.h + off, h, sizeof(double) * N, cudaMemcpyHostToDevice, s));
-    k_init_new<<<nblk(n, kB), kB, 0, s>>>(n, off, ih.id_base, slot, c->id, c->pinst, c->s0.x, c->s0.y, c->xr,
-                                          c->yr, c->s0.m, c->s0.rho, c->s0.mor);
+    k_init_new<<<nblk(n, kB), kB, 0, s>>>(n, off, ih.id_base, slot, c->id, c->pinst, c->s0, c->xr, c->yr);
     k_grow_xabs<<<1, 1, 0, s>>>(c->sc, pxa);
     c->launches += 4;
     SIMP_CUDA(c, cudaGetLastError());
@@ -593,6 +622,17 @@ int create(const simp_params *params, int32_t maxn, int32_t maxnb, int32_t max_i
     float **f1[] = {&c->s0.xf, &c->s0.yf, &c->s0.hsf, &c->s1.xf, &c->s1.yf};
     for (float **p : f1) TRY(dalloc(c, p, M));
     c->s1.hsf = c->s0.hsf;
+    if (c->prm.precision == SIMP_PREC_MIXED) {
+        // FP32 copies the mixed form's pair arithmetic reads
+        float **f2[] = {&c->s0.mf, &c->s0.morf, &c->s1.morf, &c->tau11f, &c->tau12f, &c->tau22f};
+        for (float **p : f2) TRY(dalloc(c, p, M));
+        if (c->mass1) {
+            TRY(dalloc(c, &c->mass1f, M));
+            c->s1.mf = c->mass1f;
+        } else {
+            c->s1.mf = c->s0.mf;
+        }
+    }
     TRY(dalloc(c, &c->nbr, (size_t)kMaxNbr * M));
     TRY(dalloc(c, &c->nbr_count, M));
     TRY(dalloc(c, &c->nbr_tmp, (size_t)kMaxNbr * M));
@@ -629,6 +669,7 @@ int create(const simp_params *params, int32_t maxn, int32_t maxnb, int32_t max_i
     sc.minip = 0x7fffffff;
     sc.list_scan = 1;
     SIMP_CUDA(c, cudaMemcpyAsync(c->sc, c->sc_host, sizeof(Scalars), cudaMemcpyHostToDevice, c->stream));
+    TRY(tiled_configure(c));
     TRY(layout(c));
     return SIMP_OK;
 }
@@ -1011,6 +1052,90 @@ int32_t simp_gpu_step(simp_ctx *c, int32_t nsteps, double *current_time, double 
     if (!c || nsteps < 0) return SIMP_ERR_BADARG;
     TRY(simp::step_enqueue(c, nsteps));
     return simp::step_complete(c, current_time, dt);
+}
+
+int32_t simp_gpu_set_passes(simp_ctx *c, int32_t impl, int32_t threads, int32_t cap) {
+    if (!c) return SIMP_ERR_BADARG;
+    if (impl != SIMP_PASSES_GATHER && impl != SIMP_PASSES_TILED)
+        return simp_fail(c, SIMP_ERR_BADARG, "unknown pair-pass implementation");
+    if (threads < kMinTileThreads || threads > 256 || threads % 32 != 0 || cap < 64 || cap % 4 != 0 ||
+        cap > 32767)
+        return simp_fail(c, SIMP_ERR_BADARG, "tile shape out of range");
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const size_t need = std::max(tiled_smem_bytes(c->prm.precision, 0, cap, threads),
+                                 tiled_smem_bytes(c->prm.precision, 1, cap, threads));
+    if (optin > 0 && need + 1024 > (size_t)optin)
+        return simp_fail(c, SIMP_ERR_BADARG, "tile shape exceeds the shared memory of a block");
+    const bool rechunk = threads != c->tile_threads || impl != c->pass_impl;
+    c->pass_impl = impl;   // (both keep the Verlet lists the same way)
+    c->tile_threads = threads;
+    c->tile_cap = cap;
+    TRY(tiled_configure(c));
+    if (rechunk && c->n > 0) build_chunks(c);
+    invalidate_graph(c);
+    SIMP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return SIMP_OK;
+}
+
+int32_t simp_gpu_get_passes(const simp_ctx *c, int32_t *impl, int32_t *threads, int32_t *cap) {
+    if (!c) return SIMP_ERR_BADARG;
+    if (impl) *impl = c->pass_impl;
+    if (threads) *threads = c->tile_threads;
+    if (cap) *cap = c->tile_cap;
+    return SIMP_OK;
+}
+
+// One right-hand side at the current state (kinematic pass + stress pass in
+// rates mode: no state changes), timed with events.
+static int time_rhs(simp_ctx *c, int reps, double *ms) {
+    cudaEvent_t e0, e1;
+    SIMP_CUDA(c, cudaEventCreate(&e0));
+    SIMP_CUDA(c, cudaEventCreate(&e1));
+    launch_kinematic(c, c->s0, false);          // warm-up
+    launch_stress(c, c->s0, c->s0, EPI_RATES);
+    cudaEventRecord(e0, c->stream);
+    for (int r = 0; r < reps; ++r) {
+        launch_kinematic(c, c->s0, false);
+        launch_stress(c, c->s0, c->s0, EPI_RATES);
+    }
+    cudaEventRecord(e1, c->stream);
+    cudaError_t e = cudaEventSynchronize(e1);
+    float t = 0.0f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return simp_cuda_check(c, e, "autotune timing");
+    *ms = (double)t / std::max(1, reps);
+    return SIMP_OK;
+}
+
+int32_t simp_gpu_autotune(simp_ctx *c, int32_t reps, double *ms_best) {
+    if (!c || reps < 1) return SIMP_ERR_BADARG;
+    if (!c->have_state || c->n == 0) return simp_fail(c, SIMP_ERR_STATE, "autotune needs particles");
+    struct Cand { int impl, threads, cap; };
+    const Cand cands[] = {
+        {SIMP_PASSES_TILED, 128, 512},  {SIMP_PASSES_TILED, 128, 768},  {SIMP_PASSES_TILED, 128, 1024},
+        {SIMP_PASSES_TILED, 256, 768},  {SIMP_PASSES_TILED, 256, 1024}, {SIMP_PASSES_TILED, 256, 1536},
+        {SIMP_PASSES_TILED, 64, 384},   {SIMP_PASSES_TILED, 64, 512},   {SIMP_PASSES_GATHER, 256, 1024}};
+    const Cand keep{c->pass_impl, c->tile_threads, c->tile_cap};
+    Cand best = keep;
+    double tbest = INFINITY;
+    for (const Cand &k : cands) {
+        if (simp_gpu_set_passes(c, k.impl, k.threads, k.cap) != SIMP_OK) continue;   // shape does not fit
+        double t = 0.0;
+        TRY(time_rhs(c, reps, &t));
+        if (t < tbest) {
+            tbest = t;
+            best = k;
+        }
+    }
+    TRY(simp_gpu_set_passes(c, best.impl, best.threads, best.cap));
+    (void)keep;
+    c->err.clear();
+    if (ms_best) *ms_best = tbest;
+    return SIMP_OK;
 }
 
 void *simp_gpu_stream(simp_ctx *c) { return c ? (void *)c->stream : nullptr; }

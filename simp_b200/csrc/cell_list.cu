@@ -282,6 +282,10 @@ __global__ void k_put_back(int kept, int all, DueMask due, Gather gd, State s, c
     s.xf[k] = (float)s.x[k];
     s.yf[k] = (float)s.y[k];
     s.hsf[k] = (float)s.hs[k];
+    if (s.mf) {
+        s.mf[k] = (float)s.m[k];
+        s.morf[k] = (float)s.mor[k];
+    }
 }
 
 // After a sort: displacement since the sort restarts; the Verlet lists are
@@ -377,9 +381,10 @@ int rebuild(simp_ctx *c, const DueMask &due, bool full, bool new_lists) {
     }
     k_reset_disp<<<1, 1, 0, s>>>(c->sc, keep_lists ? 1 : 0);
     c->launches += 1;
-    SIMP_CUDA(c, cudaGetLastError());
     if (!keep_lists) c->lists_valid = false;
     c->n = kept;
+    if (c->pass_impl == SIMP_PASSES_TILED) build_chunks(c);
+    SIMP_CUDA(c, cudaGetLastError());
     c->rebuilds += 1;
     return SIMP_OK;
 }

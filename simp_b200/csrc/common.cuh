@@ -23,6 +23,7 @@ struct State {
     double *m, *rho, *mor, *h, *A;
     double *hs;   // hsml (shared by S0 and S1: updated only at step end)
     float *xf, *yf, *hsf;  // FP32 copies for the candidate prefilter (hsf shared)
+    float *mf, *morf;      // FP32 copies of m and m / rho (mixed precision only, else null)
 };
 
 // Verlet neighbour lists (cell-order indices): nbr[k * stride + i],
@@ -83,6 +84,12 @@ __host__ __device__ __forceinline__ Grid inst_grid(const Inst &I, const int *cel
     g.cell_start = cell_start;
     return g;
 }
+
+// Particle chunk of the tiled pair passes: consecutive particles [p0, p1)
+// of cell row `row` of instance q.
+struct Chunk {
+    int p0, p1, q, row;
+};
 
 // Device-resident integrator scalars and per-step reductions.
 struct Scalars {

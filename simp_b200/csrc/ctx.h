@@ -50,6 +50,8 @@ struct simp_ctx {
     int *pinst = nullptr;          // instance slot of each particle (-1: being removed)
     // per-RHS intermediates from the kinematic pass
     double *tau11 = nullptr, *tau12 = nullptr, *tau22 = nullptr, *div = nullptr;
+    float *tau11f = nullptr, *tau12f = nullptr, *tau22f = nullptr;   // mixed precision only
+    float *mass1f = nullptr;       // FP32 half-step mass (mixed precision with the mass update)
     int *nbr = nullptr;            // kMaxNbr * maxn neighbour indices (column-major)
     int *nbr_count = nullptr;      // maxn
     int *nbr_tmp = nullptr;        // kMaxNbr * maxn: lists being renamed by a sort
@@ -69,6 +71,17 @@ struct simp_ctx {
     // cell lists
     int *cell_start = nullptr;
     size_t cell_cap = 0;
+    // pair-pass implementation (SIMP_PASSES_*) and its tile shape
+    int pass_impl = SIMP_PASSES_GATHER;
+    int tile_threads = 256;        // particles per chunk = threads per block
+    int tile_cap = 1024;           // halo particles a block stages
+    // chunks of the tiled passes
+    int total_rows = 0;            // cell rows over all instances
+    int2 *row_map = nullptr;       // (instance, row) of each global row
+    int *chunk_cnt = nullptr;      // chunks per row
+    int *chunk_off = nullptr;      // their exclusive scan (+ total)
+    simp::Chunk *chunks = nullptr;
+    size_t row_cap = 0, chunk_cap = 0;
     // rebuild scratch
     int *cnt = nullptr;            // per-cell counters (cell_cap)
     int *perm = nullptr;           // maxn
@@ -125,6 +138,12 @@ void launch_kinematic(simp_ctx *c, const State &s, bool diag);
 void launch_stress(simp_ctx *c, const State &nb, const State &own, EpiMode mode);
 void launch_step_finish(simp_ctx *c);
 void launch_reset_stats(simp_ctx *c);
+
+// tiled.cu
+constexpr int kMinTileThreads = 64;
+void build_chunks(simp_ctx *c);
+int tiled_configure(simp_ctx *c);
+size_t tiled_smem_bytes(int precision, int pass, int cap, int threads);
 
 // abi.cu: the step driver split for callers that overlap contexts
 int step_enqueue(simp_ctx *c, int nsteps);

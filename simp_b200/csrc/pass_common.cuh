@@ -1,0 +1,592 @@
+// Shared device code of the two pair passes of one right-hand-side evaluation (single_step.f90:5-109)
+// and the predictor-corrector update fused into the second pass's epilogue.
+//
+// Kinematic pass (single_step.f90:50-84 + internal_stress.f90:20-42), per
+// particle i, in two phases:
+//   1. candidate scan of the cell stencil with an FP32 prefilter and the
+//      exact FP64 criterion for undecided candidates (neighbors.cuh); the
+//      accepted neighbours go to a per-thread list in shared memory and to
+//      the neighbour list in HBM that the stress pass reuses;
+//   2. FP64 pair math over the dense list:
+//        wdvx = (v_i - v_j) (x) grad W_ij            (kernel.f90:515-518)
+//        div_i  -= m_j (wdvx1 + wdvx4)               (vector_divergence.f90:27)
+//        grad_i -= m_j wdvx / rho_j                  (vector_gradient.f90:56-69)
+//   then strain (single_step.f90:80-84), strength, bulk and shear viscosity,
+//   replacement pressure and stress (bulk_viscosity.f90:65-76,
+//   shear_viscosity.f90:57, eos.f90:141-147, stress_tensor.f90:31-39).
+//   Writes tau = sigma / rho^2 and div.
+//
+// Stress pass (internal_stress.f90:103-137 stress_1, boundary_kernel.f90 +
+// boundary_force.f90:74-84, wind_forcing.f90:35-51, water_drag.f90:35-53,
+// single_step.f90:104-106) over the kinematic pass's neighbour list:
+//   a_i = rho_i / (rho_ice h_i) sum_j m_j (tau_i + tau_j) . grad W_ij
+//         - sum_walls F_b / rho_i + wind + water drag
+//   followed by one of three epilogues: the rates (single_step), the
+//   predictor half step (time_integration.f90:314-338) or the corrector and
+//   final update (:343-388).
+//
+// Each pair is evaluated from both sides (gather form, no atomics on the
+// accumulations); grad W is odd in dx so both sides see the same per-pair
+// terms as the reference's scatter loop, summed in a different order.
+//
+// Two implementations share this file's helpers: passes.cu gathers each
+// particle's neighbours from HBM over Verlet lists; tiled.cu stages chunks of
+// particles with their cell halo in shared memory.
+#pragma once
+
+#include <cmath>
+#include <cstddef>
+
+#include "ctx.h"
+#include "neighbors.cuh"
+
+namespace simp {
+namespace pass {
+
+// per-thread list of a particle's pairs: the whole pair list of a particle
+// with up to kMaxPairs pairs (then written out row by row), flushed when full
+constexpr int kListSlots = kMaxPairs + 1;
+
+// Pair arithmetic type T: double for the plain form, float for the mixed
+// form.  Positions and velocities stay FP64; their differences are formed in
+// FP64 and rounded to T, after which the kernel gradient and the pair sums
+// run in T (compensated when T is float).
+__device__ __forceinline__ double rsq(double v) { return rsqrt(v); }
+__device__ __forceinline__ float rsq(float v) { return rsqrtf(v); }
+
+// Sum of pair terms a * b: plain FP64, or FP32 with Kahan compensation.
+// Every multiply-add of the pair arithmetic is an explicit fma, so the
+// rounding does not depend on which products a compiler chooses to fuse
+// (both pass implementations then give the same bits).
+template <class T>
+struct Sum {
+    double s = 0.0;
+    __device__ __forceinline__ void madd(double a, double b) { s = fma(a, b, s); }
+    __device__ __forceinline__ double get() const { return s; }
+};
+template <>
+struct Sum<float> {
+    float s = 0.0f, c = 0.0f;
+    __device__ __forceinline__ void madd(float a, float b) {
+        const float y = fmaf(a, b, -c);
+        const float t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+    __device__ __forceinline__ double get() const { return (double)s - (double)c; }
+};
+
+// Per-pair geometry and kernel gradient: dw = gfac * (dx, dy).
+// r = s * rsqrt(s) and 1/hsml_ij from the particle's own 1/hsml when the two
+// smoothing lengths are equal (then hsml_ij = hsml_i exactly).
+template <class T>
+struct PairGeom {
+    T dx, dy, gfac, w;
+};
+
+// dx, dy: x_i - x_j (differences of the FP64 positions, rounded to T);
+// hi, inv_hi, hj: the smoothing lengths in T (the FP32 copies in the mixed
+// form).
+template <class T, bool WANT_W>
+__device__ __forceinline__ PairGeom<T> pair_geom(const Phys &P, T dx, T dy, T hi, T inv_hi, T hj) {
+    PairGeom<T> g;
+    g.dx = dx;
+    g.dy = dy;
+    const T s = fma(g.dx, g.dx, g.dy * g.dy);
+    const T rs = rsq(s);
+    const T r = s * rs;
+    const T inv_h = (hj == hi) ? inv_hi : T(2) / (hi + hj);
+    const T sh = (T)P.scale_h;
+    const T shh = sh * inv_h;
+    const T q = r * shh;
+    T gq;
+    if (P.skf == SIMP_SKF_WENDLAND_C6) {
+        const T factor = (T)(78.0 / (7.0 * kPi)) * (shh * shh);
+        const T om = T(1) - q;
+        const T om2 = om * om, om4 = om2 * om2;
+        if (WANT_W) g.w = factor * (om4 * om4) * (((T(32) * q + T(25)) * q + T(8)) * q + T(1));
+        gq = factor * (T(-22) * q * (om4 * om2 * om) * ((T(16) * q + T(7)) * q + T(1)));
+    } else {
+        const T factor = (T)(15.0 / (7.0 * kPi)) * (shh * shh);
+        if (q <= T(1)) {
+            if (WANT_W) g.w = factor * fma(T(0.5) * q * q, q, fma(-q, q, (T)(2.0f / 3.0f)));
+            gq = factor * fma(T(1.5) * q, q, T(-2) * q);
+        } else {
+            const T u = T(2) - q;
+            if (WANT_W) g.w = factor * ((T)(1.0f / 6.0f) * u * u * u);
+            gq = factor * (T(-0.5) * u * u);
+        }
+    }
+    g.gfac = gq * shh * rs;
+    return g;
+}
+
+// What a pass needs to decide the reference criterion for particle i.
+struct PairCtx {
+    double xi, yi, hi;
+    float xif, yif, hif;
+    float margin;
+    bool use_f32;
+    BinRule br;
+    Grid g;                     // the particle's instance grid
+    double hmax;                // instance bounds for the stencil radius
+    unsigned long long dmax2_bits;
+};
+
+__device__ __forceinline__ PairCtx pair_ctx(const State &s, const Scalars *sc, const Inst &I,
+                                            const int *cell_start, int i) {
+    PairCtx p;
+    p.xi = s.x[i];
+    p.yi = s.y[i];
+    p.hi = s.hs[i];
+    p.xif = s.xf[i];
+    p.yif = s.yf[i];
+    p.hif = s.hsf[i];
+    p.margin = prefilter_margin(bitsd(sc->xabs_bits), I.hmin);
+    p.use_f32 = p.margin < 0.25f;
+    p.br = make_bin_rule(I.bs, p.xi, p.yi, I.hmax);
+    p.g = inst_grid(I, cell_start);
+    p.hmax = I.hmax;
+    p.dmax2_bits = I.dmax2_bits;
+    return p;
+}
+
+// The reference criterion for candidate j, decided exactly: FP32 prefilter,
+// the FP64 test of nnps.f90:277-281 when undecided, then the bucket rule.
+__device__ __forceinline__ bool is_pair(const State &s, const PairCtx &p, int j) {
+    int dec = 2;
+    if (p.use_f32) dec = prefilter(p.xif - s.xf[j], p.yif - s.yf[j], 0.5f * (p.hif + s.hsf[j]), p.margin);
+    if (dec == 0) return false;
+    if (dec == 2 || p.br.on) {
+        const double xj = s.x[j], yj = s.y[j];
+        if (dec == 2) {
+            double r;
+            const double mh = __dmul_rn(__dadd_rn(p.hi, s.hs[j]), 0.5);
+            if (!pair_test(__dsub_rn(p.xi, xj), __dsub_rn(p.yi, yj), mh, &r)) return false;
+        }
+        if (!bin_rule_ok(p.br, xj, yj)) return false;
+    }
+    return true;
+}
+
+// Visits the cell-stencil candidates of particle i (cell order).
+template <class F>
+__device__ __forceinline__ void for_stencil(const Grid &g, int i, int ci, int R, F &&f) {
+    for_stencil_rows(g, ci, R, [&](int j0, int j1) {
+        for (int j = j0; j < j1; ++j)
+            if (j != i) f(j);
+    });
+}
+
+// Every current pair of particle i: from its Verlet list when that list
+// still holds every pair, else from its cell stencil.  The lists were all
+// built at the same positions (xl, yl) with members within mhsml + skin; a
+// current pair (i, j) was then at most mhsml + |dx_i| + |dx_j| apart, so i's
+// list is complete while |dx_i| + max_j |dx_j| < skin.
+template <class F>
+__device__ __forceinline__ void for_each_current_pair(const State &s, const NbrList &nl, const Scalars *sc,
+                                                      int i, int ci, const PairCtx &p, F &&on_pair) {
+    const int cnt = nl.count[i];
+    const double dxl = p.xi - nl.xl[i], dyl = p.yi - nl.yl[i];
+    const double own = sqrt(dxl * dxl + dyl * dyl);
+    const double all = sqrt(bitsd(sc->dlist2_bits));
+    const bool valid = (own + all) * (1.0 + 1e-9) < sc->skin;
+    if (cnt <= kMaxNbr && valid) {
+        for (int k = 0; k < cnt; ++k) {
+            const int j = nl.nbr[(size_t)k * nl.stride + i];
+            if (is_pair(s, p, j)) on_pair(j);
+        }
+    } else {
+        for_stencil(p.g, i, ci, stencil_radius(p.hmax, p.dmax2_bits, p.g, 0.0), [&](int j) {
+            if (is_pair(s, p, j)) on_pair(j);
+        });
+    }
+}
+
+// Neighbour values in the pair arithmetic type: the FP64 arrays for the
+// plain form, their FP32 copies for the mixed form.
+template <class T>
+struct Nb;
+template <>
+struct Nb<double> {
+    static __device__ __forceinline__ double h(const State &s, int j) { return s.hs[j]; }
+    static __device__ __forceinline__ double m(const State &s, int j) { return s.m[j]; }
+    static __device__ __forceinline__ double mor(const State &s, int j) { return s.mor[j]; }
+    static __device__ __forceinline__ double tau(const double *t, const float *, int j) { return t[j]; }
+};
+template <>
+struct Nb<float> {
+    static __device__ __forceinline__ float h(const State &s, int j) { return s.hsf[j]; }
+    static __device__ __forceinline__ float m(const State &s, int j) { return s.mf[j]; }
+    static __device__ __forceinline__ float mor(const State &s, int j) { return s.morf[j]; }
+    static __device__ __forceinline__ float tau(const double *, const float *tf, int j) { return tf[j]; }
+};
+
+// Kinematic-pass pair terms (kernel.f90:515-518, vector_divergence.f90:27,
+// vector_gradient.f90:56-69): sums of -div and of the velocity gradient.
+template <class T>
+struct KinSums {
+    Sum<T> dv, g1, g2, g3, g4;
+    __device__ __forceinline__ void add(const PairGeom<T> &pg, T dvx, T dvy, T mj, T mrj) {
+        const T dwx = pg.gfac * pg.dx, dwy = pg.gfac * pg.dy;
+        const T w2 = dvy * dwx, w3 = dvx * dwy, w4 = dvy * dwy;
+        const T w1 = dvx * dwx;
+        dv.madd(mj, fma(dvx, dwx, w4));
+        g1.madd(mrj, w1);
+        g2.madd(mrj, w2);
+        g3.madd(mrj, w3);
+        g4.madd(mrj, w4);
+    }
+};
+
+// Stress-pass pair terms (internal_stress.f90:103-137): sum_j m_j grad W
+// and sum_j m_j tau_j . grad W.
+template <class T>
+struct StressSums {
+    Sum<T> sx, sy, tx, ty;
+    __device__ __forceinline__ void add(const PairGeom<T> &pg, T mj, T t11, T t12, T t22) {
+        const T dwx = pg.gfac * pg.dx, dwy = pg.gfac * pg.dy;
+        sx.madd(mj, dwx);
+        sy.madd(mj, dwy);
+        tx.madd(mj, fma(t11, dwx, t12 * dwy));
+        ty.madd(mj, fma(t12, dwx, t22 * dwy));
+    }
+};
+
+struct KinArgs {
+    State s;
+    const int *cell_start;
+    const Inst *inst;
+    const int *pinst;      // instance of each particle
+    const int *cell;
+    Phys P;
+    Scalars *sc;
+    double *tau11, *tau12, *tau22, *div;
+    float *tau11f, *tau12f, *tau22f;   // FP32 copies (mixed precision only)
+    double *diag;
+    NbrList nl;
+    PairList pl;
+    int n, maxn;
+    // tiled implementation
+    const Chunk *chunks;
+    const int *nchunks;
+    int cap;               // halo particles that fit in shared memory
+};
+
+// Strain rates, rheology and stress of particle i from its velocity
+// divergence dv and velocity gradient g (single_step.f90:80-84,
+// internal_stress.f90:20-42): writes tau = sigma / rho^2, div and the
+// optional diagnostics.
+__device__ __forceinline__ void kin_rheology(const KinArgs &a, int i, double dv, double g1, double g2,
+                                             double g3, double g4) {
+    const State &s = a.s;
+    const Phys &P = a.P;
+    // strain rates, single_step.f90:80-84
+    const double e11 = g1, e22 = g4, e12 = 0.5 * (g2 + g3);
+    // rheology, internal_stress.f90:20-42
+    const double hh = s.h[i], AA = s.A[i];
+    const double em2 = 1.0 / (P.e * P.e);
+    const double Pstr = P.P_star * hh * exp(-(P.c_eos * (1.0 - AA)));
+    const double delta = sqrt(fma(fma(e11, e11, e22 * e22), 1.0 + em2,
+                                  fma(4.0 * em2, e12 * e12, 2.0 * e11 * e22 * (1.0 - em2))));
+    const double dcap = (fabs(delta) < P.delta_min) ? P.delta_min : delta;
+    double zeta = 0.0, eta = 0.0, p = 0.0;
+    if (P.viscosity) {
+        zeta = 0.5 * Pstr * (1.0 + P.k_t) / dcap;
+        eta = zeta / (P.e * P.e);
+        p = Pstr;
+    }
+    if (P.pressure_force) p = (P.eos_alg == 3) ? zeta * 2.0 * delta / (1.0 + P.k_t) : Pstr;
+    const double ph = p * (1.0 - P.k_t) / 2.0;
+    const double s11 = fma(zeta + eta, e11, fma(zeta - eta, e22, -ph));
+    const double s12 = 2.0 * eta * e12;
+    const double s22 = fma(zeta + eta, e22, fma(zeta - eta, e11, -ph));
+    const double rho = s.rho[i];
+    const double ir2 = 1.0 / (rho * rho);
+    a.tau11[i] = s11 * ir2;
+    a.tau12[i] = s12 * ir2;
+    a.tau22[i] = s22 * ir2;
+    if (a.tau11f) {
+        a.tau11f[i] = (float)(s11 * ir2);
+        a.tau12f[i] = (float)(s12 * ir2);
+        a.tau22f[i] = (float)(s22 * ir2);
+    }
+    a.div[i] = dv;
+    if (a.diag) {
+        const size_t M = (size_t)a.maxn;
+        a.diag[i] = e11;
+        a.diag[M + i] = e12;
+        a.diag[2 * M + i] = e22;
+        a.diag[3 * M + i] = zeta;
+        a.diag[4 * M + i] = eta;
+        a.diag[5 * M + i] = p;
+        a.diag[6 * M + i] = s11;
+        a.diag[7 * M + i] = s12;
+        a.diag[8 * M + i] = s22;
+    }
+}
+
+struct StressArgs {
+    State rhs;     // state the right-hand side is evaluated at
+    State base;    // step-start state (own values for the integrator)
+    State out;     // state written by the epilogue
+    const int *cell_start;
+    Inst *inst;
+    const int *pinst;
+    const int *cell;
+    const double *bx, *by, *bm;
+    const int *bstart;
+    int nb;
+    Phys P;
+    Scalars *sc;
+    const double *tau11, *tau12, *tau22, *div;
+    const float *tau11f, *tau12f, *tau22f;
+    NbrList nl;
+    PairList pl;
+    double *rates;
+    const double *xr, *yr;
+    double *hs_next;
+    int n, maxn, mode;
+    // tiled implementation
+    const Chunk *chunks;
+    const int *nchunks;
+    int cap;
+};
+
+// Max of a per-instance 64-bit field over the lanes of a warp: one atomic per
+// warp when the warp holds a single instance (the common case: instances are
+// contiguous in cell order), one per lane otherwise.
+__device__ __forceinline__ void inst_max_u64(Inst *inst, int k, size_t field, unsigned long long v) {
+    const unsigned mask = __match_any_sync(0xffffffffu, k);
+    if (mask == 0xffffffffu) {
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long t = __shfl_xor_sync(0xffffffffu, v, o);
+            v = (t > v) ? t : v;
+        }
+        if ((threadIdx.x & 31) != 0) return;
+    }
+    atomicMax(reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(&inst[k]) + field), v);
+}
+
+// Block-wide max / min folded into one device atomic per block (the
+// same-address atomics of every warp would serialise in L2).  Called by all
+// threads of the block at the same point.
+template <bool MAX>
+__device__ __forceinline__ void block_reduce_u64(unsigned long long *dst, unsigned long long v) {
+    __shared__ unsigned long long part[32];
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long t = __shfl_xor_sync(0xffffffffu, v, o);
+        v = MAX ? (t > v ? t : v) : (t < v ? t : v);
+    }
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) v = MAX ? (part[w] > v ? part[w] : v) : (part[w] < v ? part[w] : v);
+        if (MAX) atomicMax(dst, v); else atomicMin(dst, v);
+    }
+    __syncthreads();
+}
+__device__ __forceinline__ void warp_max_u64(unsigned long long *dst, unsigned long long v) {
+    block_reduce_u64<true>(dst, v);
+}
+__device__ __forceinline__ void warp_min_u64(unsigned long long *dst, unsigned long long v) {
+    block_reduce_u64<false>(dst, v);
+}
+__device__ __forceinline__ void warp_max_i32(int *dst, int v) {
+    __shared__ int part[32];
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) v = max(v, part[w]);
+        atomicMax(dst, v);
+    }
+    __syncthreads();
+}
+
+// The last block of a stress pass to finish decides whether the next
+// kinematic pass rebuilds the Verlet lists: when the fastest particle moved
+// 3/4 of the skin since they were built (lists are then complete only for
+// particles that moved less than skin / 4), or when hsml changes (sle = 2).
+// Threadfence reduction; no block waits on another.  Every block of the
+// grid calls it once, with all its threads.
+__device__ __forceinline__ void lists_block_done(const StressArgs &a) {
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(&a.sc->blocks_done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        const double dl = sqrt(bitsd(atomicAdd(&a.sc->dlist2_bits, 0ull)));
+        const bool stale = (a.P.sle == 2) || !(dl < 0.75 * a.sc->skin);
+        a.sc->list_scan = stale ? 1 : 0;
+        a.sc->blocks_done = 0u;
+    }
+}
+
+// Everything of the stress pass after the pair sums S = sum_j m_j grad W_ij
+// and T = sum_j m_j tau_j . grad W_ij of particle i: internal force, walls,
+// drag, rates and the integrator epilogue with the bounds reductions.
+// Called by every thread of the block (dead lanes with live = false).
+// `lists`: the Verlet-list implementation (displacement since the lists
+// were built, and the last block's rebuild decision).
+__device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool live, int ki, const Inst &I,
+                                              bool dead, double xi, double yi, double hi, int ci, double Sx,
+                                              double Sy, double Tx, double Ty, int cnt, bool lists) {
+    const State &s = a.rhs;
+    const Phys &P = a.P;
+    const double rho = s.rho[i], hh = s.h[i], AA = s.A[i], mi = s.m[i];
+    const double fi = rho / P.rho_ice / hh;
+    double ax = fi * fma(a.tau11[i], Sx, fma(a.tau12[i], Sy, Tx));
+    double ay = fi * fma(a.tau12[i], Sx, fma(a.tau22[i], Sy, Ty));
+    // boundary force (bf_Monaghan normal component, boundary_force.f90:78-82)
+    if (P.boundary_pressure && a.nb > 0 && !dead) {
+        const Grid g = inst_grid(I, a.cell_start);
+        const double bl = I.b_length;
+        const int Rb = wall_radius(I.dmax2_bits, g, bl);
+        const BinRule bb = make_bin_rule(I.bs, xi, yi, bl);
+        double fx = 0.0, fy = 0.0;
+        cnt += for_each_wall(a.bx, a.by, a.bstart, g, ci, Rb, bb, xi, yi, bl,
+                             [&](int b, double bdx, double bdy, double d) {
+                                 const double bw = boundary_w(P, d, hi);
+                                 const double mb = a.bm[b];
+                                 const double coef = P.kappa_n * bw * 2.0 * mb / ((mi + mb) * (d * d));
+                                 fx += coef * bdx;
+                                 fy += coef * bdy;
+                             });
+        ax -= fx / rho;
+        ay -= fy / rho;
+    }
+    // drag, wind_forcing.f90:35-51 and water_drag.f90:35-53 (off at t <= 0)
+    const double vxi = s.vx[i], vyi = s.vy[i];
+    const double tnow = I.t;
+    if (P.wind_force && tnow > 0.0) {
+        double wu, wv;
+        wind_at(I, xi, yi, &wu, &wv);
+        const double ru = wu - vxi, rv = wv - vyi;
+        const double k = P.c_wind * P.rho_air / (hh * P.rho_ice);
+        ax += k * ru * fabs(ru);
+        ay += k * rv * fabs(rv);
+    }
+    if (P.water_force && tnow > 0.0) {
+        const double ru = P.current_u - vxi, rv = P.current_v - vyi;
+        const double k = P.c_water * P.rho_water / (hh * P.rho_ice);
+        ax += k * ru * fabs(ru);
+        ay += k * rv * fabs(rv);
+    }
+    // prognostic rates, single_step.f90:104-106
+    const double dv = a.div[i];
+    const double dhdt = -hh * dv / rho;
+    const double dAdt = -AA * dv / rho;
+    warp_max_i32(&a.sc->maxip, live ? cnt : 0);
+
+    if (a.mode == EPI_RATES) {
+        if (live) {
+            const size_t M = (size_t)a.maxn;
+            a.rates[i] = ax;
+            a.rates[M + i] = ay;
+            a.rates[2 * M + i] = dhdt;
+            a.rates[3 * M + i] = dAdt;
+        }
+        return;
+    }
+    const double dt = a.sc->dt;
+    const State &b = a.base;
+    const double x0 = b.x[i], y0 = b.y[i], vx0 = b.vx[i], vy0 = b.vy[i], h0 = b.h[i], A0 = b.A[i];
+    double xn, yn, vxn, vyn, hn, An;
+    if (a.mode == EPI_PREDICT) {
+        // time_integration.f90:315-323
+        xn = x0 + vxi * dt / 2.0;
+        yn = y0 + vyi * dt / 2.0;
+        vxn = vx0 + ax * dt / 2.0;
+        vyn = vy0 + ay * dt / 2.0;
+        hn = h0 + dhdt * dt / 2.0;
+        An = A0 + dAdt * dt / 2.0;
+    } else {
+        // time_integration.f90:344-367
+        const double x12 = x0 + vxi * dt / 2.0, y12 = y0 + vyi * dt / 2.0;
+        const double vx12 = vx0 + ax * dt / 2.0, vy12 = vy0 + ay * dt / 2.0;
+        const double h12 = h0 + dhdt * dt / 2.0, A12 = A0 + dAdt * dt / 2.0;
+        xn = 2.0 * x12 - x0;
+        yn = 2.0 * y12 - y0;
+        vxn = 2.0 * vx12 - vx0;
+        vyn = 2.0 * vy12 - vy0;
+        hn = 2.0 * h12 - h0;
+        An = 2.0 * A12 - A0;
+    }
+    if (An > 1.0) An = 1.0;
+    const double rhon = hn * P.rho_ice;                       // density.f90:192
+    double mn = b.m[i];
+    const double hs_old = b.hs[i];
+    if (P.sle != 2 && P.mass_from_area) {                     // mass_evolution.f90:66-69
+        const double ar = kPi * ((P.alpha * hs_old) * (P.alpha * hs_old));
+        mn = P.rho_ice * An * hn * ar;
+    }
+    double hsn = hs_old;
+    if (a.mode == EPI_CORRECT && P.sle == 2) {                // smoothing_length.f90:136-142
+        hsn = sqrt(mn / rhon) * (double)P.hsml_multiplicity;
+        if (hsn > P.max_hsml) hsn = P.max_hsml;
+    }
+    // displacement since the instance's last sort, max per instance
+    const double dxr = xn - a.xr[i], dyr = yn - a.yr[i];
+    // (non-finite values stay out of these bounds: the basin is flagged below)
+    double d2 = dxr * dxr + dyr * dyr;
+    if (!live || !isfinite(d2)) d2 = 0.0;
+    inst_max_u64(a.inst, ki, offsetof(Inst, dmax2_bits), dbits(d2));
+    if (lists) {
+        const double dxl = xn - a.nl.xl[i], dyl = yn - a.nl.yl[i];
+        double dl2 = dxl * dxl + dyl * dyl;
+        if (!live || !isfinite(dl2)) dl2 = 0.0;
+        warp_max_u64(&a.sc->dlist2_bits, dbits(dl2));
+    }
+    double xa = fmax(fabs(xn), fabs(yn));
+    if (!isfinite(xa)) xa = 0.0;
+    warp_max_u64(&a.sc->xabs_bits, dbits(xa));
+    const bool bad = !(isfinite(xn) && isfinite(yn) && isfinite(vxn) && isfinite(vyn) &&
+                       isfinite(hn) && isfinite(An));
+    if (live && bad) {
+        atomicOr(&a.sc->flags, FLAG_NONFINITE);
+        atomicOr(&a.inst[ki].flags, FLAG_NONFINITE);
+    }
+    if (live) {
+        const State &o = a.out;
+        o.x[i] = xn;
+        o.y[i] = yn;
+        o.xf[i] = (float)xn;
+        o.yf[i] = (float)yn;
+        o.vx[i] = vxn;
+        o.vy[i] = vyn;
+        o.h[i] = hn;
+        o.A[i] = An;
+        o.rho[i] = rhon;
+        if (P.sle != 2 && P.mass_from_area) {
+            o.m[i] = mn;
+            if (o.mf) o.mf[i] = (float)mn;
+        }
+        o.mor[i] = mn / rhon;
+        if (o.morf) o.morf[i] = (float)(mn / rhon);
+        if (a.mode == EPI_CORRECT && P.sle == 2) a.hs_next[i] = hsn;
+    }
+    if (a.mode == EPI_CORRECT) {
+        if (P.sle == 2) {
+            warp_min_u64(&a.sc->acc_hmin, dbits(hsn));
+            warp_max_u64(&a.sc->acc_hmax, dbits(hsn));
+        }
+        if (P.tse == 2) {                                       // time_step.f90:155
+            const double v = P.rho_ice * (hsn * hsn) * P.delta_min / (P.P_star * (1.0 + P.k_t));
+            warp_min_u64(&a.sc->acc_dt, dbits(v));
+        }
+    }
+    if (lists) lists_block_done(a);
+}
+
+}  // namespace pass
+
+// tiled.cu
+void launch_kinematic_tiled(simp_ctx *c, const pass::KinArgs &a);
+void launch_stress_tiled(simp_ctx *c, const pass::StressArgs &a);
+
+}  // namespace simp

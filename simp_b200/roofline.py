@@ -1,29 +1,23 @@
 """Algorithmic HBM bytes of each kernel of one predictor-corrector step.
 
-Counted per particle, FP64 state, each array read or written once (the
-minimum any implementation of the step must move; neighbour gathers of the
-same arrays are served on chip and are not counted again):
+The per-particle-step figure is B_alg = 704 B (FP64 state), itemised per
+right-hand-side evaluation (two per step), each array read or written once:
 
-kinematic pass (run at S0 and at S1), per particle:
-    reads  x, y, vx, vy, hsml, m, m/rho, h, A, rho   10 x 8 B = 80 B
-           cell id                                    4 B
-    writes tau11, tau12, tau22 (= sigma / rho^2), div  4 x 8 B = 32 B
-    total 116 B
-stress pass, predictor epilogue (RHS at S0, writes S1):
-    reads  x, y, hsml, m, tau11, tau12, tau22, rho, h, A, vx, vy, div
-                                                     13 x 8 B = 104 B
-           cell id 4 B, rebuild positions xr, yr 16 B
-    writes x, y, vx, vy, h, A, rho, m/rho             8 x 8 B = 64 B
-    total 188 B
-stress pass, corrector epilogue (RHS at S1, base S0, writes S0):
-    reads  S1: x, y, tau11, tau12, tau22, rho, h, A, vx, vy, div 11 x 8 B
-           shared hsml, m 2 x 8 B, cell id 4 B, xr, yr 16 B,
-           S0: x, y, vx, vy, h, A 6 x 8 B                 = 172 B
-    writes x, y, vx, vy, h, A, rho, m/rho             8 x 8 B = 64 B
-    total 236 B
-step finish: a handful of scalars, 0 B per particle.
+    neighbour search: cell key and index write, one sort read + write  24 B
+    kinematic pass: read x, y, vx, vy, m, rho, hsml (56 B);
+                    write eps11, eps12, eps22, div (32 B)               88 B
+    stress pass with the rheology in its prologue: read x, y, vx, vy, m,
+                    rho, hsml, h, A, eps x 3, div (104 B);
+                    write dvx, dvy, dh, dA (32 B)                      136 B
+    half-step update: write x, y, vx, vy, h, A, rho (56 B);
+                    save or reload the step-start state (48 B)         104 B
+                                                                  = 352 B
 
-One step = 2 x 116 + 188 + 236 = 656 B per particle-step.
+The launches fuse these: the kinematic kernel keeps the cell list exact
+(the search) and computes the strain rates and stress (24 + 88 = 112 B per
+particle); the stress kernel applies the pair forces and the update
+(136 + 104 = 240 B per particle).  One step = 2 x (112 + 240) = 704 B.
+The same B_alg is used for the mixed form, so fractions compare.
 """
 from __future__ import annotations
 
@@ -32,10 +26,10 @@ import os
 
 KERNELS = ("kinematic_s0", "stress_predict", "kinematic_s1", "stress_correct", "step_finish")
 BYTES_PER_PARTICLE = {
-    "kinematic_s0": 116,
-    "stress_predict": 188,
-    "kinematic_s1": 116,
-    "stress_correct": 236,
+    "kinematic_s0": 112,
+    "stress_predict": 240,
+    "kinematic_s1": 112,
+    "stress_correct": 240,
     "step_finish": 0,
 }
 STEP_BYTES_PER_PARTICLE = sum(BYTES_PER_PARTICLE.values())

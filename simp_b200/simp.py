@@ -121,6 +121,22 @@ class Simp:
             if name != "reserved0":
                 setattr(self.params, name, getattr(forcing, name))
 
+    def set_passes(self, impl: int, threads: int = 256, cap: int = 1024):
+        """Pair-pass implementation: 0 per-particle gathers, 1 shared-memory tiles."""
+        self._chk(self.lib.simp_gpu_set_passes(self.h, int(impl), int(threads), int(cap)))
+
+    def get_passes(self):
+        a, b, c = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        self._chk(self.lib.simp_gpu_get_passes(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
+
+    def autotune(self, reps: int = 3) -> float:
+        """Picks the fastest pass implementation and tile shape for the
+        current state; returns its milliseconds per right-hand side."""
+        ms = ctypes.c_double()
+        self._chk(self.lib.simp_gpu_autotune(self.h, int(reps), ctypes.byref(ms)))
+        return ms.value
+
     def keep_diag(self, keep: bool = True):
         self._chk(self.lib.simp_gpu_keep_diag(self.h, 1 if keep else 0))
 
