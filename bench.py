@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--forms", default="mixed,batched,served",
                     help="comma list of the other forms to measure on rank 0 ('' for none)")
-    ap.add_argument("--served-requests", type=int, default=32)
+    ap.add_argument("--served-requests", type=int, default=48)
     ap.add_argument("--served-steps-scale", type=float, default=0.25)
     return ap.parse_args()
 
@@ -349,11 +349,13 @@ def run_forms(args, which):
             "steps": args.steps, "launches_per_step": launches / args.steps,
             "l2": "not flushed: one call of K steps; working set > 126 MB L2"}
     if "served" in which:
-        reqs = serve.sample_stream(args.served_requests, seed=5, rate_hz=20.0,
+        # offered load well above either arm's capacity (arrivals within a
+        # fraction of a second), so the makespan measures capacity
+        reqs = serve.sample_stream(args.served_requests, seed=5, rate_hz=100.0,
                                    steps_scale=args.served_steps_scale)
         big = max(r.basin.n for r in reqs)
         with serve.Server(reqs[0].basin.params, 150e9, max_instances=256, max_request_particles=big,
-                          quantum_steps=16, spot_every=8) as srv:
+                          quantum_steps=32, spot_every=8) as srv:
             ids = [srv.submit(r) for r in reqs]
             srv.run()
             sst = srv.stats()
@@ -364,7 +366,7 @@ def run_forms(args, which):
         ser = serve.serial_fp64(reqs)
         served_value = sst["particle_steps"] / sst["makespan_s"]
         out["served_stream"] = {
-            "workload": (f"{len(reqs)} requests, Poisson 20/s, particles log-uniform 1,024..1,048,576, "
+            "workload": (f"{len(reqs)} requests, Poisson 100/s, particles log-uniform 1,024..1,048,576, "
                          f"steps U(100, 2000) x {args.served_steps_scale}, dx=1 km, dt=1e-4 s, mixed, "
                          "HBM budget 150 GB, FP64 replica of every 8th request"),
             "metric": METRIC, "value": served_value, "p50_s": float(np.percentile(lat, 50)),

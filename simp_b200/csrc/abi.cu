@@ -52,10 +52,7 @@ __global__ void k_init_new(int n, int off, int id_base, int slot, int *id, int *
     xr[i] = s.x[i];
     yr[i] = s.y[i];
     s.mor[i] = s.m[i] / s.rho[i];
-    if (s.mf) {
-        s.mf[i] = (float)s.m[i];
-        s.morf[i] = (float)s.mor[i];
-    }
+    refresh_views(s, i);
 }
 
 __global__ void k_mark_removed(int n, int slot, int *pinst) {
@@ -178,9 +175,10 @@ void free_all(simp_ctx *c) {
                     c->bid, c->binst, c->bcell, c->bcell_start, c->cell_start, c->cnt, c->perm, c->tmp,
                     c->itmp, c->scan_tmp, c->sc, c->pair_cnt, c->bpair_cnt, c->pair_buf_i,
                     c->pair_buf_j, c->pair_buf_r, c->pair_buf_h, c->nbr, c->nbr_count,
-                    c->pair_j, c->pair_count, c->nbr_tmp, c->s0.xf, c->s0.yf, c->s0.hsf, c->s1.xf, c->s1.yf,
-                    c->inst_dev, c->row_map, c->chunk_cnt, c->chunk_off, c->chunks, c->s0.mf, c->s0.morf,
-                    c->s1.morf, c->mass1f, c->tau11f, c->tau12f, c->tau22f};
+                    c->pair_j, c->pair_count, c->nbr_tmp, c->s0.hsf,
+                    c->inst_dev, c->row_map, c->chunk_cnt, c->chunk_off, c->chunks, c->s0.xy, c->s0.vxy,
+                    c->s0.pf, c->s0.mm, c->s0.hmm, c->s1.xy, c->s1.vxy, c->s1.pf, c->s1.mm, c->s1.hmm,
+                    c->tau_a, c->tau_b, c->tau_q};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->sc_host) cudaFreeHost(c->sc_host);
@@ -619,19 +617,21 @@ int create(const simp_params *params, int32_t maxn, int32_t maxnb, int32_t max_i
         c->s1.m = c->s0.m;
     }
     c->s1.hs = c->s0.hs;
-    float **f1[] = {&c->s0.xf, &c->s0.yf, &c->s0.hsf, &c->s1.xf, &c->s1.yf};
-    for (float **p : f1) TRY(dalloc(c, p, M));
+    TRY(dalloc(c, &c->s0.hsf, M));
     c->s1.hsf = c->s0.hsf;
+    // packed neighbour copies of both state sets, and the stress records
+    for (State *st : {&c->s0, &c->s1}) {
+        TRY(dalloc(c, &st->xy, M));
+        TRY(dalloc(c, &st->vxy, M));
+        TRY(dalloc(c, &st->pf, M));
+        if (c->prm.precision == SIMP_PREC_MIXED) TRY(dalloc(c, &st->hmm, M));
+        else TRY(dalloc(c, &st->mm, M));
+    }
     if (c->prm.precision == SIMP_PREC_MIXED) {
-        // FP32 copies the mixed form's pair arithmetic reads
-        float **f2[] = {&c->s0.mf, &c->s0.morf, &c->s1.morf, &c->tau11f, &c->tau12f, &c->tau22f};
-        for (float **p : f2) TRY(dalloc(c, p, M));
-        if (c->mass1) {
-            TRY(dalloc(c, &c->mass1f, M));
-            c->s1.mf = c->mass1f;
-        } else {
-            c->s1.mf = c->s0.mf;
-        }
+        TRY(dalloc(c, &c->tau_q, M));
+    } else {
+        TRY(dalloc(c, &c->tau_a, M));
+        TRY(dalloc(c, &c->tau_b, M));
     }
     TRY(dalloc(c, &c->nbr, (size_t)kMaxNbr * M));
     TRY(dalloc(c, &c->nbr_count, M));

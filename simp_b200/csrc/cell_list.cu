@@ -279,13 +279,7 @@ __global__ void k_put_back(int kept, int all, DueMask due, Gather gd, State s, c
     for (int a = 0; a < kGathered; ++a) const_cast<double *>(gd.src[a])[k] = gd.dst[a][k];
     id[k] = id_new[k];
     pinst[k] = pinst_new[k];
-    s.xf[k] = (float)s.x[k];
-    s.yf[k] = (float)s.y[k];
-    s.hsf[k] = (float)s.hs[k];
-    if (s.mf) {
-        s.mf[k] = (float)s.m[k];
-        s.morf[k] = (float)s.mor[k];
-    }
+    refresh_views(s, k);
 }
 
 // After a sort: displacement since the sort restarts; the Verlet lists are

@@ -22,9 +22,26 @@ struct State {
     double *x, *y, *vx, *vy;
     double *m, *rho, *mor, *h, *A;
     double *hs;   // hsml (shared by S0 and S1: updated only at step end)
-    float *xf, *yf, *hsf;  // FP32 copies for the candidate prefilter (hsf shared)
-    float *mf, *morf;      // FP32 copies of m and m / rho (mixed precision only, else null)
+    float *hsf;   // its FP32 copy (shared)
+    // Packed copies that the pair passes gather per neighbour (one or two
+    // vector loads per neighbour instead of one scalar load per array):
+    double2 *xy, *vxy;   // (x, y), (vx, vy)
+    float4 *pf;          // (x, y, hsml, 0) in FP32: the candidate prefilter
+    double2 *mm;         // (m, m / rho): plain form (null in the mixed form)
+    float4 *hmm;         // (hsml, m, m / rho, 0) in FP32: mixed form (null in the plain form)
 };
+
+// Rewrites the packed copies of particle k from the FP64 arrays.
+__device__ __forceinline__ void refresh_views(const State &s, int k) {
+    const double x = s.x[k], y = s.y[k], hs = s.hs[k], m = s.m[k], mor = s.mor[k];
+    const float hsf = (float)hs;
+    s.hsf[k] = hsf;
+    s.xy[k] = make_double2(x, y);
+    s.vxy[k] = make_double2(s.vx[k], s.vy[k]);
+    s.pf[k] = make_float4((float)x, (float)y, hsf, 0.0f);
+    if (s.hmm) s.hmm[k] = make_float4(hsf, (float)m, (float)mor, 0.0f);
+    else s.mm[k] = make_double2(m, mor);
+}
 
 // Verlet neighbour lists (cell-order indices): nbr[k * stride + i],
 // k < count[i], holding every j within mhsml + skin of i at the positions

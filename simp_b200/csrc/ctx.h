@@ -50,8 +50,9 @@ struct simp_ctx {
     int *pinst = nullptr;          // instance slot of each particle (-1: being removed)
     // per-RHS intermediates from the kinematic pass
     double *tau11 = nullptr, *tau12 = nullptr, *tau22 = nullptr, *div = nullptr;
-    float *tau11f = nullptr, *tau12f = nullptr, *tau22f = nullptr;   // mixed precision only
-    float *mass1f = nullptr;       // FP32 half-step mass (mixed precision with the mass update)
+    // the stress pass's packed neighbour records (written by the kinematic pass)
+    double2 *tau_a = nullptr, *tau_b = nullptr;   // plain form: (tau11, tau12), (tau22, m)
+    float4 *tau_q = nullptr;                      // mixed form: (tau11, tau12, tau22, m)
     int *nbr = nullptr;            // kMaxNbr * maxn neighbour indices (column-major)
     int *nbr_count = nullptr;      // maxn
     int *nbr_tmp = nullptr;        // kMaxNbr * maxn: lists being renamed by a sort

@@ -139,9 +139,10 @@ __device__ __forceinline__ PairCtx pair_ctx(const State &s, const Scalars *sc, c
     p.xi = s.x[i];
     p.yi = s.y[i];
     p.hi = s.hs[i];
-    p.xif = s.xf[i];
-    p.yif = s.yf[i];
-    p.hif = s.hsf[i];
+    const float4 f = s.pf[i];
+    p.xif = f.x;
+    p.yif = f.y;
+    p.hif = f.z;
     p.margin = prefilter_margin(bitsd(sc->xabs_bits), I.hmin);
     p.use_f32 = p.margin < 0.25f;
     p.br = make_bin_rule(I.bs, p.xi, p.yi, I.hmax);
@@ -155,10 +156,14 @@ __device__ __forceinline__ PairCtx pair_ctx(const State &s, const Scalars *sc, c
 // the FP64 test of nnps.f90:277-281 when undecided, then the bucket rule.
 __device__ __forceinline__ bool is_pair(const State &s, const PairCtx &p, int j) {
     int dec = 2;
-    if (p.use_f32) dec = prefilter(p.xif - s.xf[j], p.yif - s.yf[j], 0.5f * (p.hif + s.hsf[j]), p.margin);
+    if (p.use_f32) {
+        const float4 f = s.pf[j];
+        dec = prefilter(p.xif - f.x, p.yif - f.y, 0.5f * (p.hif + f.z), p.margin);
+    }
     if (dec == 0) return false;
     if (dec == 2 || p.br.on) {
-        const double xj = s.x[j], yj = s.y[j];
+        const double2 q = s.xy[j];
+        const double xj = q.x, yj = q.y;
         if (dec == 2) {
             double r;
             const double mh = __dmul_rn(__dadd_rn(p.hi, s.hs[j]), 0.5);
@@ -203,23 +208,48 @@ __device__ __forceinline__ void for_each_current_pair(const State &s, const NbrL
     }
 }
 
-// Neighbour values in the pair arithmetic type: the FP64 arrays for the
-// plain form, their FP32 copies for the mixed form.
+// Per-neighbour scalars in the pair arithmetic type: the FP64 arrays for
+// the plain form, the packed FP32 copies for the mixed form.
+template <class T>
+struct KinNb {
+    T h, m, mor;
+};
+template <class T>
+struct StressNb {
+    T h, m, t11, t12, t22;
+};
+// Packed stress-pass neighbour records written by the kinematic pass:
+// plain form (tau11, tau12), (tau22, m); mixed form (tau11, tau12, tau22, m).
+struct TauRec {
+    double2 *ta, *tb;   // plain form
+    float4 *tq;         // mixed form
+};
+
 template <class T>
 struct Nb;
 template <>
 struct Nb<double> {
     static __device__ __forceinline__ double h(const State &s, int j) { return s.hs[j]; }
-    static __device__ __forceinline__ double m(const State &s, int j) { return s.m[j]; }
-    static __device__ __forceinline__ double mor(const State &s, int j) { return s.mor[j]; }
-    static __device__ __forceinline__ double tau(const double *t, const float *, int j) { return t[j]; }
+    static __device__ __forceinline__ KinNb<double> kin(const State &s, int j) {
+        const double2 q = s.mm[j];
+        return {s.hs[j], q.x, q.y};
+    }
+    static __device__ __forceinline__ StressNb<double> stress(const State &s, const TauRec &t, int j) {
+        const double2 a = t.ta[j], b = t.tb[j];
+        return {s.hs[j], b.y, a.x, a.y, b.x};
+    }
 };
 template <>
 struct Nb<float> {
     static __device__ __forceinline__ float h(const State &s, int j) { return s.hsf[j]; }
-    static __device__ __forceinline__ float m(const State &s, int j) { return s.mf[j]; }
-    static __device__ __forceinline__ float mor(const State &s, int j) { return s.morf[j]; }
-    static __device__ __forceinline__ float tau(const double *, const float *tf, int j) { return tf[j]; }
+    static __device__ __forceinline__ KinNb<float> kin(const State &s, int j) {
+        const float4 q = s.hmm[j];
+        return {q.x, q.y, q.z};
+    }
+    static __device__ __forceinline__ StressNb<float> stress(const State &s, const TauRec &t, int j) {
+        const float4 q = t.tq[j];
+        return {s.hsf[j], q.w, q.x, q.y, q.z};
+    }
 };
 
 // Kinematic-pass pair terms (kernel.f90:515-518, vector_divergence.f90:27,
@@ -262,7 +292,7 @@ struct KinArgs {
     Phys P;
     Scalars *sc;
     double *tau11, *tau12, *tau22, *div;
-    float *tau11f, *tau12f, *tau22f;   // FP32 copies (mixed precision only)
+    TauRec rec;            // the stress pass's neighbour records (written here)
     double *diag;
     NbrList nl;
     PairList pl;
@@ -306,10 +336,11 @@ __device__ __forceinline__ void kin_rheology(const KinArgs &a, int i, double dv,
     a.tau11[i] = s11 * ir2;
     a.tau12[i] = s12 * ir2;
     a.tau22[i] = s22 * ir2;
-    if (a.tau11f) {
-        a.tau11f[i] = (float)(s11 * ir2);
-        a.tau12f[i] = (float)(s12 * ir2);
-        a.tau22f[i] = (float)(s22 * ir2);
+    if (a.rec.tq) {
+        a.rec.tq[i] = make_float4((float)(s11 * ir2), (float)(s12 * ir2), (float)(s22 * ir2), (float)s.m[i]);
+    } else {
+        a.rec.ta[i] = make_double2(s11 * ir2, s12 * ir2);
+        a.rec.tb[i] = make_double2(s22 * ir2, s.m[i]);
     }
     a.div[i] = dv;
     if (a.diag) {
@@ -340,7 +371,7 @@ struct StressArgs {
     Phys P;
     Scalars *sc;
     const double *tau11, *tau12, *tau22, *div;
-    const float *tau11f, *tau12f, *tau22f;
+    TauRec rec;
     NbrList nl;
     PairList pl;
     double *rates;
@@ -402,6 +433,45 @@ __device__ __forceinline__ void warp_max_i32(int *dst, int v) {
         atomicMax(dst, v);
     }
     __syncthreads();
+}
+
+// The per-step bounds of the stress pass in one block-wide reduction (a warp
+// shuffle per value, one barrier, one atomic per value and block):
+// maxip (max), the list displacement (max), max |coordinate| (max), the next
+// hsml minimum and maximum, and the VP time step (min).  Values whose bit in
+// `active` is clear are skipped.  Every thread of the block calls it.
+constexpr int kBounds = 6;
+__device__ __forceinline__ void block_bounds(Scalars *sc, unsigned active, unsigned long long (&v)[kBounds]) {
+    __shared__ unsigned long long part[32][kBounds];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < kBounds; ++q) {
+        if (!((active >> q) & 1u)) continue;
+        const bool mn = (q == 3 || q == 5);
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long t = __shfl_xor_sync(0xffffffffu, v[q], o);
+            v[q] = mn ? (t < v[q] ? t : v[q]) : (t > v[q] ? t : v[q]);
+        }
+        if (lane == 0) part[w][q] = v[q];
+    }
+    __syncthreads();
+    const int q = threadIdx.x;
+    if (q < kBounds && ((active >> q) & 1u)) {
+        const bool mn = (q == 3 || q == 5);
+        unsigned long long r = part[0][q];
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) {
+            const unsigned long long t = part[k][q];
+            r = mn ? (t < r ? t : r) : (t > r ? t : r);
+        }
+        switch (q) {
+            case 0: atomicMax(&sc->maxip, (int)r); break;
+            case 1: atomicMax(&sc->dlist2_bits, r); break;
+            case 2: atomicMax(&sc->xabs_bits, r); break;
+            case 3: atomicMin(&sc->acc_hmin, r); break;
+            case 4: atomicMax(&sc->acc_hmax, r); break;
+            default: atomicMin(&sc->acc_dt, r); break;
+        }
+    }
 }
 
 // The last block of a stress pass to finish decides whether the next
@@ -481,9 +551,8 @@ __device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool l
     const double dv = a.div[i];
     const double dhdt = -hh * dv / rho;
     const double dAdt = -AA * dv / rho;
-    warp_max_i32(&a.sc->maxip, live ? cnt : 0);
-
     if (a.mode == EPI_RATES) {
+        warp_max_i32(&a.sc->maxip, live ? cnt : 0);
         if (live) {
             const size_t M = (size_t)a.maxn;
             a.rates[i] = ax;
@@ -536,15 +605,14 @@ __device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool l
     double d2 = dxr * dxr + dyr * dyr;
     if (!live || !isfinite(d2)) d2 = 0.0;
     inst_max_u64(a.inst, ki, offsetof(Inst, dmax2_bits), dbits(d2));
+    double dl2 = 0.0;
     if (lists) {
         const double dxl = xn - a.nl.xl[i], dyl = yn - a.nl.yl[i];
-        double dl2 = dxl * dxl + dyl * dyl;
+        dl2 = dxl * dxl + dyl * dyl;
         if (!live || !isfinite(dl2)) dl2 = 0.0;
-        warp_max_u64(&a.sc->dlist2_bits, dbits(dl2));
     }
     double xa = fmax(fabs(xn), fabs(yn));
     if (!isfinite(xa)) xa = 0.0;
-    warp_max_u64(&a.sc->xabs_bits, dbits(xa));
     const bool bad = !(isfinite(xn) && isfinite(yn) && isfinite(vxn) && isfinite(vyn) &&
                        isfinite(hn) && isfinite(An));
     if (live && bad) {
@@ -553,33 +621,39 @@ __device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool l
     }
     if (live) {
         const State &o = a.out;
+        const double morn = mn / rhon;
         o.x[i] = xn;
         o.y[i] = yn;
-        o.xf[i] = (float)xn;
-        o.yf[i] = (float)yn;
         o.vx[i] = vxn;
         o.vy[i] = vyn;
         o.h[i] = hn;
         o.A[i] = An;
         o.rho[i] = rhon;
-        if (P.sle != 2 && P.mass_from_area) {
-            o.m[i] = mn;
-            if (o.mf) o.mf[i] = (float)mn;
-        }
-        o.mor[i] = mn / rhon;
-        if (o.morf) o.morf[i] = (float)(mn / rhon);
+        if (P.sle != 2 && P.mass_from_area) o.m[i] = mn;
+        o.mor[i] = morn;
+        const float hsf = (float)hs_old;
+        o.xy[i] = make_double2(xn, yn);
+        o.vxy[i] = make_double2(vxn, vyn);
+        o.pf[i] = make_float4((float)xn, (float)yn, hsf, 0.0f);
+        if (o.hmm) o.hmm[i] = make_float4(hsf, (float)mn, (float)morn, 0.0f);
+        else o.mm[i] = make_double2(mn, morn);
         if (a.mode == EPI_CORRECT && P.sle == 2) a.hs_next[i] = hsn;
     }
-    if (a.mode == EPI_CORRECT) {
-        if (P.sle == 2) {
-            warp_min_u64(&a.sc->acc_hmin, dbits(hsn));
-            warp_max_u64(&a.sc->acc_hmax, dbits(hsn));
-        }
-        if (P.tse == 2) {                                       // time_step.f90:155
-            const double v = P.rho_ice * (hsn * hsn) * P.delta_min / (P.P_star * (1.0 + P.k_t));
-            warp_min_u64(&a.sc->acc_dt, dbits(v));
-        }
+    // this step's bounds, one block-wide reduction
+    const bool corr = a.mode == EPI_CORRECT;
+    unsigned active = 1u | (lists ? 2u : 0u) | 4u;
+    unsigned long long v[kBounds] = {(unsigned long long)(live ? cnt : 0), dbits(dl2), dbits(xa), ~0ull, 0ull,
+                                     ~0ull};
+    if (corr && P.sle == 2) {                                   // smoothing_length.f90:136-142
+        active |= 8u | 16u;
+        v[3] = dbits(hsn);
+        v[4] = dbits(hsn);
     }
+    if (corr && P.tse == 2) {                                   // time_step.f90:155
+        active |= 32u;
+        v[5] = dbits(P.rho_ice * (hsn * hsn) * P.delta_min / (P.P_star * (1.0 + P.k_t)));
+    }
+    block_bounds(a.sc, active, v);
     if (lists) lists_block_done(a);
 }
 

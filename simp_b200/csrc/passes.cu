@@ -16,12 +16,22 @@ using namespace pass;
 constexpr int kBlock = 128;
 // minimum resident blocks per SM (register caps 73 and 64): more warps in
 // flight to hide the latency of the neighbour gathers
-constexpr int kMinBlocksKin = 7;
-constexpr int kMinBlocksStress = 8;
+#ifndef SIMP_KIN_MIN_BLOCKS
+#define SIMP_KIN_MIN_BLOCKS 7
+#endif
+#ifndef SIMP_STRESS_MIN_BLOCKS
+#define SIMP_STRESS_MIN_BLOCKS 8
+#endif
+constexpr int kMinBlocksKin = SIMP_KIN_MIN_BLOCKS;
+constexpr int kMinBlocksStress = SIMP_STRESS_MIN_BLOCKS;
+// per-thread pair list in shared memory: a typical particle's pairs fit;
+// a longer list is processed in batches.  Kept small: the shared memory of
+// the resident blocks comes out of the L1 cache that serves the gathers.
+constexpr int kGatherSlots = 24;
 
 template <class T>
 __global__ void __launch_bounds__(kBlock, kMinBlocksKin) k_kinematic(KinArgs a) {
-    __shared__ int s_list[kListSlots * kBlock];
+    __shared__ int s_list[kGatherSlots * kBlock];
     const int t = threadIdx.x;
     const int i = blockIdx.x * blockDim.x + t;
     if (i >= a.n) return;
@@ -39,20 +49,24 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksKin) k_kinematic(KinArgs a) 
     const T hiT = Nb<T>::h(s, i), inv_hiT = (T)inv_hi;
     int cnt = 0;       // entries in this thread's shared-memory list
     int npairs = 0;    // exact pairs found so far
+    int done = 0;      // pairs already processed (and written to the pair list)
     auto flush = [&]() {
 #pragma unroll 4
         for (int k = 0; k < cnt; ++k) {
             const int j = s_list[k * kBlock + t];
-            const PairGeom<T> pg = pair_geom<T, false>(P, (T)(xi - s.x[j]), (T)(yi - s.y[j]), hiT, inv_hiT,
-                                                       Nb<T>::h(s, j));
-            ks.add(pg, (T)(vxi - s.vx[j]), (T)(vyi - s.vy[j]), Nb<T>::m(s, j), Nb<T>::mor(s, j));
+            if (done + k < kMaxPairs) a.pl.pj[(size_t)(done + k) * a.pl.stride + i] = j;
+            const double2 q = s.xy[j], v = s.vxy[j];
+            const KinNb<T> nb = Nb<T>::kin(s, j);
+            const PairGeom<T> pg = pair_geom<T, false>(P, (T)(xi - q.x), (T)(yi - q.y), hiT, inv_hiT, nb.h);
+            ks.add(pg, (T)(vxi - v.x), (T)(vyi - v.y), nb.m, nb.mor);
         }
+        done += cnt;
         cnt = 0;
     };
     auto on_pair = [&](int j) {
         s_list[cnt * kBlock + t] = j;
         ++npairs;
-        if (++cnt == kListSlots) flush();   // more than kMaxPairs pairs: no pair list
+        if (++cnt == kGatherSlots) flush();
     };
     if (a.sc->list_scan && i == 0) atomicExch(&a.sc->dlist2_bits, 0ull);
     if (dead) {
@@ -68,8 +82,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksKin) k_kinematic(KinArgs a) 
         const float skinf = (float)skin, grow = 1.0f + pc.margin;
         int total = 0;
         for_stencil(pc.g, i, a.cell[i], stencil_radius(pc.hmax, pc.dmax2_bits, pc.g, pc.hmax + skin), [&](int j) {
-            const float dxf = pc.xif - s.xf[j], dyf = pc.yif - s.yf[j];
-            const float lim = 0.5f * (pc.hif + s.hsf[j]) + skinf;
+            const float4 f = s.pf[j];
+            const float dxf = pc.xif - f.x, dyf = pc.yif - f.y;
+            const float lim = 0.5f * (pc.hif + f.z) + skinf;
             if (dxf * dxf + dyf * dyf > lim * lim * grow) return;
             if (total < kMaxNbr) a.nl.nbr[(size_t)total * a.nl.stride + i] = j;
             ++total;
@@ -81,11 +96,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksKin) k_kinematic(KinArgs a) 
     } else {
         for_each_current_pair(s, a.nl, a.sc, i, a.cell[i], pc, on_pair);
     }
-    // the stress pass's pair list, one coalesced row per k
-    if (npairs <= kMaxPairs)
-        for (int k = 0; k < cnt; ++k) a.pl.pj[(size_t)k * a.pl.stride + i] = s_list[k * kBlock + t];
+    flush();   // (also writes the stress pass's pair list, a coalesced row per k)
     a.pl.count[i] = npairs;
-    flush();
     kin_rheology(a, i, -ks.dv.get(), -ks.g1.get(), -ks.g2.get(), -ks.g3.get(), -ks.g4.get());
 }
 
@@ -105,10 +117,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksStress) k_stress(StressArgs 
     StressSums<T> ss;
     const T hiT = Nb<T>::h(s, i), inv_hiT = (T)inv_hi;
     auto accumulate = [&](int j) {
-        const PairGeom<T> pg = pair_geom<T, false>(P, (T)(xi - s.x[j]), (T)(yi - s.y[j]), hiT, inv_hiT,
-                                                   Nb<T>::h(s, j));
-        ss.add(pg, Nb<T>::m(s, j), Nb<T>::tau(a.tau11, a.tau11f, j), Nb<T>::tau(a.tau12, a.tau12f, j),
-               Nb<T>::tau(a.tau22, a.tau22f, j));
+        const double2 q = s.xy[j];
+        const StressNb<T> nb = Nb<T>::stress(s, a.rec, j);
+        const PairGeom<T> pg = pair_geom<T, false>(P, (T)(xi - q.x), (T)(yi - q.y), hiT, inv_hiT, nb.h);
+        ss.add(pg, nb.m, nb.t11, nb.t12, nb.t22);
     };
     int cnt = a.pl.count[i];
     if (cnt <= kMaxPairs) {
@@ -130,13 +142,15 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksStress) k_stress(StressArgs 
 }
 
 // New hsml of the next step (sle = 2) and its FP32 copy.
-__global__ void k_commit_hsml(int n, const double *__restrict__ hs_next, double *__restrict__ hs,
-                              float *__restrict__ hsf) {
+__global__ void k_commit_hsml(int n, const double *__restrict__ hs_next, State s0) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double v = hs_next[i];
-    hs[i] = v;
-    hsf[i] = (float)v;
+    const float vf = (float)v;
+    s0.hs[i] = v;
+    s0.hsf[i] = vf;
+    s0.pf[i].z = vf;
+    if (s0.hmm) s0.hmm[i].x = vf;
 }
 
 // End of a predictor-corrector step: time_step's new dt, current_time += dt
@@ -190,6 +204,14 @@ NbrList nbr_list(simp_ctx *c) {
     return nl;
 }
 
+TauRec tau_rec(simp_ctx *c) {
+    TauRec r;
+    r.ta = c->tau_a;
+    r.tb = c->tau_b;
+    r.tq = c->tau_q;
+    return r;
+}
+
 PairList pair_list(simp_ctx *c) {
     PairList pl;
     pl.pj = c->pair_j;
@@ -213,9 +235,7 @@ void launch_kinematic(simp_ctx *c, const State &s, bool diag) {
     a.tau12 = c->tau12;
     a.tau22 = c->tau22;
     a.div = c->div;
-    a.tau11f = c->tau11f;
-    a.tau12f = c->tau12f;
-    a.tau22f = c->tau22f;
+    a.rec = tau_rec(c);
     a.diag = diag ? c->diag : nullptr;
     a.nl = nbr_list(c);
     a.pl = pair_list(c);
@@ -252,9 +272,7 @@ void launch_stress(simp_ctx *c, const State &rhs, const State &base, EpiMode mod
     a.tau12 = c->tau12;
     a.tau22 = c->tau22;
     a.div = c->div;
-    a.tau11f = c->tau11f;
-    a.tau12f = c->tau12f;
-    a.tau22f = c->tau22f;
+    a.rec = tau_rec(c);
     a.nl = nbr_list(c);
     a.pl = pair_list(c);
     a.rates = c->rates;
@@ -277,7 +295,7 @@ void launch_stress(simp_ctx *c, const State &rhs, const State &base, EpiMode mod
 
 void launch_step_finish(simp_ctx *c) {
     if (c->prm.sle == 2) {
-        k_commit_hsml<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->n, c->tmp, c->s0.hs, c->s0.hsf);
+        k_commit_hsml<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->n, c->tmp, c->s0);
         c->launches += 1;
     }
     k_step_finish<<<1, kFinishThreads, 0, c->stream>>>(c->sc, c->inst_dev, c->ninst, c->prm.tse, c->prm.sle);

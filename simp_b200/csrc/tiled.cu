@@ -189,15 +189,17 @@ __global__ void __launch_bounds__(kMaxTileThreads) k_kin_tiled(KinArgs a) {
     const KinTile<T> tl = kin_tile<T>(smem, a.cap);
     if (fits) {
         for_halo(h, [&](int j, int k) {
-            tl.x[k] = s.x[j];
-            tl.y[k] = s.y[j];
+            const double2 q = s.xy[j], v = s.vxy[j];
+            const KinNb<T> nb = Nb<T>::kin(s, j);
+            tl.x[k] = q.x;
+            tl.y[k] = q.y;
             tl.hs[k] = s.hs[j];
-            tl.vx[k] = s.vx[j];
-            tl.vy[k] = s.vy[j];
-            tl.pf[k] = make_float4(s.xf[j], s.yf[j], s.hsf[j], 0.0f);
-            tl.m[k] = Nb<T>::m(s, j);
-            tl.mor[k] = Nb<T>::mor(s, j);
-            tl.hT[k] = Nb<T>::h(s, j);
+            tl.vx[k] = v.x;
+            tl.vy[k] = v.y;
+            tl.pf[k] = s.pf[j];
+            tl.m[k] = nb.m;
+            tl.mor[k] = nb.mor;
+            tl.hT[k] = nb.h;
         });
     }
     __syncthreads();
@@ -319,15 +321,18 @@ __global__ void __launch_bounds__(kMaxTileThreads) k_kin_tiled(KinArgs a) {
         auto on_pair = [&](int j) {
             if (npairs < kMaxPairs) pl.pj[(size_t)npairs * pl.stride + i] = j;
             ++npairs;
-            pair_terms(s.x[j], s.y[j], Nb<T>::h(s, j), s.vx[j], s.vy[j], Nb<T>::m(s, j), Nb<T>::mor(s, j));
+            const double2 q = s.xy[j], v = s.vxy[j];
+            const KinNb<T> nb = Nb<T>::kin(s, j);
+            pair_terms(q.x, q.y, nb.h, v.x, v.y, nb.m, nb.mor);
         };
         if (scan) {
             const float skinf = (float)skin, grow = 1.0f + pc.margin;
             int total = 0;
             const Grid g = inst_grid(I, a.cell_start);
             for_stencil(g, i, a.cell[i], stencil_radius(I.hmax, I.dmax2_bits, g, I.hmax + skin), [&](int j) {
-                const float dxf = pc.xif - s.xf[j], dyf = pc.yif - s.yf[j];
-                const float lim = 0.5f * (pc.hif + s.hsf[j]) + skinf;
+                const float4 f = s.pf[j];
+                const float dxf = pc.xif - f.x, dyf = pc.yif - f.y;
+                const float lim = 0.5f * (pc.hif + f.z) + skinf;
                 if (dxf * dxf + dyf * dyf > lim * lim * grow) return;
                 if (total < kMaxNbr) nl.nbr[(size_t)total * nl.stride + i] = j;
                 ++total;
@@ -388,13 +393,15 @@ __global__ void __launch_bounds__(kMaxTileThreads) k_stress_tiled(StressArgs a) 
     const StressTile<T> tl = stress_tile<T>(smem, a.cap);
     if (fits) {
         for_halo(h, [&](int j, int k) {
-            tl.x[k] = s.x[j];
-            tl.y[k] = s.y[j];
-            tl.hT[k] = Nb<T>::h(s, j);
-            tl.m[k] = Nb<T>::m(s, j);
-            tl.t11[k] = Nb<T>::tau(a.tau11, a.tau11f, j);
-            tl.t12[k] = Nb<T>::tau(a.tau12, a.tau12f, j);
-            tl.t22[k] = Nb<T>::tau(a.tau22, a.tau22f, j);
+            const double2 q = s.xy[j];
+            const StressNb<T> nb = Nb<T>::stress(s, a.rec, j);
+            tl.x[k] = q.x;
+            tl.y[k] = q.y;
+            tl.hT[k] = nb.h;
+            tl.m[k] = nb.m;
+            tl.t11[k] = nb.t11;
+            tl.t12[k] = nb.t12;
+            tl.t22[k] = nb.t22;
         });
     }
     __syncthreads();
@@ -411,8 +418,9 @@ __global__ void __launch_bounds__(kMaxTileThreads) k_stress_tiled(StressArgs a) 
         ss.add(pair_geom<T, false>(P, (T)(xi - xj), (T)(yi - yj), hiT, inv_hiT, hj), mj, t11, t12, t22);
     };
     auto global_terms = [&](int j) {
-        terms(s.x[j], s.y[j], Nb<T>::h(s, j), Nb<T>::m(s, j), Nb<T>::tau(a.tau11, a.tau11f, j),
-              Nb<T>::tau(a.tau12, a.tau12f, j), Nb<T>::tau(a.tau22, a.tau22f, j));
+        const double2 q = s.xy[j];
+        const StressNb<T> nb = Nb<T>::stress(s, a.rec, j);
+        terms(q.x, q.y, nb.h, nb.m, nb.t11, nb.t12, nb.t22);
     };
     auto any_terms = [&](int j) {
         const int sl = fits ? slot_of(h, j) : -1;
