@@ -178,7 +178,7 @@ void free_all(simp_ctx *c) {
                     c->pair_j, c->pair_count, c->nbr_tmp, c->s0.hsf,
                     c->inst_dev, c->row_map, c->chunk_cnt, c->chunk_off, c->chunks, c->s0.xy, c->s0.vxy,
                     c->s0.pf, c->s0.mm, c->s0.hmm, c->s1.xy, c->s1.vxy, c->s1.pf, c->s1.mm, c->s1.hmm,
-                    c->tau_a, c->tau_b, c->tau_q};
+                    c->tau_a, c->tau_b, c->tau_q, c->pair_dw};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->sc_host) cudaFreeHost(c->sc_host);
@@ -638,6 +638,13 @@ int create(const simp_params *params, int32_t maxn, int32_t maxnb, int32_t max_i
     TRY(dalloc(c, &c->nbr_tmp, (size_t)kMaxNbr * M));
     TRY(dalloc(c, &c->pair_j, (size_t)kMaxPairs * M));
     TRY(dalloc(c, &c->pair_count, M));
+    if (c->prm.precision == SIMP_PREC_MIXED) {
+        // the mixed form keeps its pairs' kernel gradients for the stress
+        // pass (measured: in the plain form the 16-byte records cost the
+        // kinematic pass more than they save the stress pass)
+        if (cudaMalloc(&c->pair_dw, (size_t)kDwRows * M * sizeof(float2)) != cudaSuccess)
+            return simp_fail(c, SIMP_ERR_NOMEM, "device allocation failed");
+    }
     TRY(dalloc(c, &c->diag, 9 * M));
     TRY(dalloc(c, &c->rates, 4 * M));
     TRY(dalloc(c, &c->cell, M));
@@ -689,6 +696,24 @@ simp_forcing forcing_of(const simp_params &p) {
 }  // namespace
 
 namespace simp {
+
+// Device bytes per unit of maxn of a context with these parameters (the
+// allocations of create() below, with room for its cell lists).
+double bytes_per_particle(const simp_params &p) {
+    const bool mixed = p.precision == SIMP_PREC_MIXED;
+    double b = 26 * 8.0;                                      // FP64 state sets and per-RHS fields
+    if (p.mass_from_area && p.sle != 2) b += 8.0;             // half-step mass
+    b += 4.0;                                                 // hsml in FP32
+    b += 2 * (3 * 16.0 + 16.0);                               // packed neighbour copies, two sets
+    b += mixed ? 16.0 : 32.0;                                 // stress records
+    b += 2 * kMaxNbr * 4.0 + 4.0;                             // Verlet lists and their renaming copy
+    b += kMaxPairs * 4.0 + 4.0;                               // pair lists
+    b += mixed ? kDwRows * 8.0 : 0.0;                         // kept kernel gradients
+    b += 9 * 8.0 + 4 * 8.0;                                   // diagnostics, rates
+    b += 4 * 4.0 + 14 * 8.0 + 5 * 4.0 + 4.0;                  // sort keys, scratch
+    b += 16.0 / kMinTileThreads + 48.0;                       // chunks, cell lists (worst case)
+    return b;
+}
 
 // Enqueues nsteps steps of every basin of the context on its stream without
 // waiting for them (profiling mode waits step by step).

@@ -55,6 +55,11 @@ struct NbrList {
     int stride;
 };
 
+// The kernel gradients of a right-hand side's pairs, kept by the kinematic
+// pass for the stress pass (same pairs, same state): row k, particle i, for
+// the first kDwRows pairs of each particle (the others are recomputed).
+constexpr int kDwRows = 32;
+
 // Exact pairs of the current right-hand side, written by the kinematic pass
 // and consumed by the stress pass: pj[k * stride + i], k < count[i]; a count
 // above kMaxPairs means the stress pass finds that particle's pairs itself.

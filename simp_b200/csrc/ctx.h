@@ -59,6 +59,7 @@ struct simp_ctx {
     bool lists_valid = false;      // every particle's list was built by a kinematic pass
     int *pair_j = nullptr;         // kMaxPairs * maxn exact pairs of the current RHS
     int *pair_count = nullptr;     // maxn
+    void *pair_dw = nullptr;       // kernel gradient per pair: kDwRows x maxn float2 (mixed form only)
     // diagnostics (epsilon_11.. sigma_22, zeta, eta, p)
     double *diag = nullptr;        // 9 * maxn
     // rates of the last single_step (cell order): ax, ay, dhdt, dAdt
@@ -145,6 +146,9 @@ constexpr int kMinTileThreads = 64;
 void build_chunks(simp_ctx *c);
 int tiled_configure(simp_ctx *c);
 size_t tiled_smem_bytes(int precision, int pass, int cap, int threads);
+
+// abi.cu: device bytes per particle of capacity
+double bytes_per_particle(const simp_params &p);
 
 // abi.cu: the step driver split for callers that overlap contexts
 int step_enqueue(simp_ctx *c, int nsteps);

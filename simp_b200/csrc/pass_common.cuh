@@ -238,6 +238,10 @@ struct Nb<double> {
         const double2 a = t.ta[j], b = t.tb[j];
         return {s.hs[j], b.y, a.x, a.y, b.x};
     }
+    static __device__ __forceinline__ StressNb<double> stress_rec(const TauRec &t, int j) {
+        const double2 a = t.ta[j], b = t.tb[j];
+        return {0.0, b.y, a.x, a.y, b.x};
+    }
 };
 template <>
 struct Nb<float> {
@@ -250,6 +254,10 @@ struct Nb<float> {
         const float4 q = t.tq[j];
         return {s.hsf[j], q.w, q.x, q.y, q.z};
     }
+    static __device__ __forceinline__ StressNb<float> stress_rec(const TauRec &t, int j) {
+        const float4 q = t.tq[j];
+        return {0.0f, q.w, q.x, q.y, q.z};
+    }
 };
 
 // Kinematic-pass pair terms (kernel.f90:515-518, vector_divergence.f90:27,
@@ -257,8 +265,8 @@ struct Nb<float> {
 template <class T>
 struct KinSums {
     Sum<T> dv, g1, g2, g3, g4;
-    __device__ __forceinline__ void add(const PairGeom<T> &pg, T dvx, T dvy, T mj, T mrj) {
-        const T dwx = pg.gfac * pg.dx, dwy = pg.gfac * pg.dy;
+    // grad W_ij = (dwx, dwy)
+    __device__ __forceinline__ void add(T dwx, T dwy, T dvx, T dvy, T mj, T mrj) {
         const T w2 = dvy * dwx, w3 = dvx * dwy, w4 = dvy * dwy;
         const T w1 = dvx * dwx;
         dv.madd(mj, fma(dvx, dwx, w4));
@@ -274,13 +282,27 @@ struct KinSums {
 template <class T>
 struct StressSums {
     Sum<T> sx, sy, tx, ty;
-    __device__ __forceinline__ void add(const PairGeom<T> &pg, T mj, T t11, T t12, T t22) {
-        const T dwx = pg.gfac * pg.dx, dwy = pg.gfac * pg.dy;
+    __device__ __forceinline__ void add(T dwx, T dwy, T mj, T t11, T t12, T t22) {
         sx.madd(mj, dwx);
         sy.madd(mj, dwy);
         tx.madd(mj, fma(t11, dwx, t12 * dwy));
         ty.madd(mj, fma(t12, dwx, t22 * dwy));
     }
+};
+
+// Vector of two values of the pair arithmetic type (the per-pair kernel
+// gradients kept for the stress pass, common.cuh: kDwRows).
+template <class T>
+struct Vec2;
+template <>
+struct Vec2<double> {
+    using type = double2;
+    static __device__ __forceinline__ double2 make(double a, double b) { return make_double2(a, b); }
+};
+template <>
+struct Vec2<float> {
+    using type = float2;
+    static __device__ __forceinline__ float2 make(float a, float b) { return make_float2(a, b); }
 };
 
 struct KinArgs {
@@ -293,6 +315,7 @@ struct KinArgs {
     Scalars *sc;
     double *tau11, *tau12, *tau22, *div;
     TauRec rec;            // the stress pass's neighbour records (written here)
+    void *dw;              // grad W per pair row (Vec2<T>), kDwRows rows of stride pl.stride
     double *diag;
     NbrList nl;
     PairList pl;
@@ -372,6 +395,7 @@ struct StressArgs {
     Scalars *sc;
     const double *tau11, *tau12, *tau22, *div;
     TauRec rec;
+    const void *dw;
     NbrList nl;
     PairList pl;
     double *rates;

@@ -47,6 +47,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksKin) k_kinematic(KinArgs a) 
     const double inv_hi = 1.0 / hi;
     KinSums<T> ks;     // -div and the velocity gradient, negated
     const T hiT = Nb<T>::h(s, i), inv_hiT = (T)inv_hi;
+    typename Vec2<T>::type *dwr = reinterpret_cast<typename Vec2<T>::type *>(a.dw);
     int cnt = 0;       // entries in this thread's shared-memory list
     int npairs = 0;    // exact pairs found so far
     int done = 0;      // pairs already processed (and written to the pair list)
@@ -58,7 +59,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksKin) k_kinematic(KinArgs a) 
             const double2 q = s.xy[j], v = s.vxy[j];
             const KinNb<T> nb = Nb<T>::kin(s, j);
             const PairGeom<T> pg = pair_geom<T, false>(P, (T)(xi - q.x), (T)(yi - q.y), hiT, inv_hiT, nb.h);
-            ks.add(pg, (T)(vxi - v.x), (T)(vyi - v.y), nb.m, nb.mor);
+            const T dwx = pg.gfac * pg.dx, dwy = pg.gfac * pg.dy;
+            if (dwr && done + k < kDwRows) dwr[(size_t)(done + k) * a.pl.stride + i] = Vec2<T>::make(dwx, dwy);
+            ks.add(dwx, dwy, (T)(vxi - v.x), (T)(vyi - v.y), nb.m, nb.mor);
         }
         done += cnt;
         cnt = 0;
@@ -120,10 +123,20 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksStress) k_stress(StressArgs 
         const double2 q = s.xy[j];
         const StressNb<T> nb = Nb<T>::stress(s, a.rec, j);
         const PairGeom<T> pg = pair_geom<T, false>(P, (T)(xi - q.x), (T)(yi - q.y), hiT, inv_hiT, nb.h);
-        ss.add(pg, nb.m, nb.t11, nb.t12, nb.t22);
+        ss.add(pg.gfac * pg.dx, pg.gfac * pg.dy, nb.m, nb.t11, nb.t12, nb.t22);
     };
     int cnt = a.pl.count[i];
-    if (cnt <= kMaxPairs) {
+    if (a.dw && cnt <= kDwRows && !dead) {
+        // the kinematic pass kept these pairs' kernel gradients
+        const typename Vec2<T>::type *dwr = reinterpret_cast<const typename Vec2<T>::type *>(a.dw);
+#pragma unroll 4
+        for (int k = 0; k < cnt; ++k) {
+            const size_t r = (size_t)k * a.pl.stride + i;
+            const typename Vec2<T>::type g = dwr[r];
+            const StressNb<T> nb = Nb<T>::stress_rec(a.rec, a.pl.pj[r]);
+            ss.add(g.x, g.y, nb.m, nb.t11, nb.t12, nb.t22);
+        }
+    } else if (cnt <= kMaxPairs) {
         // the kinematic pass of this right-hand side found the pairs
 #pragma unroll 4
         for (int k = 0; k < cnt; ++k) accumulate(a.pl.pj[(size_t)k * a.pl.stride + i]);
@@ -236,6 +249,7 @@ void launch_kinematic(simp_ctx *c, const State &s, bool diag) {
     a.tau22 = c->tau22;
     a.div = c->div;
     a.rec = tau_rec(c);
+    a.dw = c->pair_dw;
     a.diag = diag ? c->diag : nullptr;
     a.nl = nbr_list(c);
     a.pl = pair_list(c);
@@ -273,6 +287,7 @@ void launch_stress(simp_ctx *c, const State &rhs, const State &base, EpiMode mod
     a.tau22 = c->tau22;
     a.div = c->div;
     a.rec = tau_rec(c);
+    a.dw = c->pair_dw;
     a.nl = nbr_list(c);
     a.pl = pair_list(c);
     a.rates = c->rates;

@@ -15,11 +15,8 @@
 
 namespace {
 
-// Device bytes one particle (and one wall slot) of a batch context takes:
-// the allocations of simp_gpu_create_batch per unit of maxn (maxnb), plus
-// room for its cell lists.
-constexpr double kBytesPerParticle = 1100.0 + 16.0;
-constexpr int kWallsPerParticleDiv = 4;   // wall capacity = particles / 4
+// Wall capacity of a batch = particles / 4; bytes per wall slot.
+constexpr int kWallsPerParticleDiv = 4;
 constexpr double kBytesPerWall = 48.0;
 constexpr int kSpotSlots = 64;            // FP64 replicas resident at once
 
@@ -181,13 +178,15 @@ int32_t simp_server_create(const simp_params *params, const simp_server_config *
     *out = s;
     s->prm = *params;
     s->cfg = *cfg;
-    const double per = kBytesPerParticle + kBytesPerWall / kWallsPerParticleDiv;
+    const double per = simp::bytes_per_particle(s->prm) + kBytesPerWall / kWallsPerParticleDiv;
     double budget = cfg->hbm_budget_bytes;
     if (cfg->spot_every > 0) {
+        simp_params p64 = s->prm;
+        p64.precision = SIMP_PREC_FP64;
         const double spot_n = 2.0 * cfg->max_request_particles;
         s->maxn_spot = (int)spot_n;
         s->maxnb_spot = std::max(1, s->maxn_spot / kWallsPerParticleDiv);
-        budget -= spot_n * per;
+        budget -= spot_n * (simp::bytes_per_particle(p64) + kBytesPerWall / kWallsPerParticleDiv);
     }
     const double cap = std::floor(budget / per);
     if (cap < cfg->max_request_particles)

@@ -214,9 +214,14 @@ __global__ void __launch_bounds__(kMaxTileThreads) k_kin_tiled(KinArgs a) {
     KinSums<T> ks;
     int npairs = 0;
     const T hiT = Nb<T>::h(s, i), inv_hiT = (T)inv_hi;
-    auto pair_terms = [&](double xj, double yj, T hj, double vxj, double vyj, T mj, T mrj) {
+    typename Vec2<T>::type *dwr = reinterpret_cast<typename Vec2<T>::type *>(a.dw);
+    // row: the pair's position in the particle's pair list (its kernel
+    // gradient is kept for the stress pass when row < kDwRows)
+    auto pair_terms = [&](int row, double xj, double yj, T hj, double vxj, double vyj, T mj, T mrj) {
         const PairGeom<T> pg = pair_geom<T, false>(P, (T)(xi - xj), (T)(yi - yj), hiT, inv_hiT, hj);
-        ks.add(pg, (T)(vxi - vxj), (T)(vyi - vyj), mj, mrj);
+        const T dwx = pg.gfac * pg.dx, dwy = pg.gfac * pg.dy;
+        if (dwr && row < kDwRows) dwr[(size_t)row * pl.stride + i] = Vec2<T>::make(dwx, dwy);
+        ks.add(dwx, dwy, (T)(vxi - vxj), (T)(vyi - vyj), mj, mrj);
     };
     if (dead) {
         // a basin flagged non-finite is carried without a search
@@ -252,9 +257,9 @@ __global__ void __launch_bounds__(kMaxTileThreads) k_kin_tiled(KinArgs a) {
                     tl.list[kept * blockDim.x + t] = (unsigned short)sl;
                 else if (npairs < kMaxPairs)
                     pl.pj[(size_t)npairs * pl.stride + i] = index_of(h, sl);
+                pair_terms(npairs, xj, yj, tl.hT[sl], tl.vx[sl], tl.vy[sl], tl.m[sl], tl.mor[sl]);
                 ++kept;
                 ++npairs;
-                pair_terms(xj, yj, tl.hT[sl], tl.vx[sl], tl.vy[sl], tl.m[sl], tl.mor[sl]);
             }
             cnt = final ? kept : 0;
         };
@@ -320,10 +325,10 @@ __global__ void __launch_bounds__(kMaxTileThreads) k_kin_tiled(KinArgs a) {
         // halo too large for shared memory: the same pairs from HBM
         auto on_pair = [&](int j) {
             if (npairs < kMaxPairs) pl.pj[(size_t)npairs * pl.stride + i] = j;
-            ++npairs;
             const double2 q = s.xy[j], v = s.vxy[j];
             const KinNb<T> nb = Nb<T>::kin(s, j);
-            pair_terms(q.x, q.y, nb.h, v.x, v.y, nb.m, nb.mor);
+            pair_terms(npairs, q.x, q.y, nb.h, v.x, v.y, nb.m, nb.mor);
+            ++npairs;
         };
         if (scan) {
             const float skinf = (float)skin, grow = 1.0f + pc.margin;
@@ -415,7 +420,8 @@ __global__ void __launch_bounds__(kMaxTileThreads) k_stress_tiled(StressArgs a) 
     StressSums<T> ss;
     const T hiT = Nb<T>::h(s, i), inv_hiT = (T)inv_hi;
     auto terms = [&](double xj, double yj, T hj, T mj, T t11, T t12, T t22) {
-        ss.add(pair_geom<T, false>(P, (T)(xi - xj), (T)(yi - yj), hiT, inv_hiT, hj), mj, t11, t12, t22);
+        const PairGeom<T> pg = pair_geom<T, false>(P, (T)(xi - xj), (T)(yi - yj), hiT, inv_hiT, hj);
+        ss.add(pg.gfac * pg.dx, pg.gfac * pg.dy, mj, t11, t12, t22);
     };
     auto global_terms = [&](int j) {
         const double2 q = s.xy[j];
@@ -430,6 +436,22 @@ __global__ void __launch_bounds__(kMaxTileThreads) k_stress_tiled(StressArgs a) 
     int cnt = live ? a.pl.count[i] : 0;
     if (dead || !live) {
         cnt = 0;
+    } else if (a.dw && cnt <= kDwRows) {
+        // the kinematic pass kept these pairs' kernel gradients
+        const typename Vec2<T>::type *dwr = reinterpret_cast<const typename Vec2<T>::type *>(a.dw);
+#pragma unroll 4
+        for (int k = 0; k < cnt; ++k) {
+            const size_t r = (size_t)k * a.pl.stride + i;
+            const typename Vec2<T>::type g = dwr[r];
+            const int j = a.pl.pj[r];
+            const int sl = fits ? slot_of(h, j) : -1;
+            if (sl >= 0) {
+                ss.add(g.x, g.y, tl.m[sl], tl.t11[sl], tl.t12[sl], tl.t22[sl]);
+            } else {
+                const StressNb<T> nb = Nb<T>::stress_rec(a.rec, j);
+                ss.add(g.x, g.y, nb.m, nb.t11, nb.t12, nb.t22);
+            }
+        }
     } else if (cnt <= kMaxPairs) {
 #pragma unroll 4
         for (int k = 0; k < cnt; ++k) any_terms(a.pl.pj[(size_t)k * a.pl.stride + i]);

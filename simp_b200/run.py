@@ -2,8 +2,9 @@
 
     python -m simp_b200.run --workload cfg2 --steps 100
 
-Workloads: cfg1 (2,500 particles), cfg2 (262,144), cfg2x4 (the cfg2 physics
-on a 1024 x 1024 lattice, 1,048,576 particles, FP64).  The role of the
+Workloads: cfg1 (2,500 particles), cfg2 (262,144), cfg3 (1,048,576, vortex,
+mixed), cfg2x4 (the cfg2 physics on a 1024 x 1024 lattice, 1,048,576
+particles, FP64).  The role of the
 reference's `make all` + simp.out run (Makefile:56-60), without CSV output.
 """
 from __future__ import annotations
@@ -23,6 +24,8 @@ def workload(name: str):
         return basins.cfg1()
     if name == "cfg2":
         return basins.cfg2()
+    if name == "cfg3":
+        return basins.cfg3()
     if name == "cfg2x4":
         return basins.make_basin(1024, 250.0, 2, name="cfg2x4_1048576", walls="+x", wind=(10.0, 0.0))
     raise SystemExit(f"unknown workload {name}")
@@ -35,12 +38,19 @@ def main():
     ap.add_argument("--chunk", type=int, default=0, help="steps per call (0: all in one call)")
     ap.add_argument("--precision", choices=("fp64", "mixed"), default=None,
                     help="override the workload's precision")
+    ap.add_argument("--passes", choices=("gather", "tiled"), default="gather",
+                    help="pair-pass implementation")
+    ap.add_argument("--moving", action="store_true",
+                    help="start from a smooth non-zero velocity field instead of rest")
     args = ap.parse_args()
     b = workload(args.workload)
+    if args.moving:
+        b.vx = basins.smooth_velocity(b.x, b.L, amp=0.3, seed=22)
     prm = b.params.copy()
     if args.precision:
         prm.precision = 1 if args.precision == "mixed" else 0
     sim = Simp.from_basin(b, prm)
+    sim.set_passes(1 if args.passes == "tiled" else 0)
     t0 = time.perf_counter()
     done = 0
     chunk = args.chunk or args.steps

@@ -79,7 +79,7 @@ def test_budget_limits_residency(gpu_lib):
     and all still complete, each with the same bits as alone."""
     reqs = _stream(count=5, seed=33, n_hi=8000, steps=(5, 15))
     big = max(r.basin.n for r in reqs)
-    budget = 1.2 * big * 1200.0
+    budget = 1.2 * big * 1800.0
     with serve.Server(reqs[0].basin.params, budget, max_instances=8, max_request_particles=big,
                       quantum_steps=4) as srv:
         ids = [srv.submit(r) for r in reqs]
