@@ -53,6 +53,8 @@ typedef struct simp_server_stats {
     int32_t reserved0;
     double makespan_s;              /* run start to the last completion         */
     double capacity_particles;      /* particle capacity the budget gave        */
+    double admit_s, step_s, retire_s; /* wall time in admissions, stepping and  */
+                                    /* retirements (results out, slots freed)   */
 } simp_server_stats;
 
 /* params: the served physics (fixed dt, fixed hsml); its precision is the

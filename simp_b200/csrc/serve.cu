@@ -258,6 +258,7 @@ int32_t simp_server_run(simp_server *s) {
         const size_t before = s->resident.size();
         int rc = admit(s, t);
         if (rc != SIMP_OK) return rc;
+        s->stats.admit_s += now() - t;
         for (size_t k = before; k < s->resident.size(); ++k) s->reqs[s->resident[k]].st.admitted_s = now();
         if (s->resident.empty()) {
             if (s->next >= s->order.size()) break;   // all done
@@ -268,6 +269,7 @@ int32_t simp_server_run(simp_server *s) {
         // requests with no steps left leave at once
         int64_t q = s->cfg.quantum_steps;
         for (int id : s->resident) q = std::min<int64_t>(q, s->reqs[id].remaining);
+        const double ts = now();
         if (q > 0) {
             rc = simp::step_enqueue(s->main, (int)q);
             if (rc != SIMP_OK) return ctx_error(s, s->main, rc);
@@ -284,6 +286,8 @@ int32_t simp_server_run(simp_server *s) {
             }
             s->stats.batch_steps += q;
         }
+        const double tr = now();
+        s->stats.step_s += tr - ts;
         std::vector<int> keep;
         for (int id : s->resident) {
             Request &r = s->reqs[id];
@@ -298,6 +302,7 @@ int32_t simp_server_run(simp_server *s) {
             }
         }
         s->resident.swap(keep);
+        s->stats.retire_s += now() - tr;
     }
     return SIMP_OK;
 }

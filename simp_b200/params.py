@@ -87,7 +87,8 @@ class ServerStats(ctypes.Structure):
                 ("particle_steps", ctypes.c_int64), ("batch_steps", ctypes.c_int64),
                 ("peak_resident_particles", ctypes.c_int64), ("peak_resident_requests", ctypes.c_int32),
                 ("reserved0", ctypes.c_int32), ("makespan_s", ctypes.c_double),
-                ("capacity_particles", ctypes.c_double)]
+                ("capacity_particles", ctypes.c_double), ("admit_s", ctypes.c_double),
+                ("step_s", ctypes.c_double), ("retire_s", ctypes.c_double)]
 
 
 def _real4(v: float) -> float:
