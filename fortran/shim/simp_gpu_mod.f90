@@ -30,6 +30,12 @@ module simp_gpu_mod
                           dt, max_hsml, skin
     end type simp_params
 
+    ! Mirror of struct simp_forcing (per-basin wind of a batch).
+    type, bind(C) :: simp_forcing
+        integer(c_int32_t) :: wind_kind, reserved0
+        real(c_double) :: wind_u, wind_v, vortex_x, vortex_y, vortex_umax, vortex_radius
+    end type simp_forcing
+
     interface
         subroutine simp_params_reference_default(p) bind(C, name="simp_params_reference_default")
             import :: simp_params
@@ -123,6 +129,54 @@ module simp_gpu_mod
             integer(c_int32_t), value :: nsteps
             real(c_double), intent(out) :: current_time, dt
             integer(c_int32_t) :: simp_gpu_step
+        end function
+
+        function simp_gpu_set_forcing(ctx, f) bind(C, name="simp_gpu_set_forcing")
+            import :: c_ptr, c_int32_t, simp_forcing
+            type(c_ptr), value :: ctx
+            type(simp_forcing), intent(in) :: f
+            integer(c_int32_t) :: simp_gpu_set_forcing
+        end function
+
+        ! Batches of basins advanced together by simp_gpu_step.
+        function simp_gpu_create_batch(p, maxn, maxnb, max_instances, ctx)  &
+                                       bind(C, name="simp_gpu_create_batch")
+            import :: simp_params, c_int32_t, c_ptr
+            type(simp_params), intent(in) :: p
+            integer(c_int32_t), value :: maxn, maxnb, max_instances
+            type(c_ptr), intent(out) :: ctx
+            integer(c_int32_t) :: simp_gpu_create_batch
+        end function
+
+        function simp_gpu_batch_add(ctx, f, ntotal, x, vx, mass, rho, hsml,    &
+                                    A, h, ntotalb, xb, massb, slot)            &
+                                    bind(C, name="simp_gpu_batch_add")
+            import :: c_ptr, c_int32_t, c_double, simp_forcing
+            type(c_ptr), value :: ctx
+            type(simp_forcing), intent(in) :: f
+            integer(c_int32_t), value :: ntotal, ntotalb
+            real(c_double), intent(in) :: x(*), vx(*), mass(*), rho(*),        &
+                                          hsml(*), A(*), h(*), xb(*), massb(*)
+            integer(c_int32_t), intent(out) :: slot
+            integer(c_int32_t) :: simp_gpu_batch_add
+        end function
+
+        function simp_gpu_batch_remove(ctx, slot) bind(C, name="simp_gpu_batch_remove")
+            import :: c_ptr, c_int32_t
+            type(c_ptr), value :: ctx
+            integer(c_int32_t), value :: slot
+            integer(c_int32_t) :: simp_gpu_batch_remove
+        end function
+
+        function simp_gpu_batch_get_state(ctx, slot, x, vx, mass, rho, hsml,   &
+                                          A, h, current_time)                  &
+                                          bind(C, name="simp_gpu_batch_get_state")
+            import :: c_ptr, c_int32_t, c_double
+            type(c_ptr), value :: ctx
+            integer(c_int32_t), value :: slot
+            real(c_double), intent(out) :: x(*), vx(*), mass(*), rho(*),       &
+                                           hsml(*), A(*), h(*), current_time
+            integer(c_int32_t) :: simp_gpu_batch_get_state
         end function
 
         function simp_gpu_last_error_c(ctx) bind(C, name="simp_gpu_last_error")

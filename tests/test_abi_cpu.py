@@ -72,6 +72,26 @@ def test_struct_layouts_match_c(tmp_path, cname, pyname, header):
         assert int(out[f]) == getattr(cls, f).offset, f
 
 
+def test_fortran_forcing_mirror_field_order():
+    from simp_b200.params import SimpForcing
+    src = open(os.path.join(ROOT, "fortran", "shim", "simp_gpu_mod.f90")).read()
+    body = src[src.index("type, bind(C) :: simp_forcing"):src.index("end type simp_forcing")]
+    names = []
+    for line in body.splitlines()[1:]:
+        if "::" in line:
+            names += [n.strip() for n in line.split("::", 1)[1].split(",") if n.strip()]
+    assert [n.lower() for n in names] == [f.lower() for f, _ in SimpForcing._fields_]
+
+
+def test_fortran_interfaces_name_exported_symbols(lib):
+    """Every bind(C, name=...) of the Fortran module is exported by the library."""
+    src = open(os.path.join(ROOT, "fortran", "shim", "simp_gpu_mod.f90")).read()
+    names = re.findall(r'bind\(C,\s*name="(simp_\w+)"\)', src)
+    assert len(names) >= 15
+    for n in names:
+        assert hasattr(lib, n), n
+
+
 def test_fortran_mirror_field_order():
     """The bind(C) type in the Fortran shim lists the members in C order."""
     src = open(os.path.join(ROOT, "fortran", "shim", "simp_gpu_mod.f90")).read()
