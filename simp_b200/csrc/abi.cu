@@ -43,12 +43,13 @@ __global__ void k_deinterleave(int n, const double *__restrict__ in, double *__r
 
 // New particles [off, off + n): ids, instance, sort positions, m / rho.
 __global__ void k_init_new(int n, int off, int id_base, int slot, int *id, int *pinst, State s, double *xr,
-                           double *yr) {
+                           double *yr, int *nbr_count) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const int i = off + k;
     id[i] = id_base + k;
     pinst[i] = slot;
+    nbr_count[i] = -1;   // its Verlet list is built by the next kinematic pass
     xr[i] = s.x[i];
     yr[i] = s.y[i];
     s.mor[i] = s.m[i] / s.rho[i];
@@ -230,10 +231,16 @@ int layout(simp_ctx *c) {
     std::vector<Inst> cur(c->max_inst);
     SIMP_CUDA(c, cudaMemcpyAsync(cur.data(), c->inst_dev, sizeof(Inst) * c->max_inst, cudaMemcpyDeviceToHost, s));
     SIMP_CUDA(c, cudaStreamSynchronize(s));
+    // cell-key bases in admission order, so that a new basin's keys come
+    // after every resident one (it is appended in memory, nothing moves)
+    std::vector<int> by_order;
+    for (int q = 0; q < c->max_inst; ++q)
+        if (c->insts[q].active) by_order.push_back(q);
+    std::sort(by_order.begin(), by_order.end(),
+              [&](int a, int b) { return c->insts[a].order < c->insts[b].order; });
     int base = 0, top = 0;
-    for (int q = 0; q < c->max_inst; ++q) {
+    for (int q : by_order) {
         InstHost &h = c->insts[q];
-        if (!h.active) continue;
         if (h.I.base >= 0) {   // already on the device: keep its evolving fields
             h.I.t = cur[q].t;
             h.I.dmax2_bits = cur[q].dmax2_bits;
@@ -244,7 +251,7 @@ int layout(simp_ctx *c) {
         }
         h.I.base = base;
         base += h.I.ncx * h.I.ncy;
-        top = q + 1;
+        top = std::max(top, q + 1);
     }
     c->total_cells = base;
     c->ninst = std::max(top, 1);
@@ -267,9 +274,8 @@ int layout(simp_ctx *c) {
     }
     // cell rows of all instances, for the chunks of the tiled passes
     std::vector<int2> rows;
-    for (int q = 0; q < c->max_inst; ++q)
-        if (c->insts[q].active)
-            for (int r = 0; r < c->insts[q].I.ncy; ++r) rows.push_back(make_int2(q, r));
+    for (int q : by_order)
+        for (int r = 0; r < c->insts[q].I.ncy; ++r) rows.push_back(make_int2(q, r));
     c->total_rows = (int)rows.size();
     const size_t need_chunks = (size_t)c->maxn / kMinTileThreads + rows.size() + 2;
     if (rows.size() + 2 > c->row_cap || need_chunks > c->chunk_cap) {
@@ -386,6 +392,7 @@ int add_instance(simp_ctx *c, int slot, const simp_forcing &f, int n, const doub
     ih.n = n;
     ih.nb = nb;
     ih.id_base = c->id_stride * slot;
+    ih.order = c->next_order++;
     ih.xb.assign(xb, xb + 2 * (size_t)nb);
     ih.massb.assign(massb, massb + nb);
     size_inst_grid(c, ih, xmin, xmax, ymin, ymax, hmax);
@@ -419,26 +426,38 @@ int add_instance(simp_ctx *c, int slot, const simp_forcing &f, int n, const doub
     SIMP_CUDA(c, cudaMemcpyAsync(c->s0.hs + off, hsml, sizeof(double) * N, cudaMemcpyHostToDevice, s));
     SIMP_CUDA(c, cudaMemcpyAsync(c->s0.A + off, A, sizeof(double) * N, cudaMemcpyHostToDevice, s));
     SIMP_CUDA(c, cudaMemcpyAsync(c->s0.h + off, h, sizeof(double) * N, cudaMemcpyHostToDevice, s));
-    k_init_new<<<nblk(n, kB), kB, 0, s>>>(n, off, ih.id_base, slot, c->id, c->pinst, c->s0, c->xr, c->yr);
+    k_init_new<<<nblk(n, kB), kB, 0, s>>>(n, off, ih.id_base, slot, c->id, c->pinst, c->s0, c->xr, c->yr,
+                                          c->nbr_count);
     k_grow_xabs<<<1, 1, 0, s>>>(c->sc, pxa);
     c->launches += 4;
     SIMP_CUDA(c, cudaGetLastError());
     c->n += n;
+    // the new basin's keys come last: only its own range is sorted, and the
+    // resident basins keep their places and their Verlet lists
     TRY(layout(c));
-    TRY(rebuild(c, mask_of(slot), true, true));
+    TRY(rebuild(c, mask_of(slot), off, false));
     SIMP_CUDA(c, cudaStreamSynchronize(s));
     return SIMP_OK;
+}
+
+// First position of an instance in memory (instances lie in admission order).
+int inst_offset(const simp_ctx *c, int slot) {
+    int off = 0;
+    for (const InstHost &h : c->insts)
+        if (h.active && h.order < c->insts[slot].order) off += h.n;
+    return off;
 }
 
 int remove_instance(simp_ctx *c, int slot) {
     InstHost &h = c->insts[slot];
     if (!h.active) return simp_fail(c, SIMP_ERR_BADARG, "slot is free");
+    const int from = inst_offset(c, slot);   // the basins after it shift down
     cudaStream_t s = c->stream;
     k_mark_removed<<<nblk(c->n, kB), kB, 0, s>>>(c->n, slot, c->pinst);
     c->launches += 1;
     h = InstHost{};
     TRY(layout(c));
-    TRY(rebuild(c, DueMask{}, true, false));
+    TRY(rebuild(c, DueMask{}, from, false));
     SIMP_CUDA(c, cudaStreamSynchronize(s));
     return SIMP_OK;
 }
@@ -571,7 +590,7 @@ int maybe_regrid(simp_ctx *c, bool *done) {
     }
     size_inst_grid(c, h, xmin, xmax, ymin, ymax, I.hmax);
     TRY(layout(c));
-    TRY(rebuild(c, mask_of(0), false, false));
+    TRY(rebuild(c, mask_of(0), c->n, false));
     h.steps_since_sort = 0;
     return SIMP_OK;
 }
@@ -742,7 +761,7 @@ int step_enqueue(simp_ctx *c, int nsteps) {
             if (c->graph_profiled) SIMP_CUDA(c, cudaEventRecord(c->sort_ev[0], s));
             TRY(maybe_regrid(c, &regridded));   // hsml grew past the grid (sle = 2)
             if (regridded) TRY(ensure_graph(c, c->keep_diag));
-            else TRY(rebuild(c, due, false, false));
+            else TRY(rebuild(c, due, c->n, false));
             if (c->graph_profiled) {
                 SIMP_CUDA(c, cudaEventRecord(c->sort_ev[1], s));
                 SIMP_CUDA(c, cudaEventSynchronize(c->sort_ev[1]));

@@ -195,21 +195,21 @@ __device__ __forceinline__ bool is_due(const DueMask &m, int q) {
     return q >= 0 && ((m.w[q >> 6] >> (q & 63)) & 1ull);
 }
 
-// Positions of the new order whose particle may differ from the old one: all
-// of them after an admission or a removal (instance ranges shift), else only
-// those of the due instances (every instance keeps its range of positions,
-// and the others keep their order).
-__device__ __forceinline__ bool moves(int all, const DueMask &due, const int *pinst, int k) {
-    return all || is_due(due, pinst[k]);
+// Positions of the new order whose particle may differ from the old one:
+// every position from `from` on (an admission appends a basin there; a
+// removal shifts the basins after it down), and those of the due basins
+// (each basin keeps its range of positions; the others keep their order).
+__device__ __forceinline__ bool moves(int from, const DueMask &due, const int *pinst, int k) {
+    return k >= from || is_due(due, pinst[k]);
 }
 
 // New order into scratch; inv[old] = new for every moved particle.
-__global__ void k_gather(int kept, int all, DueMask due, const int *__restrict__ perm, Gather gd,
+__global__ void k_gather(int kept, int from, DueMask due, const int *__restrict__ perm, Gather gd,
                          const int *__restrict__ key, int *__restrict__ cell_out, const int *__restrict__ id_in,
                          int *__restrict__ id_out, const int *__restrict__ pinst_in, int *__restrict__ pinst_out,
                          int *__restrict__ inv) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= kept || !moves(all, due, pinst_in, k)) return;
+    if (k >= kept || !moves(from, due, pinst_in, k)) return;
     const int o = perm[k];
 #pragma unroll
     for (int a = 0; a < kGathered; ++a) gd.dst[a][k] = gd.src[a][o];
@@ -224,17 +224,19 @@ __global__ void k_gather(int kept, int all, DueMask due, const int *__restrict__
 // index order exactly as a fresh scan of the cell stencil would.  An entry
 // whose new index cannot be confirmed (perm[inv[v]] != v) turns the row into
 // an overflowed one, which the kinematic pass answers by a stencil scan.
-__global__ void k_remap_lists(int kept, int all, DueMask due, const int *__restrict__ pinst,
+__global__ void k_remap_lists(int kept, int from, DueMask due, const int *__restrict__ pinst,
                               const int *__restrict__ perm, const int *__restrict__ inv, int n_old,
                               NbrList nl, int *__restrict__ nbr_out, int *__restrict__ cnt_out,
                               double *__restrict__ xl_out, double *__restrict__ yl_out) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= kept || !moves(all, due, pinst, k)) return;
+    if (k >= kept || !moves(from, due, pinst, k)) return;
     const int o = perm[k];
     int cnt = nl.count[o];
     xl_out[k] = nl.xl[o];
     yl_out[k] = nl.yl[o];
-    if (cnt >= 0 && cnt <= kMaxNbr) {
+    if (cnt < 0) {
+        // (a particle whose list is still to be built keeps that mark)
+    } else if (cnt <= kMaxNbr) {
         int row[kMaxNbr];
         for (int e = 0; e < cnt; ++e) {
             const int v = nl.nbr[(size_t)e * nl.stride + o];
@@ -256,25 +258,24 @@ __global__ void k_remap_lists(int kept, int all, DueMask due, const int *__restr
     cnt_out[k] = cnt;
 }
 
-__global__ void k_put_back_lists(int kept, int all, DueMask due, const int *__restrict__ pinst, NbrList nl,
+__global__ void k_put_back_lists(int kept, int from, DueMask due, const int *__restrict__ pinst, NbrList nl,
                                  const int *__restrict__ nbr_in, const int *__restrict__ cnt_in,
                                  const double *__restrict__ xl_in, const double *__restrict__ yl_in) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= kept || !moves(all, due, pinst, k)) return;
+    if (k >= kept || !moves(from, due, pinst, k)) return;
     const int cnt = cnt_in[k];
     nl.count[k] = cnt;
     nl.xl[k] = xl_in[k];
     nl.yl[k] = yl_in[k];
-    if (cnt <= kMaxNbr)
-        for (int e = 0; e < cnt; ++e) nl.nbr[(size_t)e * nl.stride + k] = nbr_in[(size_t)e * nl.stride + k];
+    for (int e = 0; e < cnt && cnt <= kMaxNbr; ++e) nl.nbr[(size_t)e * nl.stride + k] = nbr_in[(size_t)e * nl.stride + k];
 }
 
 // Scratch back into the state arrays (pointers stay fixed so the captured
 // step graph remains valid), with the FP32 copies of the moved particles.
-__global__ void k_put_back(int kept, int all, DueMask due, Gather gd, State s, const int *__restrict__ id_new,
+__global__ void k_put_back(int kept, int from, DueMask due, Gather gd, State s, const int *__restrict__ id_new,
                            int *__restrict__ id, const int *__restrict__ pinst_new, int *__restrict__ pinst) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= kept || !moves(all, due, pinst, k)) return;
+    if (k >= kept || !moves(from, due, pinst, k)) return;
 #pragma unroll
     for (int a = 0; a < kGathered; ++a) const_cast<double *>(gd.src[a])[k] = gd.dst[a][k];
     id[k] = id_new[k];
@@ -313,14 +314,14 @@ void launch_scan_i32(const int *in, int *out, int n, void *tmp, cudaStream_t s) 
 
 // Sorts the particles into cell order (instance-major keys, within a cell by
 // global id).  Instances in `due` re-bin at their current positions; the
-// others keep their sort positions, so their order does not change.  With
-// `full` (after an admission or a removal) every position is rewritten;
-// otherwise only the due instances' ranges move.  Particles of removed
-// instances (instance -1) end up after all others and are dropped: c->n
-// shrinks to the kept count.  The Verlet lists follow the particles unless
-// `new_lists` (or no list was built yet), in which case the next kinematic
-// pass rebuilds them.
-int rebuild(simp_ctx *c, const DueMask &due, bool full, bool new_lists) {
+// others keep their sort positions, so their order does not change.
+// Positions from `from` on are rewritten (after an admission or a removal:
+// the first position whose basin changed), before it only the due
+// instances' ranges move.  Particles of removed instances (instance -1) end
+// up after all others and are dropped: c->n shrinks to the kept count.  The
+// Verlet lists follow the particles unless `new_lists` (or no list was built
+// yet), in which case the next kinematic pass rebuilds them all.
+int rebuild(simp_ctx *c, const DueMask &due, int from, bool new_lists) {
     const int n = c->n;
     cudaStream_t s = c->stream;
     const int B = 256;
@@ -335,7 +336,6 @@ int rebuild(simp_ctx *c, const DueMask &due, bool full, bool new_lists) {
     for (const InstHost &h : c->insts)
         if (h.active) kept += h.n;
     const bool keep_lists = c->lists_valid && !new_lists;
-    const int all = full ? 1 : 0;
     if (n > 0) {
         k_refresh_sortpos<<<nblk(n, B), B, 0, s>>>(n, c->pinst, due, c->inst_dev, c->s0.x, c->s0.y, c->xr, c->yr);
         k_reset_inst_disp<<<nblk(c->ninst, 128), 128, 0, s>>>(c->inst_dev, c->ninst, due);
@@ -355,19 +355,19 @@ int rebuild(simp_ctx *c, const DueMask &due, bool full, bool new_lists) {
         }
         c->launches += 7 + kScanKernels;
         if (kept > 0) {
-            k_gather<<<nblk(kept, B), B, 0, s>>>(kept, all, due, c->perm, gd, key, c->cell, c->id, id_new,
+            k_gather<<<nblk(kept, B), B, 0, s>>>(kept, from, due, c->perm, gd, key, c->cell, c->id, id_new,
                                                  c->pinst, pinst_new, inv);
             c->launches += 1;
             if (keep_lists) {
                 NbrList nl{c->nbr, c->nbr_count, c->xl, c->yl, c->maxn};
                 double *xl_new = c->tmp + 12 * MX, *yl_new = c->tmp + 13 * MX;
-                k_remap_lists<<<nblk(kept, 128), 128, 0, s>>>(kept, all, due, c->pinst, c->perm, inv, n, nl,
+                k_remap_lists<<<nblk(kept, 128), 128, 0, s>>>(kept, from, due, c->pinst, c->perm, inv, n, nl,
                                                               c->nbr_tmp, cnt_new, xl_new, yl_new);
-                k_put_back_lists<<<nblk(kept, B), B, 0, s>>>(kept, all, due, c->pinst, nl, c->nbr_tmp, cnt_new,
+                k_put_back_lists<<<nblk(kept, B), B, 0, s>>>(kept, from, due, c->pinst, nl, c->nbr_tmp, cnt_new,
                                                              xl_new, yl_new);
                 c->launches += 2;
             }
-            k_put_back<<<nblk(kept, B), B, 0, s>>>(kept, all, due, gd, c->s0, id_new, c->id, pinst_new, c->pinst);
+            k_put_back<<<nblk(kept, B), B, 0, s>>>(kept, from, due, gd, c->s0, id_new, c->id, pinst_new, c->pinst);
             c->launches += 1;
         }
     } else {

@@ -16,6 +16,7 @@ struct InstHost {
     int n = 0, nb = 0;             // particles and wall particles
     int id_base = 0;               // global particle id = id_base + local index
     double grid_hmax = 0.0;        // max(hsml) its grid was sized for
+    long long order = 0;           // admission sequence: instances lie in this order in memory
     long long steps_since_sort = 0;
     long long steps_done = 0;
     std::vector<double> xb, massb; // its walls (re-binned when the layout changes)
@@ -38,6 +39,7 @@ struct simp_ctx {
     simp::Inst *inst_dev = nullptr;
     int ninst = 0;                 // table entries in use (highest active slot + 1)
     int id_stride = 0;             // 0 for a single basin, 1 << 21 for batches
+    long long next_order = 0;      // admission counter
     int total_cells = 0;           // cell keys over all instances
 
     // particle state sets (device, cell order)
@@ -129,7 +131,7 @@ constexpr int kMaxSlots = 1024;
 struct DueMask {
     unsigned long long w[kMaxSlots / 64];
 };
-int rebuild(simp_ctx *c, const DueMask &due, bool full, bool new_lists);   // sort into cell order
+int rebuild(simp_ctx *c, const DueMask &due, int from, bool new_lists);   // sort into cell order
 void launch_scan_i32(const int *in, int *out, int n, void *tmp, cudaStream_t s);
 constexpr int kScanKernels = 4;         // kernels per launch_scan_i32
 size_t scan_tmp_bytes(int n);

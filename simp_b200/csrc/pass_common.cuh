@@ -196,7 +196,7 @@ __device__ __forceinline__ void for_each_current_pair(const State &s, const NbrL
     const double own = sqrt(dxl * dxl + dyl * dyl);
     const double all = sqrt(bitsd(sc->dlist2_bits));
     const bool valid = (own + all) * (1.0 + 1e-9) < sc->skin;
-    if (cnt <= kMaxNbr && valid) {
+    if (cnt >= 0 && cnt <= kMaxNbr && valid) {
         for (int k = 0; k < cnt; ++k) {
             const int j = nl.nbr[(size_t)k * nl.stride + i];
             if (is_pair(s, p, j)) on_pair(j);

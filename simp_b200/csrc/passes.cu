@@ -72,13 +72,15 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksKin) k_kinematic(KinArgs a) 
         if (++cnt == kGatherSlots) flush();
     };
     if (a.sc->list_scan && i == 0) atomicExch(&a.sc->dlist2_bits, 0ull);
+    // (a particle of a newly admitted basin builds its list on its own)
+    const bool build = a.sc->list_scan || a.nl.count[i] < 0;
     if (dead) {
-        if (a.sc->list_scan) {
+        if (build) {
             a.nl.count[i] = 0;
             a.nl.xl[i] = xi;
             a.nl.yl[i] = yi;
         }
-    } else if (a.sc->list_scan) {
+    } else if (build) {
         // rebuild the Verlet list from the cell stencil: members are the
         // candidates not certainly beyond mhsml + skin (FP32, with margin)
         const double skin = a.sc->skin;

@@ -175,16 +175,19 @@ __global__ void __launch_bounds__(kMaxTileThreads) k_kin_tiled(KinArgs a) {
     if ((int)blockIdx.x >= *a.nchunks) return;
     const Chunk ch = a.chunks[blockIdx.x];
     const Inst &I = a.inst[ch.q];
-    const bool scan = a.sc->list_scan != 0;   // this pass rebuilds the Verlet lists
-    const double skin = a.sc->skin;
-    if (threadIdx.x == 0)
-        make_halo(ch, I, a.cell_start, a.cell, a.cap, scan ? I.hmax + skin : 0.0, h, fits);
-    __syncthreads();
-    const State &s = a.s;
-    const Phys &P = a.P;
     const int t = threadIdx.x;
     const int i = ch.p0 + t;
     const bool live = i < ch.p1;
+    // this pass rebuilds every Verlet list, or the particle's own (a newly
+    // admitted basin); the halo then reaches mhsml + skin
+    const bool scan = a.sc->list_scan != 0 || (live && a.nl.count[i] < 0);
+    const bool any_scan = __syncthreads_or(scan) != 0;
+    const double skin = a.sc->skin;
+    if (threadIdx.x == 0)
+        make_halo(ch, I, a.cell_start, a.cell, a.cap, any_scan ? I.hmax + skin : 0.0, h, fits);
+    __syncthreads();
+    const State &s = a.s;
+    const Phys &P = a.P;
     const bool dead = (I.flags & FLAG_NONFINITE) != 0;
     const KinTile<T> tl = kin_tile<T>(smem, a.cap);
     if (fits) {
@@ -204,7 +207,7 @@ __global__ void __launch_bounds__(kMaxTileThreads) k_kin_tiled(KinArgs a) {
     }
     __syncthreads();
     if (!live) return;
-    if (scan && i == 0) atomicExch(&a.sc->dlist2_bits, 0ull);
+    if (a.sc->list_scan && i == 0) atomicExch(&a.sc->dlist2_bits, 0ull);
     const PairCtx pc = pair_ctx(s, a.sc, I, a.cell_start, i);
     const double xi = pc.xi, yi = pc.yi, hi = pc.hi;
     const double vxi = s.vx[i], vyi = s.vy[i];
