@@ -52,11 +52,20 @@ enum {
     SIMP_ERR_STATE = 9      /* entry point called before simp_gpu_set_state    */
 };
 
-/* Smoothing kernel selector: the reference's skf codes (globals.f90:136-147). */
+/* Smoothing kernel selector: the reference's skf codes (globals.f90:136-147,
+ * kernel.f90:20-45, boundary_kernel.f90:20-45); scale_h as in
+ * initialize.f90:208-217. */
 enum {
-    SIMP_SKF_WENDLAND_C6 = 6, /* kernel.f90:471-520, boundary_kernel.f90:438-504 */
+    SIMP_SKF_QUADRATIC = 1,   /* kernel.f90:241-290, scale_h 2                       */
+    SIMP_SKF_GAUSSIAN = 2,    /* kernel.f90:108-157, scale_h 3                       */
+    SIMP_SKF_QUINTIC = 3,     /* kernel.f90:165-233, scale_h 3                       */
+    SIMP_SKF_WENDLAND_C2 = 4, /* kernel.f90:359-408, scale_h 1                       */
+    SIMP_SKF_WENDLAND_C4 = 5, /* kernel.f90:415-464, scale_h 1                       */
+    SIMP_SKF_WENDLAND_C6 = 6, /* kernel.f90:471-520, boundary_kernel.f90:438-504    */
+    SIMP_SKF_MARQUIS = 7,     /* kernel.f90:527-576, scale_h 3; walls: Gaussian      */
+    SIMP_SKF_MARQUIS2 = 8,    /* kernel.f90:583-633, scale_h 3; walls: Gaussian      */
     SIMP_SKF_CUBIC = 9        /* kernel.f90:297-352 (commented out in the
-                                 reference, restored here with scale_h = 2)     */
+                                 reference, restored here with scale_h = 2)          */
 };
 
 enum { SIMP_PREC_FP64 = 0, SIMP_PREC_MIXED = 1 };

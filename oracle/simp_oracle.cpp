@@ -111,42 +111,122 @@ void reduce_pairs(int npairs, double *dst, size_t len, int chunk, Body body) {
 }
 
 // ---------------------------------------------------------------------------
+// scale_h of kernel skf, initialize.f90:208-217 (9: the restored cubic, 2).
+int scale_h_of(int skf) {
+    if (skf == 4 || skf == 5 || skf == 6) return 1;
+    if (skf == 1 || skf == 9) return 2;
+    return 3;
+}
+
+// Fortran's x ** n for a small integer n, by multiplication.
+double ipow(double x, int n) {
+    double r = 1.0;
+    for (int k = 0; k < n; ++k) r *= x;
+    return r;
+}
+
 // Pair kernel, kernel.f90:5-45 dispatch.
 //   in : r, hij (hsml_ij), dx(2)  out: w, dw(2), k0 (kernel_zero value)
-// Wendland C6: kernel.f90:498-508.
-// Cubic spline: kernel.f90:324-340 (commented out in the reference), restored
-// with factor = 15/(7 pi) (scale_h/hsml_ij)^2 so that it is normalised like
-// the other kernels (kernel.f90:500); scale_h = 2.
+// Each kernel in the reference's own arithmetic; default-real literals keep
+// their single-precision values (real4).  Cubic spline: kernel.f90:324-340
+// (commented out in the reference), restored with factor = 15/(7 pi)
+// (scale_h/hsml_ij)^2 so that it is normalised like the other kernels.
 void pair_kernel(const Orc &o, double r, double hij, const double dx[2],
                  double *w, double dw[2], double *k0) {
     const double sh = (double)o.scale_h;
     const double q = r / hij * sh;
-    if (o.P.skf == SIMP_SKF_WENDLAND_C6) {
-        const double factor = 78.0 / (7.0 * PI) * p2(sh / hij);
-        *k0 = factor;
-        const double om = 1.0 - q;
-        *w = factor * p8(om) * (32.0 * p3(q) + 25.0 * p2(q) + 8.0 * q + 1.0);
-        const double g = factor * (-22.0 * q * p7(om) * (16.0 * p2(q) + 7.0 * q + 1.0));
-        for (int d = 0; d < 2; ++d) dw[d] = g / hij * (dx[d] / r) * sh;
-    } else {  // SIMP_SKF_CUBIC
-        const double factor = 15.0 / (7.0 * PI) * p2(sh / hij);
-        const double c23 = real4(2.0f / 3.0f), c16 = real4(1.0f / 6.0f);
-        *k0 = factor * c23;
-        double wt = 0.0, g = 0.0;
-        if (q >= 0.0 && q <= 1.0) {
-            wt = factor * (c23 - p2(q) + 0.5 * p3(q));
-            g = factor * (-2.0 * q + 1.5 * p2(q));
+    double wt = 0.0, g = 0.0;
+    switch (o.P.skf) {
+        case 1: {   // Quadratic, kernel.f90:269-276
+            const double factor = 2.0 / PI * p2(sh / hij);
+            *k0 = factor * (3.0 / 4.0);
+            wt = factor * (3.0 / 16.0 * p2(q) - 3.0 / 4.0 * q + 3.0 / 4.0);
+            g = factor * (3.0 / 8.0 * q - 3.0 / 4.0);
+            break;
         }
-        if (q > 1.0 && q <= 2.0) {
-            wt = factor * (c16 * p3(2.0 - q));
-            g = factor * (-0.5 * p2(2.0 - q));
+        case 2: {   // Gaussian, kernel.f90:136-144
+            const double factor = 1.0 / PI * p2(sh / hij);
+            *k0 = factor;
+            wt = factor * std::exp(-p2(q));
+            g = factor * (-2 * q * std::exp(-p2(q)));
+            break;
         }
-        *w = wt;
-        for (int d = 0; d < 2; ++d) dw[d] = g / hij * (dx[d] / r) * sh;
+        case 3: {   // quintic spline, kernel.f90:193-219
+            const double factor = 7.0 / (478.0 * PI) * p2(sh / hij);
+            *k0 = factor * (243 - 6 * 32 + 15);
+            if (q >= 0.0 && q <= 1.0) {
+                wt = factor * (ipow(3 - q, 5) - 6 * ipow(2 - q, 5) + 15 * ipow(1 - q, 5));
+                g = factor * (-5 * ipow(3 - q, 4) + 30 * ipow(2 - q, 4) - 75 * ipow(1 - q, 4));
+            }
+            if (q > 1.0 && q <= 2.0) {
+                wt = factor * (ipow(3 - q, 5) - 6 * ipow(2 - q, 5));
+                g = factor * (-5 * ipow(3 - q, 4) + 30 * ipow(2 - q, 4));
+            }
+            if (q > 2.0 && q <= 3.0) {
+                wt = factor * ipow(3 - q, 5);
+                g = factor * (-5 * ipow(3 - q, 4));
+            }
+            break;
+        }
+        case 4: {   // Wendland C2, kernel.f90:387-393
+            const double factor = 3.0 / (2.0 * PI) * p2(sh / hij);
+            *k0 = factor;
+            wt = factor * (ipow(1.0 - q, 4) * (1 + 4 * q));
+            g = factor * (20.0 * (ipow(q, 4) - 3 * p3(q) + 3 * p2(q) - q));
+            break;
+        }
+        case 5: {   // Wendland C4, kernel.f90:443-450
+            const double factor = 3.0 / PI * p2(sh / hij);
+            *k0 = factor * 3;
+            wt = factor * (ipow(1 - q, 6) * (35 * p2(q) + 18 * q + 3));
+            g = factor * (-56 * q * (5 * q + 1) * ipow(1 - q, 5));
+            break;
+        }
+        case 6: {   // Wendland C6, kernel.f90:498-508
+            const double factor = 78.0 / (7.0 * PI) * p2(sh / hij);
+            *k0 = factor;
+            const double om = 1.0 - q;
+            wt = factor * p8(om) * (32.0 * p3(q) + 25.0 * p2(q) + 8.0 * q + 1.0);
+            g = factor * (-22.0 * q * p7(om) * (16.0 * p2(q) + 7.0 * q + 1.0));
+            break;
+        }
+        case 7: {   // Marquis, kernel.f90:555-563
+            const double factor = 1.0 / PI * p2(sh / hij);
+            *k0 = factor * (0.5 - 0.5 * std::tanh(0.0));
+            wt = factor * (0.5 - 0.5 * std::tanh(300 * (q - 1)));
+            g = factor * (-150 * std::pow(std::cosh(300 * (-1 + q)), -2));
+            break;
+        }
+        case 8: {   // Marquis2, kernel.f90:612-620 (log(2.) of a default real)
+            const double C1 = 10.0, C2 = 50.0;
+            const double l2 = (double)std::log(2.0f);
+            const double factor = 1.0 / (real4(34.1558f) * PI * p2(hij));
+            *k0 = factor * C2 * (std::log(std::cosh(C1)) / C1 + 1 + l2 / C1);
+            wt = factor * C2 * (std::log(std::cosh(C1 * (1 - q))) / C1 - q + 1 + l2 / C1);
+            g = factor * (-C2 * std::tanh(C1 * (1 - q)) - 1);
+            break;
+        }
+        default: {  // 9, cubic spline
+            const double factor = 15.0 / (7.0 * PI) * p2(sh / hij);
+            const double c23 = real4(2.0f / 3.0f), c16 = real4(1.0f / 6.0f);
+            *k0 = factor * c23;
+            if (q >= 0.0 && q <= 1.0) {
+                wt = factor * (c23 - p2(q) + 0.5 * p3(q));
+                g = factor * (-2.0 * q + 1.5 * p2(q));
+            }
+            if (q > 1.0 && q <= 2.0) {
+                wt = factor * (c16 * p3(2.0 - q));
+                g = factor * (-0.5 * p2(2.0 - q));
+            }
+            break;
+        }
     }
+    *w = wt;
+    for (int d = 0; d < 2; ++d) dw[d] = g / hij * (dx[d] / r) * sh;
 }
 
-// Boundary kernel value bw, boundary_kernel.f90:20-45 dispatch.
+// Boundary kernel value bw, boundary_kernel.f90:20-45 dispatch (the Marquis
+// kernels use b_Gaussian there).
 // Wendland C6: :489-494, with factor from hsml_ij(int_id) (the pair array of
 // the particle NNPS indexed by the boundary-pair index, as the reference does).
 // Cubic: in the style of b_Quadratic (:106-112), support b_length, scale_h = 2.
@@ -154,18 +234,38 @@ double boundary_w(const Orc &o, double br, int int_id) {
     const double sh = (double)o.scale_h;
     const double bl = o.P.b_length;
     const double q = br / bl * sh;
-    if (o.P.skf == SIMP_SKF_WENDLAND_C6) {
-        const double hij = (int_id - 1 < (int)o.hsml_ij.size()) ? o.hsml_ij[int_id - 1] : 0.0;
-        const double factor = 78.0 / (7.0 * PI) * p2(sh / hij);
-        const double om = 1.0 - q;
-        return factor * p8(om) * (32.0 * p3(q) + 25.0 * p2(q) + 8.0 * q + 1.0);
+    switch (o.P.skf) {
+        case 1:     // b_Quadratic, :106-108
+            return 2.0 / PI * p2(sh / bl) * (3.0 / 16.0 * p2(q) - 3.0 / 4.0 * q + 3.0 / 4.0);
+        case 2: case 7: case 8:   // b_Gaussian, :177-179
+            return 1.0 / PI * p2(sh / bl) * std::exp(-p2(q));
+        case 3: {   // b_quintic_spline, :250-269
+            const double factor = 15.0 / (478.0 * PI) * p2(sh / bl);
+            double bw = 0.0;
+            if (q >= 0.0 && q <= 1.0) bw = factor * (ipow(3 - q, 5) - 6 * ipow(2 - q, 5) + 15 * ipow(1 - q, 5));
+            if (q > 1.0 && q <= 2.0) bw = factor * (ipow(3 - q, 5) - 6 * ipow(2 - q, 5));
+            if (q > 2.0 && q <= 3.0) bw = factor * ipow(3 - q, 5);
+            return bw;
+        }
+        case 4:     // b_Wendland_C2, :342-344
+            return 3.0 / (2.0 * PI) * p2(sh / bl) * (ipow(1.0 - q, 4) * (1 + 4 * q));
+        case 5:     // b_Wendland_C4, :416-418
+            return 3.0 / PI * p2(sh / bl) * (ipow(1 - q, 6) * (35 * p2(q) + 18 * q + 3));
+        case 6: {
+            const double hij = (int_id - 1 < (int)o.hsml_ij.size()) ? o.hsml_ij[int_id - 1] : 0.0;
+            const double factor = 78.0 / (7.0 * PI) * p2(sh / hij);
+            const double om = 1.0 - q;
+            return factor * p8(om) * (32.0 * p3(q) + 25.0 * p2(q) + 8.0 * q + 1.0);
+        }
+        default: {
+            const double factor = 15.0 / (7.0 * PI) * p2(sh / bl);
+            const double c23 = real4(2.0f / 3.0f), c16 = real4(1.0f / 6.0f);
+            double bw = 0.0;
+            if (q >= 0.0 && q <= 1.0) bw = factor * (c23 - p2(q) + 0.5 * p3(q));
+            if (q > 1.0 && q <= 2.0) bw = factor * (c16 * p3(2.0 - q));
+            return bw;
+        }
     }
-    const double factor = 15.0 / (7.0 * PI) * p2(sh / bl);
-    const double c23 = real4(2.0f / 3.0f), c16 = real4(1.0f / 6.0f);
-    double bw = 0.0;
-    if (q >= 0.0 && q <= 1.0) bw = factor * (c23 - p2(q) + 0.5 * p3(q));
-    if (q > 1.0 && q <= 2.0) bw = factor * (c16 * p3(2.0 - q));
-    return bw;
 }
 
 // ---------------------------------------------------------------------------
@@ -641,7 +741,7 @@ void *orc_create(const simp_params *P, int maxn, int maxnb) {
     Orc *o = new Orc();
     o->P = *P;
     o->maxn = maxn; o->maxnb = maxnb;
-    o->scale_h = (P->skf == SIMP_SKF_CUBIC) ? 2 : 1;   // initialize.f90:208-217
+    o->scale_h = scale_h_of(P->skf);   // initialize.f90:208-217
     return o;
 }
 
@@ -782,7 +882,7 @@ int orc_step(void *hh, int nsteps, double *t, double *dt) {
 // Single pair-kernel evaluation for known-answer tests.
 int orc_kernel(const simp_params *P, double r, double hij, double dx, double dy,
                double *w, double *dwx, double *dwy, double *k0) {
-    Orc o; o.P = *P; o.scale_h = (P->skf == SIMP_SKF_CUBIC) ? 2 : 1;
+    Orc o; o.P = *P; o.scale_h = scale_h_of(P->skf);
     const double d[2] = {dx, dy};
     double dw[2];
     pair_kernel(o, r, hij, d, w, dw, k0);
@@ -791,7 +891,7 @@ int orc_kernel(const simp_params *P, double r, double hij, double dx, double dy,
 }
 
 double orc_boundary_w(const simp_params *P, double br) {
-    Orc o; o.P = *P; o.scale_h = (P->skf == SIMP_SKF_CUBIC) ? 2 : 1;
+    Orc o; o.P = *P; o.scale_h = scale_h_of(P->skf);
     o.hsml_ij.assign(1, P->b_length);
     return boundary_w(o, br, 1);
 }

@@ -108,7 +108,7 @@ __global__ void k_grow_xabs(Scalars *sc, double xa) {
 Phys make_phys(const simp_params &p, double max_hsml) {
     Phys P{};
     P.skf = p.skf;
-    P.scale_h = (p.skf == SIMP_SKF_CUBIC) ? 2 : 1;
+    P.scale_h = scale_h_of(p.skf);
     P.viscosity = p.viscosity;
     P.pressure_force = p.pressure_force;
     P.eos_alg = p.eos_alg;
@@ -150,7 +150,7 @@ int check_params(simp_ctx *c, const simp_params &p, bool batch) {
     if (p.rheology != 1) return bad("rheology (only 1, elliptical)");
     if (p.eos_alg != 1 && p.eos_alg != 3) return bad("eos_alg (1 or 3)");
     if (p.pa_sph != 1) return bad("pa_sph (only 1)");
-    if (p.skf != SIMP_SKF_WENDLAND_C6 && p.skf != SIMP_SKF_CUBIC) return bad("skf (6 or 9)");
+    if (!skf_known(p.skf)) return bad("skf (1 to 9)");
     if (p.den_alg != 3) return bad("den_alg (3 in the step; the summation density is simp_gpu_sum_density)");
     if (p.bfa != 1) return bad("bfa (only 1, Monaghan)");
     if (p.boundary_friction) return bad("boundary_friction");

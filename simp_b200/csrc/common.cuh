@@ -151,7 +151,7 @@ __device__ __forceinline__ double bitsd(unsigned long long b) {
 // Compile-time physics switches and constants for the pair passes.
 struct Phys {
     int skf;        // SIMP_SKF_*
-    int scale_h;    // 1 (C6) or 2 (cubic)
+    int scale_h;    // scale_h_of(skf)
     int viscosity, pressure_force, eos_alg;
     int wind_force, water_force, wind_kind;
     int boundary_pressure;
@@ -199,73 +199,204 @@ __device__ __forceinline__ long long ref_bin(double v, double bs) {
 }
 
 // ---------------------------------------------------------------------------
-// Pair kernel gradient factor.  With q = r / hij * scale_h this returns
-//   w      (kernel value)
-//   gfac   such that dwdx = gfac * dx  (i.e. dW/dq-term / hij / r * scale_h)
-// kernel.f90:498-508 (Wendland C6) and kernel.f90:324-340 (cubic spline,
-// restored with factor = 15/(7 pi) (scale_h / hij)^2).
+// Smoothing kernels (kernel.f90:5-633).  With q = r / hsml_ij * scale_h and
+// shh = scale_h / hsml_ij, kernel_wg gives W and gq = factor * dW/dq, so that
+// grad W = gq * shh * (dx / r).  The reference's default-real literals keep
+// their single-precision values.
+__host__ __device__ constexpr int scale_h_of(int skf) {   // initialize.f90:208-217
+    return (skf == SIMP_SKF_WENDLAND_C2 || skf == SIMP_SKF_WENDLAND_C4 || skf == SIMP_SKF_WENDLAND_C6) ? 1
+         : (skf == SIMP_SKF_QUADRATIC || skf == SIMP_SKF_CUBIC) ? 2 : 3;
+}
+__host__ __device__ constexpr bool skf_known(int skf) { return skf >= 1 && skf <= 9; }
+
+__device__ __forceinline__ double kexp(double v) { return exp(v); }
+__device__ __forceinline__ float kexp(float v) { return expf(v); }
+__device__ __forceinline__ double ktanh(double v) { return tanh(v); }
+__device__ __forceinline__ float ktanh(float v) { return tanhf(v); }
+__device__ __forceinline__ double kcosh(double v) { return cosh(v); }
+__device__ __forceinline__ float kcosh(float v) { return coshf(v); }
+__device__ __forceinline__ double klog(double v) { return log(v); }
+__device__ __forceinline__ float klog(float v) { return logf(v); }
+
+// The reference's log(2.) takes a default-real argument: the single-precision
+// logarithm of 2 (0.693147182464599609375), promoted.
+constexpr double kLog2Real4 = 0.693147182464599609375;
+constexpr double kMarquis2C1 = 10.0, kMarquis2C2 = 50.0;   // kernel.f90:602-603
+
+template <class T, bool WANT_W>
+__device__ __forceinline__ void kernel_wg(int skf, T q, T shh, T inv_h, T *w, T *gq) {
+    const T s2 = shh * shh;
+    switch (skf) {
+        case SIMP_SKF_QUADRATIC: {   // kernel.f90:269-276
+            const T f = (T)(2.0 / kPi) * s2;
+            if (WANT_W) *w = f * fma(T(0.1875) * q, q, fma(T(-0.75), q, T(0.75)));
+            *gq = f * fma(T(0.375), q, T(-0.75));
+            break;
+        }
+        case SIMP_SKF_GAUSSIAN: {    // kernel.f90:136-144
+            const T f = (T)(1.0 / kPi) * s2;
+            const T e = kexp(-(q * q));
+            if (WANT_W) *w = f * e;
+            *gq = f * (T(-2) * q * e);
+            break;
+        }
+        case SIMP_SKF_QUINTIC: {     // kernel.f90:193-219
+            const T f = (T)(7.0 / (478.0 * kPi)) * s2;
+            const T u3 = T(3) - q, u2 = T(2) - q, u1 = T(1) - q;
+            const T a3 = u3 * u3, a2 = u2 * u2, a1 = u1 * u1;
+            T wq = 0, g = 0;
+            if (q <= T(1)) {
+                wq = a3 * a3 * u3 - T(6) * a2 * a2 * u2 + T(15) * a1 * a1 * u1;
+                g = T(-5) * a3 * a3 + T(30) * a2 * a2 - T(75) * a1 * a1;
+            } else if (q <= T(2)) {
+                wq = a3 * a3 * u3 - T(6) * a2 * a2 * u2;
+                g = T(-5) * a3 * a3 + T(30) * a2 * a2;
+            } else if (q <= T(3)) {
+                wq = a3 * a3 * u3;
+                g = T(-5) * a3 * a3;
+            }
+            if (WANT_W) *w = f * wq;
+            *gq = f * g;
+            break;
+        }
+        case SIMP_SKF_WENDLAND_C2: { // kernel.f90:387-393
+            const T f = (T)(3.0 / (2.0 * kPi)) * s2;
+            const T om = T(1) - q, om2 = om * om;
+            if (WANT_W) *w = f * (om2 * om2 * fma(T(4), q, T(1)));
+            *gq = f * (T(-20) * q * (om2 * om));
+            break;
+        }
+        case SIMP_SKF_WENDLAND_C4: { // kernel.f90:443-450
+            const T f = (T)(3.0 / kPi) * s2;
+            const T om = T(1) - q, om2 = om * om, om4 = om2 * om2;
+            if (WANT_W) *w = f * (om4 * om2 * fma(fma(T(35), q, T(18)), q, T(3)));
+            *gq = f * (T(-56) * q * fma(T(5), q, T(1)) * (om4 * om));
+            break;
+        }
+        case SIMP_SKF_MARQUIS: {     // kernel.f90:555-563
+            const T f = (T)(1.0 / kPi) * s2;
+            const T z = T(300) * (q - T(1));
+            if (WANT_W) *w = f * (T(0.5) - T(0.5) * ktanh(z));
+            const T c = kcosh(z);
+            *gq = f * (T(-150) / (c * c));
+            break;
+        }
+        case SIMP_SKF_MARQUIS2: {    // kernel.f90:612-620 (factor without scale_h)
+            const T f = (T)(1.0 / ((double)34.1558f * kPi)) * (inv_h * inv_h);
+            const T c1 = (T)kMarquis2C1, c2 = (T)kMarquis2C2;
+            const T z = c1 * (T(1) - q);
+            if (WANT_W) *w = f * c2 * (klog(kcosh(z)) / c1 - q + T(1) + (T)kLog2Real4 / c1);
+            *gq = f * (-c2 * ktanh(z) - T(1));
+            break;
+        }
+        case SIMP_SKF_WENDLAND_C6: { // kernel.f90:499-508
+            const T f = (T)(78.0 / (7.0 * kPi)) * s2;
+            const T om = T(1) - q;
+            const T om2 = om * om, om4 = om2 * om2;
+            if (WANT_W) *w = f * (om4 * om4) * (((T(32) * q + T(25)) * q + T(8)) * q + T(1));
+            *gq = f * (T(-22) * q * (om4 * om2 * om) * ((T(16) * q + T(7)) * q + T(1)));
+            break;
+        }
+        default: {                   // SIMP_SKF_CUBIC, kernel.f90:324-340 restored
+            const T f = (T)(15.0 / (7.0 * kPi)) * s2;
+            if (q <= T(1)) {
+                if (WANT_W) *w = f * fma(T(0.5) * q * q, q, fma(-q, q, (T)(2.0f / 3.0f)));
+                *gq = f * fma(T(1.5) * q, q, T(-2) * q);
+            } else {
+                const T u = T(2) - q;
+                if (WANT_W) *w = f * ((T)(1.0f / 6.0f) * u * u * u);
+                *gq = f * (T(-0.5) * u * u);
+            }
+            break;
+        }
+    }
+}
+
+// FP64 pair kernel: w and gfac with grad W = gfac * dx.
 template <bool WANT_W>
 __device__ __forceinline__ void pair_kernel(const Phys &P, double r, double hij,
                                             double *w, double *gfac) {
     const double sh = (double)P.scale_h;
     const double inv_h = 1.0 / hij;
-    const double q = r * inv_h * sh;
     const double shh = sh * inv_h;
-    if (P.skf == SIMP_SKF_WENDLAND_C6) {
-        const double factor = (78.0 / (7.0 * kPi)) * (shh * shh);
-        const double om = 1.0 - q;
-        const double om2 = om * om, om4 = om2 * om2;
-        const double om7 = om4 * om2 * om;
-        if (WANT_W) *w = factor * (om4 * om4) * (((32.0 * q + 25.0) * q + 8.0) * q + 1.0);
-        const double g = factor * (-22.0 * q * om7 * ((16.0 * q + 7.0) * q + 1.0));
-        *gfac = g * shh / r;
-    } else {
-        const double factor = (15.0 / (7.0 * kPi)) * (shh * shh);
-        const double c23 = (double)(2.0f / 3.0f), c16 = (double)(1.0f / 6.0f);
-        double g, wt;
-        if (q <= 1.0) {
-            wt = factor * (c23 - q * q + 0.5 * q * q * q);
-            g = factor * (-2.0 * q + 1.5 * q * q);
-        } else {
-            const double u = 2.0 - q;
-            wt = factor * (c16 * u * u * u);
-            g = factor * (-0.5 * u * u);
+    const double q = r * shh;
+    double gq;
+    kernel_wg<double, WANT_W>(P.skf, q, shh, inv_h, w, &gq);
+    *gfac = gq * shh / r;
+}
+
+// Kernel value at q = 0 with smoothing length hij (kernel_zero of each kernel).
+__device__ __forceinline__ double kernel_zero(const Phys &P, double hij) {
+    const double shh = (double)P.scale_h / hij;
+    const double s2 = shh * shh;
+    switch (P.skf) {
+        case SIMP_SKF_QUADRATIC: return (2.0 / kPi) * s2 * 0.75;
+        case SIMP_SKF_GAUSSIAN: return (1.0 / kPi) * s2;
+        case SIMP_SKF_QUINTIC: return (7.0 / (478.0 * kPi)) * s2 * 66.0;
+        case SIMP_SKF_WENDLAND_C2: return (3.0 / (2.0 * kPi)) * s2;
+        case SIMP_SKF_WENDLAND_C4: return (3.0 / kPi) * s2 * 3.0;
+        case SIMP_SKF_MARQUIS: return (1.0 / kPi) * s2 * 0.5;
+        case SIMP_SKF_MARQUIS2: {
+            const double f = 1.0 / ((double)34.1558f * kPi * hij * hij);
+            return f * kMarquis2C2 * (log(cosh(kMarquis2C1)) / kMarquis2C1 + 1.0 + kLog2Real4 / kMarquis2C1);
         }
-        if (WANT_W) *w = wt;
-        *gfac = g * shh / r;
+        case SIMP_SKF_WENDLAND_C6: return (78.0 / (7.0 * kPi)) * s2;
+        default: return (15.0 / (7.0 * kPi)) * s2 * (double)(2.0f / 3.0f);
     }
 }
 
-// Kernel value at q = 0 with smoothing length hij (kernel_zero, kernel.f90:503).
-__device__ __forceinline__ double kernel_zero(const Phys &P, double hij) {
-    const double sh = (double)P.scale_h;
-    const double shh = sh / hij;
-    if (P.skf == SIMP_SKF_WENDLAND_C6) return (78.0 / (7.0 * kPi)) * (shh * shh);
-    return (15.0 / (7.0 * kPi)) * (shh * shh) * (double)(2.0f / 3.0f);
-}
-
-// Boundary kernel value bw at distance br (support b_length).
-// Wendland C6: boundary_kernel.f90:489-494; its factor uses a particle-pair
-// smoothing length (hsml_ij indexed by the boundary-pair index), for which the
-// particle's own hsml stands here (identical whenever hsml is uniform).
-// Cubic: b_Quadratic's form (boundary_kernel.f90:106-112) with the cubic
-// spline, support b_length, scale_h = 2.
+// Boundary kernel value bw at distance br (support b_length),
+// boundary_kernel.f90:20-45 dispatch: b_Quadratic :106-112, b_Gaussian
+// :177-183 (also for the Marquis kernels), b_quintic_spline :250-276 (its
+// factor is 15/(478 pi), not the particle kernel's 7/(478 pi)),
+// b_Wendland_C2 :342-347, b_Wendland_C4 :416-420, b_Wendland_C6 :489-494.
+// The C6 factor uses a particle-pair smoothing length (hsml_ij indexed by
+// the boundary-pair index), for which the particle's own hsml stands here
+// (identical whenever hsml is uniform).  Cubic: b_Quadratic's form with the
+// cubic spline, support b_length, scale_h = 2.
 __device__ __forceinline__ double boundary_w(const Phys &P, double br, double hs_i) {
     const double sh = (double)P.scale_h;
     const double q = br / P.b_length * sh;
-    if (P.skf == SIMP_SKF_WENDLAND_C6) {
-        const double shh = sh / hs_i;
-        const double factor = (78.0 / (7.0 * kPi)) * (shh * shh);
-        const double om = 1.0 - q;
-        const double om2 = om * om, om4 = om2 * om2;
-        return factor * (om4 * om4) * (((32.0 * q + 25.0) * q + 8.0) * q + 1.0);
+    const double shb = sh / P.b_length, s2 = shb * shb;
+    switch (P.skf) {
+        case SIMP_SKF_QUADRATIC:
+            return (2.0 / kPi) * s2 * (0.1875 * q * q - 0.75 * q + 0.75);
+        case SIMP_SKF_GAUSSIAN:
+        case SIMP_SKF_MARQUIS:
+        case SIMP_SKF_MARQUIS2:
+            return (1.0 / kPi) * s2 * exp(-(q * q));
+        case SIMP_SKF_QUINTIC: {
+            const double f = (15.0 / (478.0 * kPi)) * s2;
+            const double u3 = 3.0 - q, u2 = 2.0 - q, u1 = 1.0 - q;
+            const double p3 = u3 * u3 * u3 * u3 * u3, p2 = u2 * u2 * u2 * u2 * u2, p1 = u1 * u1 * u1 * u1 * u1;
+            if (q <= 1.0) return f * (p3 - 6.0 * p2 + 15.0 * p1);
+            if (q <= 2.0) return f * (p3 - 6.0 * p2);
+            if (q <= 3.0) return f * p3;
+            return 0.0;
+        }
+        case SIMP_SKF_WENDLAND_C2: {
+            const double om = 1.0 - q, om2 = om * om;
+            return (3.0 / (2.0 * kPi)) * s2 * (om2 * om2 * (1.0 + 4.0 * q));
+        }
+        case SIMP_SKF_WENDLAND_C4: {
+            const double om = 1.0 - q, om2 = om * om;
+            return (3.0 / kPi) * s2 * (om2 * om2 * om2 * ((35.0 * q + 18.0) * q + 3.0));
+        }
+        case SIMP_SKF_WENDLAND_C6: {
+            const double shh = sh / hs_i;
+            const double factor = (78.0 / (7.0 * kPi)) * (shh * shh);
+            const double om = 1.0 - q;
+            const double om2 = om * om, om4 = om2 * om2;
+            return factor * (om4 * om4) * (((32.0 * q + 25.0) * q + 8.0) * q + 1.0);
+        }
+        default: {
+            const double factor = (15.0 / (7.0 * kPi)) * s2;
+            const double c23 = (double)(2.0f / 3.0f), c16 = (double)(1.0f / 6.0f);
+            if (q <= 1.0) return factor * (c23 - q * q + 0.5 * q * q * q);
+            if (q <= 2.0) { const double u = 2.0 - q; return factor * (c16 * u * u * u); }
+            return 0.0;
+        }
     }
-    const double shb = sh / P.b_length;
-    const double factor = (15.0 / (7.0 * kPi)) * (shb * shb);
-    const double c23 = (double)(2.0f / 3.0f), c16 = (double)(1.0f / 6.0f);
-    if (q <= 1.0) return factor * (c23 - q * q + 0.5 * q * q * q);
-    if (q <= 2.0) { const double u = 2.0 - q; return factor * (c16 * u * u * u); }
-    return 0.0;
 }
 
 // Wind at a particle of an instance: uniform (the reference hard-codes one,

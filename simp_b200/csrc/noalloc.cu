@@ -233,13 +233,13 @@ extern "C" int32_t simp_gpu_sum_density_noalloc(const double *x, const double *h
     using namespace simp;
     using namespace simp::noalloc;
     if (n < 1 || n > kMaxN || !x || !hsml || !mass || !rho || !rho_out) return SIMP_ERR_BADARG;
-    if (skf != SIMP_SKF_WENDLAND_C6 && skf != SIMP_SKF_CUBIC) return SIMP_ERR_BADARG;
+    if (!skf_known(skf)) return SIMP_ERR_BADARG;
     unsigned char *base = nullptr;
     if (scratch_address(&base) != cudaSuccess) return SIMP_ERR_CUDA;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     Phys P{};
     P.skf = skf;
-    P.scale_h = (skf == SIMP_SKF_CUBIC) ? 2 : 1;
+    P.scale_h = scale_h_of(skf);
     k_clear<<<nblk(kMaxCells + 1, 256), 256, 0, s>>>(base);
     k_bounds<<<nblk(n, kB), kB, 0, s>>>(base, n, x, hsml);
     k_grid<<<1, 1, 0, s>>>(base);

@@ -99,24 +99,9 @@ __device__ __forceinline__ PairGeom<T> pair_geom(const Phys &P, T dx, T dy, T hi
     const T sh = (T)P.scale_h;
     const T shh = sh * inv_h;
     const T q = r * shh;
-    T gq;
-    if (P.skf == SIMP_SKF_WENDLAND_C6) {
-        const T factor = (T)(78.0 / (7.0 * kPi)) * (shh * shh);
-        const T om = T(1) - q;
-        const T om2 = om * om, om4 = om2 * om2;
-        if (WANT_W) g.w = factor * (om4 * om4) * (((T(32) * q + T(25)) * q + T(8)) * q + T(1));
-        gq = factor * (T(-22) * q * (om4 * om2 * om) * ((T(16) * q + T(7)) * q + T(1)));
-    } else {
-        const T factor = (T)(15.0 / (7.0 * kPi)) * (shh * shh);
-        if (q <= T(1)) {
-            if (WANT_W) g.w = factor * fma(T(0.5) * q * q, q, fma(-q, q, (T)(2.0f / 3.0f)));
-            gq = factor * fma(T(1.5) * q, q, T(-2) * q);
-        } else {
-            const T u = T(2) - q;
-            if (WANT_W) g.w = factor * ((T)(1.0f / 6.0f) * u * u * u);
-            gq = factor * (T(-0.5) * u * u);
-        }
-    }
+    T gq, w = 0;
+    kernel_wg<T, WANT_W>(P.skf, q, shh, inv_h, &w, &gq);
+    if (WANT_W) g.w = w;
     g.gfac = gq * shh * rs;
     return g;
 }

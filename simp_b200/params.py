@@ -12,8 +12,19 @@ from __future__ import annotations
 import ctypes
 import struct
 
+SKF_QUADRATIC = 1
+SKF_GAUSSIAN = 2
+SKF_QUINTIC = 3
+SKF_WENDLAND_C2 = 4
+SKF_WENDLAND_C4 = 5
 SKF_WENDLAND_C6 = 6
+SKF_MARQUIS = 7
+SKF_MARQUIS2 = 8
 SKF_CUBIC = 9
+# kernel code -> the key of its known-answer fixture and its scale_h
+KERNELS = {1: ("quadratic", 2), 2: ("gaussian", 3), 3: ("quintic", 3), 4: ("wendland_c2", 1),
+           5: ("wendland_c4", 1), 6: ("wendland_c6", 1), 7: ("marquis", 3), 8: ("marquis2", 3),
+           9: ("cubic", 2)}
 PREC_FP64 = 0
 PREC_MIXED = 1
 WIND_UNIFORM = 0

@@ -120,7 +120,7 @@ def test_noalloc_rejects_bad_sizes_before_touching_the_device(lib):
     # n out of range and bad kernel codes are refused on the host
     assert lib.simp_gpu_sum_density_noalloc(1, 1, 1, 1, 0, 9, 1, None) == 1
     assert lib.simp_gpu_sum_density_noalloc(1, 1, 1, 1, 65537, 9, 1, None) == 1
-    assert lib.simp_gpu_sum_density_noalloc(1, 1, 1, 1, 10, 7, 1, None) == 1
+    assert lib.simp_gpu_sum_density_noalloc(1, 1, 1, 1, 10, 10, 1, None) == 1
 
 
 def test_missing_library_fails_loudly(tmp_path):

@@ -29,7 +29,11 @@ def _mixed(b, skf=None):
     return prm
 
 
-@pytest.mark.parametrize("skf", [9, SKF_WENDLAND_C6])
+# (not the Marquis kernel, 7: its gradient -150 / cosh(300 (q - 1))^2
+# vanishes to double precision at the lattice distances here, and FP32's
+# overflow of cosh^2 there turns a relative measure of a zero field into
+# noise; the plain form runs it against the oracle)
+@pytest.mark.parametrize("skf", [9, SKF_WENDLAND_C6, 1, 2, 3, 4, 5, 8])
 def test_mixed_single_step(gpu_lib, oracle_mod, skf):
     b = basins.cfg1()
     b.vx = smooth_velocity(b.x, b.L, seed=11)

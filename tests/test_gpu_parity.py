@@ -121,7 +121,7 @@ def test_max_ind_int_error(gpu_lib):
     assert e.value.code == SIMP_ERR_IND_INT
 
 
-@pytest.mark.parametrize("skf", [9, 6])
+@pytest.mark.parametrize("skf", [9, 6, 1, 2, 3, 4, 5, 7, 8])
 def test_single_step_fields(gpu_lib, oracle_mod, skf):
     """One RHS (single_step.f90) on a sheared, drifting state with drag on."""
     b = basins.cfg1()
@@ -146,6 +146,23 @@ def test_single_step_at_rest_no_drag(gpu_lib, oracle_mod):
     assert np.all(rg["dhdt"] == 0.0) and np.all(ro["dhdt"] == 0.0)
     d = g.get_diag()
     assert np.all(d["sig11"] == 0.0) and np.all(d["eps12"] == 0.0)
+
+
+@pytest.mark.parametrize("skf", [1, 2, 3, 4, 5, 7, 8])
+def test_other_kernels_density_and_steps(gpu_lib, oracle_mod, skf):
+    """Every reference kernel (kernel.f90, boundary_kernel.f90): summation
+    density and 5 steps against the oracle."""
+    b = basins.cfg1()
+    b.vx = smooth_velocity(b.x, b.L, amp=0.3, seed=30 + skf)
+    prm = b.params.copy()
+    prm.skf = skf
+    g, o = _pair(b, oracle_mod, prm)
+    assert rel_l2(g.sum_density(), o.sum_density()) < TOL_RHS
+    g.time_integration(5)
+    o.step(5)
+    sg, so = g.get_state(), o.get_state()
+    for k in ("x", "vx", "h", "A", "rho"):
+        assert rel_l2(sg[k], so[k]) < 1e-9, (k, rel_l2(sg[k], so[k]))
 
 
 def test_sum_density(gpu_lib, oracle_mod):
