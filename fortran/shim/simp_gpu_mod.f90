@@ -27,7 +27,7 @@ module simp_gpu_mod
                           b_length, kappa_n, kappa_t, alpha,                &
                           wind_u, wind_v, current_u, current_v,             &
                           vortex_x, vortex_y, vortex_umax, vortex_radius,   &
-                          dt, max_hsml, skin
+                          dt, max_hsml, skin, zeta_max, eta_max, phi
     end type simp_params
 
     ! Mirror of struct simp_forcing (per-basin wind of a batch).

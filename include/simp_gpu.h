@@ -78,13 +78,16 @@ enum { SIMP_WIND_UNIFORM = 0, SIMP_WIND_VORTEX = 1 };
  */
 typedef struct simp_params {
     /* algorithm switches, reference codes */
-    int32_t int_algorithm;     /* 2 predictor-corrector (time_integration.f90:155-282) */
+    int32_t int_algorithm;     /* 1 Euler, 2 predictor-corrector, 3 leap-frog
+                                  (time_integration.f90:86-148, 155-282, 289-391)     */
     int32_t nnps_algorithm;    /* 2 bucket search, 1 direct find (nnps.f90:21-30)       */
     int32_t sle;               /* 0 keep hsml, 2 Marquis hsml (smoothing_length.f90)    */
     int32_t tse;               /* 0 keep dt, 2 VP criterion (time_step.f90:132-157)     */
-    int32_t rheology;          /* 1 elliptical yield curve                              */
-    int32_t eos_alg;           /* 1 Hibler, 3 Kreyscher replacement pressure            */
-    int32_t pa_sph;            /* 1 (p_i/rho_i^2 + p_j/rho_j^2) form                    */
+    int32_t rheology;          /* 1 elliptical yield curve, 2 Mohr-Coulomb
+                                  (bulk_viscosity.f90, shear_viscosity.f90)           */
+    int32_t eos_alg;           /* 1 Hibler, 2 Gutfraind, 3 Kreyscher (eos.f90)         */
+    int32_t pa_sph;            /* 1 (s_i/rho_i^2 + s_j/rho_j^2) stress_1,
+                                  2 (s_i + s_j)/rho_j stress_2 (internal_stress.f90)  */
     int32_t skf;               /* SIMP_SKF_*                                            */
     int32_t den_alg;           /* 3 diagnostic, 1 summation (density.f90:20-30)         */
     int32_t bfa;               /* 1 Monaghan boundary force                             */
@@ -115,6 +118,10 @@ typedef struct simp_params {
     double max_hsml;           /* Marquis_hsml cap; <= 0: 10 * max(hsml) at set_state
                                   (initialize.f90:191)                                */
     double skin;               /* GPU cell-list skin (m); < 0: automatic               */
+    /* Mohr-Coulomb rheology (data_variables.f90:153-180): viscosity caps per unit
+       pressure (declared without a value in the reference, so 0 there) and the
+       friction angle phi (degrees; mu = tan(phi)) */
+    double zeta_max, eta_max, phi;
 } simp_params;
 
 /* Shipped values of globals.f90 and data_variables.f90, including the

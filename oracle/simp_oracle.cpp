@@ -442,19 +442,48 @@ void internal_stress(Orc &o) {
     if (P.viscosity) {
         for (int i = 0; i < n; ++i)
             o.p[i] = P.P_star * o.h[i] * std::exp(-(P.c_eos * (1.0 - o.A[i])));   // :24
-        for (int i = 0; i < n; ++i) {                                              // bulk :65-76
-            double delta = std::pow((p2(o.eps11[i]) + p2(o.eps22[i])) * (1.0 + em2) +
-                                    4.0 * em2 * p2(o.eps12[i]) +
-                                    2.0 * o.eps11[i] * o.eps22[i] * (1.0 - em2), 0.5);
-            if (std::fabs(delta) < P.delta_min) delta = P.delta_min;
-            o.zeta[i] = 0.5 * o.p[i] * (1.0 + P.k_t) / delta;
+        if (P.rheology == 2) {
+            // Mohr-Coulomb: MC_bulk_viscosity (bulk_viscosity.f90:86-145) and
+            // MC_shear_viscosity (shear_viscosity.f90:67-124); mu = tan(phi pi/180.)
+            const double zero = 1.0e-18, mu = std::tan(P.phi * PI / 180.0);
+            std::vector<double> e1(n), e2(n);
+            for (int i = 0; i < n; ++i) {
+                const double rt = std::sqrt(p2(o.eps11[i] - o.eps22[i]) + 4 * p2(o.eps12[i]));
+                e1[i] = 0.5 * ((o.eps11[i] + o.eps22[i]) + rt);
+                e2[i] = 0.5 * ((o.eps11[i] + o.eps22[i]) - rt);
+                double eI = std::fabs(e1[i] + e2[i]);
+                if (eI < zero) eI = zero;
+                o.zeta[i] = 0.5 * o.p[i] * (1 + P.k_t) / eI;
+                if (o.zeta[i] > P.zeta_max * o.p[i]) o.zeta[i] = P.zeta_max * o.p[i];
+            }
+            for (int i = 0; i < n; ++i) {
+                double eII = e1[i] - e2[i];
+                if (std::fabs(eII) < zero) eII = zero;
+                o.eta[i] = mu * (0.5 * o.p[i] * (1 + P.k_t) - o.zeta[i] * (e1[i] + e2[i])) / eII;
+                if (o.eta[i] > P.eta_max * o.p[i]) o.eta[i] = P.eta_max * o.p[i];
+            }
+        } else {
+            for (int i = 0; i < n; ++i) {                                          // bulk :65-76
+                double delta = std::pow((p2(o.eps11[i]) + p2(o.eps22[i])) * (1.0 + em2) +
+                                        4.0 * em2 * p2(o.eps12[i]) +
+                                        2.0 * o.eps11[i] * o.eps22[i] * (1.0 - em2), 0.5);
+                if (std::fabs(delta) < P.delta_min) delta = P.delta_min;
+                o.zeta[i] = 0.5 * o.p[i] * (1.0 + P.k_t) / delta;
+            }
+            for (int i = 0; i < n; ++i) o.eta[i] = o.zeta[i] / (P.e * P.e);        // shear :57
         }
-        for (int i = 0; i < n; ++i) o.eta[i] = o.zeta[i] / (P.e * P.e);            // shear :57
     }
     if (P.pressure_force) {
         if (P.eos_alg == 1) {
             for (int i = 0; i < n; ++i)
                 o.p[i] = P.P_star * o.h[i] * std::exp(-(P.c_eos * (1.0 - o.A[i])));
+        } else if (P.eos_alg == 2) {  // gutfraind_eos :96-104
+            const double rho_max = 934.0, rho_0 = P.rho_ice;
+            for (int i = 0; i < n; ++i) {
+                const double gamma = 1.9e5 * o.h[i] * std::exp(-20 * (1 - o.A[i]));
+                o.p[i] = gamma * (o.rho[i] - rho_0) / (rho_max - o.rho[i]);
+                if (o.p[i] < 0.0) o.p[i] = 0.0;
+            }
         } else {  // kreyscher_eos :141-147
             for (int i = 0; i < n; ++i) {
                 const double delta = std::pow((p2(o.eps11[i]) + p2(o.eps22[i])) * (1.0 + em2) +
@@ -471,8 +500,24 @@ void internal_stress(Orc &o) {
         o.sig22[i] = (o.zeta[i] + o.eta[i]) * o.eps22[i] + (o.zeta[i] - o.eta[i]) * o.eps11[i] -
                      o.p[i] * (1.0 - P.k_t) / 2.0;
     }
-    // stress_1 :103-137 (REDUCTION(+:dvxdt))
     const double rho_ice = P.rho_ice;
+    if (P.pa_sph == 2) {
+        // stress_2 :146-219
+        reduce_pairs(o.nip, o.dvxdt.data(), 2 * (size_t)n, 4096, [&](int k, double *dv) {
+            const int i = o.p_i[k] - 1, j = o.p_j[k] - 1;
+            const double g1 = o.dwdx[2 * k], g2 = o.dwdx[2 * k + 1];
+            double cj = (o.sig11[j] * g1 + o.sig12[j] * g2);
+            double ci = (o.sig11[i] * g1 + o.sig12[i] * g2);
+            dv[2 * i] = dv[2 * i] + o.mass[j] / rho_ice / o.h[i] / o.rho[j] * (ci + cj);
+            dv[2 * j] = dv[2 * j] - o.mass[i] / rho_ice / o.h[j] / o.rho[i] * (ci + cj);
+            cj = (o.sig12[j] * g1 + o.sig22[j] * g2);
+            ci = (o.sig12[i] * g1 + o.sig22[i] * g2);
+            dv[2 * i + 1] = dv[2 * i + 1] + o.mass[j] / rho_ice / o.h[i] / o.rho[j] * (ci + cj);
+            dv[2 * j + 1] = dv[2 * j + 1] - o.mass[i] / rho_ice / o.h[j] / o.rho[i] * (ci + cj);
+        });
+        return;
+    }
+    // stress_1 :103-137 (REDUCTION(+:dvxdt))
     reduce_pairs(o.nip, o.dvxdt.data(), 2 * (size_t)n, 4096, [&](int k, double *dv) {
         const int i = o.p_i[k] - 1, j = o.p_j[k] - 1;
         const double g1 = o.dwdx[2 * k], g2 = o.dwdx[2 * k + 1];
@@ -715,6 +760,60 @@ void predictor_corrector(Orc &o) {
     time_step(o);
 }
 
+// euler_scheme, time_integration.f90:86-148.
+void euler_scheme(Orc &o) {
+    const int n = o.ntotal;
+    const double dt = o.dt;
+    single_step(o);
+    for (int k = 0; k < 2 * n; ++k) {
+        o.x[k] = o.x[k] + o.dxdt[k] * dt;
+        o.vx[k] = o.vx[k] + o.dvxdt[k] * dt;
+    }
+    for (int i = 0; i < n; ++i) {
+        o.h[i] = o.h[i] + o.dhdt[i] * dt;
+        o.A[i] = o.A[i] + o.dAdt[i] * dt;
+    }
+    clamp_A(o);
+    density(o);
+    mass_evolution(o);
+    smoothing_length(o);
+    time_step(o);
+}
+
+// leapfrog_scheme, time_integration.f90:289-391.
+void leapfrog_scheme(Orc &o) {
+    const int n = o.ntotal;
+    const double dt = o.dt;
+    std::vector<double> x1(o.x.begin(), o.x.begin() + 2 * n), vx1(o.vx.begin(), o.vx.begin() + 2 * n);
+    std::vector<double> h1(o.h.begin(), o.h.begin() + n), A1(o.A.begin(), o.A.begin() + n);
+    single_step(o);                                                  // :321
+    for (int k = 0; k < 2 * n; ++k) {
+        o.x[k] = o.x[k] + o.dxdt[k] * dt / 2;
+        o.vx[k] = o.vx[k] + o.dvxdt[k] * dt / 2;
+    }
+    for (int i = 0; i < n; ++i) {
+        o.h[i] = o.h[i] + o.dhdt[i] * dt / 2;
+        o.A[i] = o.A[i] + o.dAdt[i] * dt / 2;
+    }
+    clamp_A(o);
+    density(o);
+    mass_evolution(o);
+    single_step(o);                                                  // :351
+    for (int k = 0; k < 2 * n; ++k) {
+        o.vx[k] = vx1[k] + o.dvxdt[k] * dt;
+        o.x[k] = x1[k] + (vx1[k] + o.dxdt[k]) * dt / 2;
+    }
+    for (int i = 0; i < n; ++i) {
+        o.h[i] = h1[i] + o.dhdt[i] * dt;
+        o.A[i] = A1[i] + o.dAdt[i] * dt;
+    }
+    clamp_A(o);
+    density(o);
+    mass_evolution(o);
+    smoothing_length(o);
+    time_step(o);
+}
+
 int fail(Orc *o, int code, const char *msg) { o->err = msg; return code; }
 
 }  // namespace
@@ -866,7 +965,9 @@ int orc_sum_density(void *hh, int k0_mode, double *rho_out) {
 int orc_step(void *hh, int nsteps, double *t, double *dt) {
     Orc *o = (Orc *)hh;
     for (int s = 0; s < nsteps && !o->bad; ++s) {
-        predictor_corrector(*o);
+        if (o->P.int_algorithm == 1) euler_scheme(*o);              // time_integration.f90:46-53
+        else if (o->P.int_algorithm == 3) leapfrog_scheme(*o);
+        else predictor_corrector(*o);
         o->itimestep += 1;
         o->current_time = o->current_time + o->dt;
     }

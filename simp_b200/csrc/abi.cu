@@ -138,18 +138,24 @@ Phys make_phys(const simp_params &p, double max_hsml) {
     P.current_u = p.current_u;
     P.current_v = p.current_v;
     P.max_hsml = max_hsml;
+    P.rheology = p.rheology;
+    P.pa_sph = p.pa_sph;
+    P.int_algorithm = p.int_algorithm;
+    P.zeta_max = p.zeta_max;
+    P.eta_max = p.eta_max;
+    P.mu = tan(p.phi * kPi / 180.0);   // data_variables.f90:180
     return P;
 }
 
 int check_params(simp_ctx *c, const simp_params &p, bool batch) {
     auto bad = [&](const char *what) { return simp_fail(c, SIMP_ERR_BADARG, std::string("unsupported switch: ") + what); };
-    if (p.int_algorithm != 2) return bad("int_algorithm (only 2, predictor-corrector, is on this path)");
+    if (p.int_algorithm < 1 || p.int_algorithm > 3) return bad("int_algorithm (1 Euler, 2 predictor-corrector, 3 leap-frog)");
     if (p.nnps_algorithm != 1 && p.nnps_algorithm != 2) return bad("nnps_algorithm (1 or 2)");
     if (p.sle != 0 && p.sle != 2) return bad("sle (0 or 2)");
     if (p.tse != 0 && p.tse != 2) return bad("tse (0 or 2)");
-    if (p.rheology != 1) return bad("rheology (only 1, elliptical)");
-    if (p.eos_alg != 1 && p.eos_alg != 3) return bad("eos_alg (1 or 3)");
-    if (p.pa_sph != 1) return bad("pa_sph (only 1)");
+    if (p.rheology != 1 && p.rheology != 2) return bad("rheology (1 elliptical, 2 Mohr-Coulomb)");
+    if (p.eos_alg < 1 || p.eos_alg > 3) return bad("eos_alg (1, 2 or 3)");
+    if (p.pa_sph != 1 && p.pa_sph != 2) return bad("pa_sph (1 or 2)");
     if (!skf_known(p.skf)) return bad("skf (1 to 9)");
     if (p.den_alg != 3) return bad("den_alg (3 in the step; the summation density is simp_gpu_sum_density)");
     if (p.bfa != 1) return bad("bfa (only 1, Monaghan)");
@@ -522,21 +528,34 @@ int get_instance_state(simp_ctx *c, int slot, double *x, double *vx, double *mas
     return SIMP_OK;
 }
 
-// One predictor-corrector step (time_integration.f90:263-390).  With
-// profiling on, external event records between the kernels time each one.
+// One step of the selected integrator.  With profiling on, external event
+// records between the kernels time each one.
 void enqueue_step(simp_ctx *c, bool diag, bool prof) {
     auto mark = [&](int k) {
         if (prof) cudaEventRecordWithFlags(c->prof_ev[k], c->stream, cudaEventRecordExternal);
     };
     mark(0);
-    launch_kinematic(c, c->s0, false);
-    mark(1);
-    launch_stress(c, c->s0, c->s0, EPI_PREDICT);
-    mark(2);
-    launch_kinematic(c, c->s1, diag);
-    mark(3);
-    launch_stress(c, c->s1, c->s0, EPI_CORRECT);
-    mark(4);
+    if (c->prm.int_algorithm == 1) {
+        // euler_scheme (time_integration.f90:86-148): one right-hand side
+        launch_kinematic(c, c->s0, diag);
+        mark(1);
+        launch_stress(c, c->s0, c->s0, EPI_EULER);
+        mark(2);
+        launch_copy_s1_to_s0(c);
+        mark(3);
+        mark(4);
+    } else {
+        // predictor_corrector (:263-390) or leapfrog_scheme (:289-391): the
+        // same first half step, a different final update
+        launch_kinematic(c, c->s0, false);
+        mark(1);
+        launch_stress(c, c->s0, c->s0, EPI_PREDICT);
+        mark(2);
+        launch_kinematic(c, c->s1, diag);
+        mark(3);
+        launch_stress(c, c->s1, c->s0, c->prm.int_algorithm == 3 ? EPI_LEAP : EPI_CORRECT);
+        mark(4);
+    }
     launch_step_finish(c);
     mark(5);
 }
@@ -865,6 +884,9 @@ void simp_params_reference_default(simp_params *p) {
     p->dt = 0.0;
     p->max_hsml = 0.0;
     p->skin = -1.0;
+    p->zeta_max = 0.0;   // data_variables.f90:154 declares them without a value
+    p->eta_max = 0.0;
+    p->phi = 45.0;       // data_variables.f90:159
 }
 
 int32_t simp_gpu_create(const simp_params *params, int32_t maxn, int32_t maxnb, simp_ctx **out) {

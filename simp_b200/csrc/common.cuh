@@ -156,6 +156,7 @@ struct Phys {
     int wind_force, water_force, wind_kind;
     int boundary_pressure;
     int sle, den_alg, mass_from_area, tse, hsml_multiplicity;
+    int rheology, pa_sph, int_algorithm;
     int max_ind_int;
     double P_star, c_eos, e, delta_min, k_t;
     double rho_ice, rho_air, rho_water, c_wind, c_water;
@@ -163,6 +164,7 @@ struct Phys {
     double wind_u, wind_v, current_u, current_v;
     double vortex_x, vortex_y, vortex_umax, vortex_radius;
     double max_hsml;
+    double zeta_max, eta_max, mu;   // Mohr-Coulomb caps and tan(phi)
 };
 
 // Interaction-count bookkeeping for nnps.f90:613-670.

@@ -137,10 +137,14 @@ constexpr int kScanKernels = 4;         // kernels per launch_scan_i32
 size_t scan_tmp_bytes(int n);
 
 // passes.cu
-enum EpiMode : int { EPI_RATES = 0, EPI_PREDICT = 1, EPI_CORRECT = 2 };
+// stress-pass epilogues: the rates (single_step), the predictor half step
+// and the corrector (predictor_corrector), the Euler step, the leap-frog
+// second half (time_integration.f90:86-148, 263-390, 289-391)
+enum EpiMode : int { EPI_RATES = 0, EPI_PREDICT = 1, EPI_CORRECT = 2, EPI_EULER = 3, EPI_LEAP = 4 };
 void launch_kinematic(simp_ctx *c, const State &s, bool diag);
 void launch_stress(simp_ctx *c, const State &nb, const State &own, EpiMode mode);
 void launch_step_finish(simp_ctx *c);
+void launch_copy_s1_to_s0(simp_ctx *c);
 void launch_reset_stats(simp_ctx *c);
 
 // tiled.cu

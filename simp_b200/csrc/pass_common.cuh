@@ -330,25 +330,56 @@ __device__ __forceinline__ void kin_rheology(const KinArgs &a, int i, double dv,
     const double dcap = (fabs(delta) < P.delta_min) ? P.delta_min : delta;
     double zeta = 0.0, eta = 0.0, p = 0.0;
     if (P.viscosity) {
-        zeta = 0.5 * Pstr * (1.0 + P.k_t) / dcap;
-        eta = zeta / (P.e * P.e);
         p = Pstr;
+        if (P.rheology == 2) {
+            // Mohr-Coulomb, bulk_viscosity.f90:86-145 and shear_viscosity.f90:67-124
+            const double root = sqrt(fma(e11 - e22, e11 - e22, 4.0 * (e12 * e12)));
+            const double eps1 = 0.5 * ((e11 + e22) + root), eps2 = 0.5 * ((e11 + e22) - root);
+            const double zero = 1.0e-18;
+            double epsI = fabs(eps1 + eps2);
+            if (epsI < zero) epsI = zero;
+            zeta = 0.5 * p * (1.0 + P.k_t) / epsI;
+            if (zeta > P.zeta_max * p) zeta = P.zeta_max * p;
+            double epsII = eps1 - eps2;
+            if (fabs(epsII) < zero) epsII = zero;
+            eta = P.mu * (0.5 * p * (1.0 + P.k_t) - zeta * (eps1 + eps2)) / epsII;
+            if (eta > P.eta_max * p) eta = P.eta_max * p;
+        } else {
+            // elliptical, bulk_viscosity.f90:65-76 and shear_viscosity.f90:57
+            zeta = 0.5 * Pstr * (1.0 + P.k_t) / dcap;
+            eta = zeta / (P.e * P.e);
+        }
     }
-    if (P.pressure_force) p = (P.eos_alg == 3) ? zeta * 2.0 * delta / (1.0 + P.k_t) : Pstr;
+    if (P.pressure_force) {   // eos.f90:20-31
+        if (P.eos_alg == 3) {
+            p = zeta * 2.0 * delta / (1.0 + P.k_t);           // Kreyscher :141-147
+        } else if (P.eos_alg == 2) {
+            // Gutfraind :96-104 (rho_0 = rho_ice, rho_max = 934)
+            const double rho = s.rho[i];
+            const double gamma = 1.9e5 * hh * exp(-20.0 * (1.0 - AA));
+            p = gamma * (rho - P.rho_ice) / (934.0 - rho);
+            if (p < 0.0) p = 0.0;
+        } else {
+            p = Pstr;                                         // Hibler :59
+        }
+    }
     const double ph = p * (1.0 - P.k_t) / 2.0;
     const double s11 = fma(zeta + eta, e11, fma(zeta - eta, e22, -ph));
     const double s12 = 2.0 * eta * e12;
     const double s22 = fma(zeta + eta, e22, fma(zeta - eta, e11, -ph));
     const double rho = s.rho[i];
-    const double ir2 = 1.0 / (rho * rho);
+    // stress_1 pairs sigma / rho^2 with m; stress_2 pairs sigma with m / rho
+    // (internal_stress.f90:103-137, 146-219)
+    const double ir2 = (P.pa_sph == 2) ? 1.0 : 1.0 / (rho * rho);
+    const double mw = (P.pa_sph == 2) ? s.mor[i] : s.m[i];
     a.tau11[i] = s11 * ir2;
     a.tau12[i] = s12 * ir2;
     a.tau22[i] = s22 * ir2;
     if (a.rec.tq) {
-        a.rec.tq[i] = make_float4((float)(s11 * ir2), (float)(s12 * ir2), (float)(s22 * ir2), (float)s.m[i]);
+        a.rec.tq[i] = make_float4((float)(s11 * ir2), (float)(s12 * ir2), (float)(s22 * ir2), (float)mw);
     } else {
         a.rec.ta[i] = make_double2(s11 * ir2, s12 * ir2);
-        a.rec.tb[i] = make_double2(s22 * ir2, s.m[i]);
+        a.rec.tb[i] = make_double2(s22 * ir2, mw);
     }
     a.div[i] = dv;
     if (a.diag) {
@@ -518,7 +549,7 @@ __device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool l
     const State &s = a.rhs;
     const Phys &P = a.P;
     const double rho = s.rho[i], hh = s.h[i], AA = s.A[i], mi = s.m[i];
-    const double fi = rho / P.rho_ice / hh;
+    const double fi = (P.pa_sph == 2) ? 1.0 / P.rho_ice / hh : rho / P.rho_ice / hh;
     double ax = fi * fma(a.tau11[i], Sx, fma(a.tau12[i], Sy, Tx));
     double ay = fi * fma(a.tau12[i], Sx, fma(a.tau22[i], Sy, Ty));
     // boundary force (bf_Monaghan normal component, boundary_force.f90:78-82)
@@ -576,13 +607,30 @@ __device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool l
     const double x0 = b.x[i], y0 = b.y[i], vx0 = b.vx[i], vy0 = b.vy[i], h0 = b.h[i], A0 = b.A[i];
     double xn, yn, vxn, vyn, hn, An;
     if (a.mode == EPI_PREDICT) {
-        // time_integration.f90:315-323
+        // time_integration.f90:315-323 (and the leap-frog's first half, :323-332)
         xn = x0 + vxi * dt / 2.0;
         yn = y0 + vyi * dt / 2.0;
         vxn = vx0 + ax * dt / 2.0;
         vyn = vy0 + ay * dt / 2.0;
         hn = h0 + dhdt * dt / 2.0;
         An = A0 + dAdt * dt / 2.0;
+    } else if (a.mode == EPI_EULER) {
+        // euler_scheme, time_integration.f90:110-117
+        xn = x0 + vxi * dt;
+        yn = y0 + vyi * dt;
+        vxn = vx0 + ax * dt;
+        vyn = vy0 + ay * dt;
+        hn = h0 + dhdt * dt;
+        An = A0 + dAdt * dt;
+    } else if (a.mode == EPI_LEAP) {
+        // leapfrog_scheme, time_integration.f90:356-364 (vx0: the step-start
+        // velocity, vxi: the half-step one)
+        vxn = vx0 + ax * dt;
+        vyn = vy0 + ay * dt;
+        hn = h0 + dhdt * dt;
+        xn = x0 + (vx0 + vxi) * dt / 2.0;
+        yn = y0 + (vy0 + vyi) * dt / 2.0;
+        An = A0 + dAdt * dt;
     } else {
         // time_integration.f90:344-367
         const double x12 = x0 + vxi * dt / 2.0, y12 = y0 + vyi * dt / 2.0;
@@ -603,8 +651,11 @@ __device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool l
         const double ar = kPi * ((P.alpha * hs_old) * (P.alpha * hs_old));
         mn = P.rho_ice * An * hn * ar;
     }
+    // the step's last update: hsml, VP time step (after the corrector, the
+    // Euler step or the leap-frog's second half)
+    const bool final_update = a.mode == EPI_CORRECT || a.mode == EPI_EULER || a.mode == EPI_LEAP;
     double hsn = hs_old;
-    if (a.mode == EPI_CORRECT && P.sle == 2) {                // smoothing_length.f90:136-142
+    if (final_update && P.sle == 2) {                         // smoothing_length.f90:136-142
         hsn = sqrt(mn / rhon) * (double)P.hsml_multiplicity;
         if (hsn > P.max_hsml) hsn = P.max_hsml;
     }
@@ -646,10 +697,10 @@ __device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool l
         o.pf[i] = make_float4((float)xn, (float)yn, hsf, 0.0f);
         if (o.hmm) o.hmm[i] = make_float4(hsf, (float)mn, (float)morn, 0.0f);
         else o.mm[i] = make_double2(mn, morn);
-        if (a.mode == EPI_CORRECT && P.sle == 2) a.hs_next[i] = hsn;
+        if (final_update && P.sle == 2) a.hs_next[i] = hsn;
     }
     // this step's bounds, one block-wide reduction
-    const bool corr = a.mode == EPI_CORRECT;
+    const bool corr = final_update;
     unsigned active = 1u | (lists ? 2u : 0u) | 4u;
     unsigned long long v[kBounds] = {(unsigned long long)(live ? cnt : 0), dbits(dl2), dbits(xa), ~0ull, 0ull,
                                      ~0ull};

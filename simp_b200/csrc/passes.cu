@@ -199,6 +199,27 @@ __global__ void __launch_bounds__(kFinishThreads) k_step_finish(Scalars *sc, Ins
     for (int k = threadIdx.x; k < ninst; k += kFinishThreads) inst[k].t = inst[k].t + dt;
 }
 
+// The Euler step writes its result into S1 (S0 is read by the pair sums of
+// the same pass); this copies it back, with the packed copies.
+__global__ void k_copy_s1_to_s0(int n, State s1, State s0) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    s0.x[i] = s1.x[i];
+    s0.y[i] = s1.y[i];
+    s0.vx[i] = s1.vx[i];
+    s0.vy[i] = s1.vy[i];
+    s0.h[i] = s1.h[i];
+    s0.A[i] = s1.A[i];
+    s0.rho[i] = s1.rho[i];
+    s0.mor[i] = s1.mor[i];
+    if (s1.m != s0.m) s0.m[i] = s1.m[i];
+    s0.xy[i] = s1.xy[i];
+    s0.vxy[i] = s1.vxy[i];
+    s0.pf[i] = s1.pf[i];
+    if (s0.hmm) s0.hmm[i] = s1.hmm[i];
+    else s0.mm[i] = s1.mm[i];
+}
+
 __global__ void k_reset_stats(Scalars *sc) {
     sc->maxip = 0;
     sc->minip = 0x7fffffff;
@@ -272,7 +293,7 @@ void launch_stress(simp_ctx *c, const State &rhs, const State &base, EpiMode mod
     StressArgs a{};
     a.rhs = rhs;
     a.base = base;
-    a.out = (mode == EPI_PREDICT) ? c->s1 : c->s0;
+    a.out = (mode == EPI_PREDICT || mode == EPI_EULER) ? c->s1 : c->s0;
     a.cell_start = c->cell_start;
     a.inst = c->inst_dev;
     a.pinst = c->pinst;
@@ -316,6 +337,11 @@ void launch_step_finish(simp_ctx *c) {
         c->launches += 1;
     }
     k_step_finish<<<1, kFinishThreads, 0, c->stream>>>(c->sc, c->inst_dev, c->ninst, c->prm.tse, c->prm.sle);
+    c->launches += 1;
+}
+
+void launch_copy_s1_to_s0(simp_ctx *c) {
+    k_copy_s1_to_s0<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->n, c->s1, c->s0);
     c->launches += 1;
 }
 

@@ -44,6 +44,7 @@ _DBL_FIELDS = [
     "wind_u", "wind_v", "current_u", "current_v",
     "vortex_x", "vortex_y", "vortex_umax", "vortex_radius",
     "dt", "max_hsml", "skin",
+    "zeta_max", "eta_max", "phi",
 ]
 
 
@@ -154,6 +155,9 @@ def reference_default() -> SimpParams:
     p.dt = 0.0
     p.max_hsml = 0.0
     p.skin = -1.0
+    p.zeta_max = 0.0          # data_variables.f90:154, declared without a value
+    p.eta_max = 0.0
+    p.phi = 45.0              # data_variables.f90:159 (mu = tan(phi pi / 180.), :180)
     return p
 
 

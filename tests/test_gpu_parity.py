@@ -240,3 +240,47 @@ def test_trajectory_vp_timestep_and_marquis_hsml(gpu_lib, oracle_mod):
     sg, so = g.get_state(), o.get_state()
     for k in ("vx", "h", "hsml"):
         assert rel_l2(sg[k], so[k]) < TOL_TRAJ_20, k
+
+
+# --- switch variants of the path -------------------------------------------
+
+def _variant(b, **kw):
+    prm = b.params.copy()
+    for k, v in kw.items():
+        setattr(prm, k, v)
+    return prm
+
+
+VARIANTS = {
+    # (Mohr-Coulomb viscosities up to these caps make the explicit step at
+    # dt = 1 s amplify rounding differences; 1e-3 s is under the VP bound)
+    "mohr_coulomb": dict(rheology=2, zeta_max=2.5e8, eta_max=1.0e8, dt=1e-3),
+    "gutfraind_eos": dict(eos_alg=2),
+    "hibler_eos": dict(eos_alg=1),
+    "stress_2": dict(pa_sph=2),
+    "euler": dict(int_algorithm=1),
+    "leapfrog": dict(int_algorithm=3),
+}
+
+
+@pytest.mark.parametrize("name", sorted(VARIANTS))
+def test_switch_variants_against_oracle(gpu_lib, oracle_mod, name):
+    """Rheology (bulk_viscosity.f90, shear_viscosity.f90), equation of state
+    (eos.f90), stress form (internal_stress.f90) and integrator
+    (time_integration.f90) switches: one right-hand side and 10 steps."""
+    b = basins.cfg1()
+    b.vx = smooth_velocity(b.x, b.L, amp=0.3, seed=40)
+    b.h = b.h * np.linspace(0.9, 1.1, b.n)      # thickness varies: the Gutfraind pressure is live
+    b.rho = b.h * 900.0
+    prm = _variant(b, **VARIANTS[name])
+    g, o = _pair(b, oracle_mod, prm)
+    rg, ro = g.single_step(3600.0), o.single_step(3600.0)
+    for k in ("dvxdt", "dhdt", "dAdt"):
+        assert rel_l2(rg[k], ro[k]) < TOL_RHS, (k, rel_l2(rg[k], ro[k]))
+    g2, o2 = _pair(b, oracle_mod, prm)
+    g2.time_integration(10)
+    o2.step(10)
+    sg, so = g2.get_state(), o2.get_state()
+    for k in ("x", "vx", "h", "A", "rho"):
+        assert rel_l2(sg[k], so[k]) < 1e-9, (k, rel_l2(sg[k], so[k]))
+    assert sg["current_time"] == pytest.approx(so["current_time"])
