@@ -27,7 +27,8 @@ module simp_gpu_mod
                           b_length, kappa_n, kappa_t, alpha,                &
                           wind_u, wind_v, current_u, current_v,             &
                           vortex_x, vortex_y, vortex_umax, vortex_radius,   &
-                          dt, max_hsml, skin, zeta_max, eta_max, phi
+                          dt, max_hsml, skin, zeta_max, eta_max, phi,       &
+                          xi, Y, nu
     end type simp_params
 
     ! Mirror of struct simp_forcing (per-basin wind of a batch).
@@ -136,6 +137,33 @@ module simp_gpu_mod
             type(c_ptr), value :: ctx
             type(simp_forcing), intent(in) :: f
             integer(c_int32_t) :: simp_gpu_set_forcing
+        end function
+
+        ! b_normal(2, ntotalb) of the walls, for the Wang boundary force.
+        function simp_gpu_set_wall_normals(ctx, ntotalb, b_normal)         &
+                bind(C, name="simp_gpu_set_wall_normals")
+            import :: c_ptr, c_int32_t, c_double
+            type(c_ptr), value :: ctx
+            integer(c_int32_t), value :: ntotalb
+            real(c_double), intent(in) :: b_normal(*)
+            integer(c_int32_t) :: simp_gpu_set_wall_normals
+        end function
+
+        ! The reference's output files (output.f90:61-78), appended from the
+        ! device state; folder is a NUL-terminated path.
+        function simp_csv_create_output(folder)                            &
+                bind(C, name="simp_csv_create_output")
+            import :: c_int32_t, c_char
+            character(kind=c_char), intent(in) :: folder(*)
+            integer(c_int32_t) :: simp_csv_create_output
+        end function
+
+        function simp_gpu_write_output(ctx, folder)                        &
+                bind(C, name="simp_gpu_write_output")
+            import :: c_ptr, c_int32_t, c_char
+            type(c_ptr), value :: ctx
+            character(kind=c_char), intent(in) :: folder(*)
+            integer(c_int32_t) :: simp_gpu_write_output
         end function
 
         ! Batches of basins advanced together by simp_gpu_step.

@@ -1,6 +1,6 @@
 !!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!
 !   Drop-in replacement of SIMP's time_integration (integration/          !
-!   time_integration.f90:114-181) that runs the predictor-corrector on    !
+!   time_integration.f90:6-71) that runs the predictor-corrector on       !
 !   the GPU.  State goes up once, steps stay resident, and the module     !
 !   globals are refreshed only when output is due (save_step).            !
 !   Link with -lsimp_gpu; compile simp_gpu_mod.f90 first.                  !

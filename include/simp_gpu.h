@@ -81,7 +81,8 @@ typedef struct simp_params {
     int32_t int_algorithm;     /* 1 Euler, 2 predictor-corrector, 3 leap-frog
                                   (time_integration.f90:86-148, 155-282, 289-391)     */
     int32_t nnps_algorithm;    /* 2 bucket search, 1 direct find (nnps.f90:21-30)       */
-    int32_t sle;               /* 0 keep hsml, 2 Marquis hsml (smoothing_length.f90)    */
+    int32_t sle;               /* 0 keep hsml, 1 Benz hsml, 2 Marquis hsml
+                                  (smoothing_length.f90:24-30)                          */
     int32_t tse;               /* 0 keep dt, 2 VP criterion (time_step.f90:132-157)     */
     int32_t rheology;          /* 1 elliptical yield curve, 2 Mohr-Coulomb
                                   (bulk_viscosity.f90, shear_viscosity.f90)           */
@@ -89,14 +90,16 @@ typedef struct simp_params {
     int32_t pa_sph;            /* 1 (s_i/rho_i^2 + s_j/rho_j^2) stress_1,
                                   2 (s_i + s_j)/rho_j stress_2 (internal_stress.f90)  */
     int32_t skf;               /* SIMP_SKF_*                                            */
-    int32_t den_alg;           /* 3 diagnostic, 1 summation (density.f90:20-30)         */
-    int32_t bfa;               /* 1 Monaghan boundary force                             */
+    int32_t den_alg;           /* 3 diagnostic, 2 continuity (con_density) in the step;
+                                  1 summation: simp_gpu_sum_density (density.f90:20-30)  */
+    int32_t bfa;               /* boundary force (boundary_force.f90:20-27): 1 Monaghan,
+                                  2 Wang (needs simp_gpu_set_wall_normals), 3 Marquis  */
     int32_t viscosity;         /* globals.f90:180-187 logical switches (0/1)            */
     int32_t pressure_force;
     int32_t wind_force;
     int32_t water_force;
     int32_t boundary_pressure;
-    int32_t boundary_friction; /* must be 0: friction branch not on this path          */
+    int32_t boundary_friction; /* friction branch of the boundary force                */
     int32_t mass_from_area;    /* 1: mass_update_from_area when sle is 0 or 1 (as the
                                   reference); 0: particle mass held constant         */
     int32_t max_ind_int;       /* 200 (globals.f90:24)                                 */
@@ -122,6 +125,10 @@ typedef struct simp_params {
        pressure (declared without a value in the reference, so 0 there) and the
        friction angle phi (degrees; mu = tan(phi)) */
     double zeta_max, eta_max, phi;
+    /* boundary friction (data_variables.f90:157-158, 175): friction coefficient
+       xi of bf_Wang, Young modulus Y and Poisson ratio nu of the sound speed
+       c_yang used by bf_Monaghan's friction term */
+    double xi, Y, nu;
 } simp_params;
 
 /* Shipped values of globals.f90 and data_variables.f90, including the
@@ -218,6 +225,13 @@ typedef struct simp_forcing {
     double vortex_x, vortex_y, vortex_umax, vortex_radius;
 } simp_forcing;
 
+/* Unit normals of the walls of a single-basin context, b_normal(2, ntotalb)
+ * in the order of set_state's xb (data_variables.f90:46, set with the walls
+ * by boundaries.f90:232-287, pointing into the ice).  Read by the Wang
+ * boundary force (bfa = 2, boundary_force.f90:146-172), which refuses to run
+ * without them.  A new set_state clears them. */
+SIMP_API int32_t simp_gpu_set_wall_normals(simp_ctx *ctx, int32_t ntotalb, const double *b_normal);
+
 /* Forcing of a single-basin context (the wind fields of its simp_params),
  * used from the next simp_gpu_set_state on and by the basin already set.
  * The reference hard-codes its wind (wind_forcing.f90:36-37). */
@@ -303,6 +317,49 @@ SIMP_API int64_t simp_gpu_kernel_launches(const simp_ctx *ctx);
 SIMP_API int32_t simp_gpu_profile(simp_ctx *ctx, int32_t on);
 SIMP_API int32_t simp_gpu_kernel_times(simp_ctx *ctx, double *ms, int32_t n_kernels,
                                        int64_t *steps_timed);
+
+/* ---- snapshot files -------------------------------------------------------
+ * The reference's output files, in its formats (in_out/output.f90:61-78):
+ *   particle_momentum.csv  " i , x/1000 , y/1000 , 100 vx , 100 vy"  (1x,I7,4(1x,A1,1x,e15.8E3))
+ *   particle_state.csv     " i , mass , p , hsml , A , h , eps11 , eps12 , eps22 ,
+ *                           sig11 , sig12 , sig22"                   (1x,I7,11(1x,A1,1x,e15.8E3))
+ *   particle_other.csv     " ntotal , ntotalb , current_time/3600"   (1x,2(I7,1x,A1,1x),e15.8E3)
+ *   boundary_particles.csv " j , xb/1000 , yb/1000 , massb"          (1x,I5,3(1x,A1,1x,e14.8))
+ * `folder` is a directory path (with or without the trailing '/'). */
+
+/* Creates the three particle files empty (initialize.f90:83-95). */
+SIMP_API int32_t simp_csv_create_output(const char *folder);
+/* Appends one snapshot of a single-basin context, as `output` does: its
+ * state and the diagnostics of the last right-hand side that kept them
+ * (simp_gpu_single_step, or simp_gpu_step after simp_gpu_keep_diag). */
+SIMP_API int32_t simp_gpu_write_output(simp_ctx *ctx, const char *folder);
+/* The same from host arrays (x, vx interleaved as x(2, ntotal)). */
+SIMP_API int32_t simp_csv_append_snapshot(const char *folder, int32_t ntotal, int32_t ntotalb,
+                                          double current_time, const double *x, const double *vx,
+                                          const double *mass, const double *p, const double *hsml,
+                                          const double *A, const double *h, const double *eps11,
+                                          const double *eps12, const double *eps22, const double *sig11,
+                                          const double *sig12, const double *sig22);
+/* Writes boundary_particles.csv (boundaries.f90:52-63). */
+SIMP_API int32_t simp_csv_write_walls(const char *folder, int32_t ntotalb, const double *xb,
+                                      const double *massb);
+/* Spin-up reader (replaces particle_reading, initialize.f90:234-330, which
+ * reads 14 columns per state record where output writes 11, and only the
+ * first snapshot).  Reads snapshot `snapshot` (0-based; negative counts
+ * from the last, -1 = the last) in SI units (x in m, vx in m/s,
+ * current_time in s).  With every array null it only returns the sizes;
+ * more than `cap` particles is SIMP_ERR_MAXN, like the reference's STOP.
+ * rho is not in the files: with the diagnostic density it is h rho_ice. */
+SIMP_API int32_t simp_csv_read_snapshot(const char *folder, int32_t snapshot, int32_t cap,
+                                        int32_t *ntotal, int32_t *ntotalb, double *current_time,
+                                        double *x, double *vx, double *mass, double *p, double *hsml,
+                                        double *A, double *h);
+/* Reads boundary_particles.csv (boundary_reading, boundaries.f90:119-160;
+ * all walls converted to m, where the reference converts the first ntotal). */
+SIMP_API int32_t simp_csv_read_walls(const char *folder, int32_t cap, int32_t *ntotalb, double *xb,
+                                     double *massb);
+/* Text of the last error of the simp_csv_* calls on this thread. */
+SIMP_API const char *simp_csv_last_error(void);
 
 /* Human-readable text of the last error on this context ("" if none). */
 SIMP_API const char *simp_gpu_last_error(const simp_ctx *ctx);

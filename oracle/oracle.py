@@ -50,6 +50,9 @@ def lib():
         L.orc_kernel.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp, _dp, _dp, _dp]
         L.orc_boundary_w.restype = ctypes.c_double
         L.orc_boundary_w.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.orc_boundary_fdwdq.restype = ctypes.c_double
+        L.orc_boundary_fdwdq.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.orc_set_wall_normals.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
         L.orc_interaction_stats.argtypes = [ctypes.c_void_p, _ip, _ip, ctypes.POINTER(ctypes.c_longlong), _ip]
         L.orc_set_threads.argtypes = [ctypes.c_int]
         L.orc_max_threads.restype = ctypes.c_int
@@ -108,7 +111,14 @@ class Oracle:
         prm = b.params if params is None else params
         o = cls(prm, b.n, max(b.nb, 1))
         o.set_state(b.x, b.vx, b.mass, b.rho, b.hsml, b.A, b.h, b.xb, b.massb, prm.dt, 0.0)
+        if prm.bfa == 2 and b.nb > 0 and getattr(b, "bn", None) is not None:
+            o.set_wall_normals(b.bn)
         return o
+
+    def set_wall_normals(self, b_normal):
+        bn = np.ascontiguousarray(b_normal, np.float64).reshape(-1, 2)
+        self._keep_bn = bn
+        self._chk(lib().orc_set_wall_normals(self.h, bn.shape[0], _p(bn)))
 
     def set_state(self, x, vx, mass, rho, hsml, A, h, xb, massb, dt, t):
         arrs = [np.ascontiguousarray(a, np.float64) for a in (x, vx, mass, rho, hsml, A, h, xb, massb)]
@@ -191,3 +201,8 @@ def kernel(params, r, hij, dx, dy):
 
 def boundary_w(params, br):
     return float(lib().orc_boundary_w(ctypes.byref(params), float(br)))
+
+
+def boundary_fdwdq(params, br):
+    """factor * dW/dq of the boundary kernel (bdwdx = -that / b_length * (bdx / br) * scale_h)."""
+    return float(lib().orc_boundary_fdwdq(ctypes.byref(params), float(br)))

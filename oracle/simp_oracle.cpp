@@ -52,7 +52,7 @@ struct Orc {
     double dt = 0.0, current_time = 0.0, max_hsml = 0.0;
     // data_variables.f90:26-124, column-major x(2, n) stored interleaved
     std::vector<double> x, vx, mass, rho, p, hsml, A, h, c;
-    std::vector<double> xb, massb;
+    std::vector<double> xb, massb, b_normal;
     std::vector<double> dvxdt, dxdt, dAdt, dhdt, drhodt;
     std::vector<double> kernel_zero;
     std::vector<double> eps11, eps12, eps22, zeta, eta, sig11, sig12, sig22;
@@ -264,6 +264,47 @@ double boundary_w(const Orc &o, double br, int int_id) {
             if (q >= 0.0 && q <= 1.0) bw = factor * (c23 - p2(q) + 0.5 * p3(q));
             if (q > 1.0 && q <= 2.0) bw = factor * (c16 * p3(2.0 - q));
             return bw;
+        }
+    }
+}
+
+// factor * dW/dq of the boundary kernels, from which boundary_kernel.f90
+// forms bdwdx = -factor * (dW/dq) / b_length * (bdx / br) * scale_h
+// (b_Quadratic :111-112, b_Gaussian :182-184, b_quintic_spline :257-274,
+// b_Wendland_C2 :348-349, b_Wendland_C4 :422-423, b_Wendland_C6 :495-496;
+// the restored cubic: its kernel's derivative).
+double boundary_fdwdq(const Orc &o, double br, int int_id) {
+    const double sh = (double)o.scale_h;
+    const double bl = o.P.b_length;
+    const double q = br / bl * sh;
+    switch (o.P.skf) {
+        case 1:
+            return 2.0 / PI * p2(sh / bl) * (3.0 / 8.0 * q - 3.0 / 4.0);
+        case 2: case 7: case 8:
+            return 1.0 / PI * p2(sh / bl) * (-2 * q * std::exp(-p2(q)));
+        case 3: {
+            const double factor = 15.0 / (478.0 * PI) * p2(sh / bl);
+            double d = 0.0;
+            if (q >= 0.0 && q <= 1.0) d = factor * (-5 * ipow(3 - q, 4) + 30 * ipow(2 - q, 4) - 75 * ipow(1 - q, 4));
+            if (q > 1.0 && q <= 2.0) d = factor * (-5 * ipow(3 - q, 4) + 30 * ipow(2 - q, 4));
+            if (q > 2.0 && q <= 3.0) d = factor * (-5 * ipow(3 - q, 4));
+            return d;
+        }
+        case 4:
+            return 3.0 / (2.0 * PI) * p2(sh / bl) * (20.0 * (ipow(q, 4) - 3 * p3(q) + 3 * p2(q) - q));
+        case 5:
+            return 3.0 / PI * p2(sh / bl) * (-56 * q * (5 * q + 1) * ipow(1 - q, 5));
+        case 6: {
+            const double hij = (int_id - 1 < (int)o.hsml_ij.size()) ? o.hsml_ij[int_id - 1] : 0.0;
+            const double factor = 78.0 / (7.0 * PI) * p2(sh / hij);
+            return factor * (-22.0 * q * p7(1 - q) * (16 * p2(q) + 7.0 * q + 1));
+        }
+        default: {
+            const double factor = 15.0 / (7.0 * PI) * p2(sh / bl);
+            double d = 0.0;
+            if (q >= 0.0 && q <= 1.0) d = factor * (1.5 * p2(q) - 2.0 * q);
+            if (q > 1.0 && q <= 2.0) d = factor * (-0.5 * p2(2.0 - q));
+            return d;
         }
     }
 }
@@ -535,20 +576,54 @@ void internal_stress(Orc &o) {
 // boundary_kernel.f90:477-502 + boundary_force.f90:74-84 (bf_Monaghan,
 // normal force).  The reference updates dvxdt from a called routine inside a
 // reduction region (a race with several threads); this loop is serial.
+// boundary_kernel.f90:5-45 (one loop per kernel, the same for all) with
+// boundary_force.f90 called per boundary pair: bfa 1 bf_Monaghan :38-102,
+// 2 bf_Wang :109-176, 3 bf_Marquis :183-225.
 void boundary_kernel(Orc &o) {
     const simp_params &P = o.P;
+    const double sh = (double)o.scale_h;
     for (int k = 0; k < o.bnip; ++k) {
         const int ci = o.bp_j[k] - 1;  // particle
         const int cj = o.bp_i[k] - 1;  // boundary particle
         const double bdx[2] = {o.xb[2 * cj] - o.x[2 * ci], o.xb[2 * cj + 1] - o.x[2 * ci + 1]};
         const double br = o.br_ij[k];
         const double bw = boundary_w(o, br, k + 1);
-        if (P.boundary_pressure) {
-            for (int d = 0; d < 2; ++d) {
-                const double Fb = P.kappa_n * bdx[d] * bw * 2.0 * o.massb[cj] /
-                                  ((o.mass[ci] + o.massb[cj]) * p2(br));
-                o.dvxdt[2 * ci + d] = o.dvxdt[2 * ci + d] + (-1.0 * Fb) / o.rho[ci];
+        const double fd = boundary_fdwdq(o, br, k + 1);
+        const double bdwdx[2] = {-fd / P.b_length * (bdx[0] / br) * sh, -fd / P.b_length * (bdx[1] / br) * sh};
+        const double *v = &o.vx[2 * ci];
+        if (P.bfa == 1) {
+            if (P.boundary_pressure) {
+                for (int d = 0; d < 2; ++d) {
+                    const double Fb = P.kappa_n * bdx[d] * bw * 2.0 * o.massb[cj] /
+                                      ((o.mass[ci] + o.massb[cj]) * p2(br));
+                    o.dvxdt[2 * ci + d] = o.dvxdt[2 * ci + d] + (-1.0 * Fb) / o.rho[ci];
+                }
             }
+            if (P.boundary_friction) {                                    // :85-100
+                const double v_r = v[0] * bdx[0] + v[1] * bdx[1];
+                const double pi_aj = P.kappa_t * o.c[ci] * v_r / br / o.rho[ci];
+                for (int d = 0; d < 2; ++d)
+                    o.dvxdt[2 * ci + d] = o.dvxdt[2 * ci + d] + (-1.0 * o.massb[cj] * pi_aj * bdwdx[d]) / o.rho[ci];
+            }
+        } else if (P.bfa == 2) {
+            if (P.boundary_pressure) {                                    // :146-172
+                const double *bn = &o.b_normal[2 * cj];
+                double vv[2];
+                vv[0] = bn[0] * v[0] + bn[1] * v[1];
+                vv[1] = std::sqrt(p2(v[0]) + p2(v[1])) - vv[0];
+                double F[2] = {o.mass[ci] * vv[0] / o.dt, o.mass[ci] * vv[1] / o.dt};
+                if (P.boundary_friction && std::fabs(vv[1]) > std::fabs(P.xi * vv[0])) {
+                    vv[1] = vv[1] * P.xi * std::fabs(F[0] / F[1]);
+                    F[1] = o.mass[ci] * vv[1] / o.dt;
+                }
+                o.dvxdt[2 * ci] = o.dvxdt[2 * ci] + (F[0] * bn[0] + F[1] * bn[1]);
+                o.dvxdt[2 * ci + 1] = o.dvxdt[2 * ci + 1] + (F[0] * bn[1] - F[1] * bn[0]);
+            }
+        } else if (P.bfa == 3) {
+            if (P.boundary_pressure) continue;                            // :208-210
+            if (P.boundary_friction)                                      // :213-216
+                for (int d = 0; d < 2; ++d)
+                    o.dvxdt[2 * ci + d] = o.dvxdt[2 * ci + d] - v[d] * (1 - (br / P.b_length));
         }
     }
 }
@@ -672,14 +747,38 @@ void sum_density(Orc &o, int k0_mode, double *out) {
     for (int i = 0; i < n; ++i) out[i] = num[i] / den[i];
 }
 
+// density.f90:107-165 (con_density): drhodt over the last NNPS's pairs and
+// kernel gradients with the current velocities.
+void con_density(Orc &o) {
+    std::fill(o.drhodt.begin(), o.drhodt.begin() + o.ntotal, 0.0);
+    for (int k = 0; k < o.nip; ++k) {
+        const int i = o.p_i[k] - 1, j = o.p_j[k] - 1;
+        const double dvx[2] = {o.vx[2 * i] - o.vx[2 * j], o.vx[2 * i + 1] - o.vx[2 * j + 1]};
+        const double w1 = dvx[0] * o.dwdx[2 * k], w4 = dvx[1] * o.dwdx[2 * k + 1];
+        const double v_ij = w1 + w4;
+        o.drhodt[i] = o.drhodt[i] + o.mass[j] * v_ij;
+        o.drhodt[j] = o.drhodt[j] + o.mass[i] * v_ij;
+    }
+}
+
 void density(Orc &o) {
-    if (o.P.den_alg == 1) {
+    if (o.P.den_alg == 2) {
+        con_density(o);
+    } else if (o.P.den_alg == 1) {
         std::vector<double> r(o.ntotal);
         sum_density(o, 0, r.data());
         std::copy(r.begin(), r.end(), o.rho.begin());
     } else if (o.P.den_alg == 3) {
         for (int i = 0; i < o.ntotal; ++i) o.rho[i] = o.h[i] * o.P.rho_ice;   // :192
     }
+}
+
+// sound_speed.f90:20-27 with c_yang :54-55: only when something reads c.
+void sound_speed(Orc &o) {
+    const simp_params &P = o.P;
+    if (!P.boundary_friction) return;   // (artificial_visc is off; tse = 1 is not a path here)
+    for (int i = 0; i < o.ntotal; ++i)
+        o.c[i] = std::pow(P.Y * (1 - P.nu) / (o.rho[i] * (1 + P.nu) * (1 - 2 * P.nu)), 0.5);
 }
 
 // mass_evolution.f90:20-71.
@@ -691,8 +790,30 @@ void mass_evolution(Orc &o) {
     }
 }
 
+// smoothing_length.f90:40-111 (Benz_hsml).  Without con_density the pair
+// loop adds to drhodt, which nothing clears: it accumulates over the steps.
+void benz_hsml(Orc &o) {
+    const int n = o.ntotal;
+    if (o.P.den_alg != 2) {
+        for (int k = 0; k < o.nip; ++k) {
+            const int i = o.p_i[k] - 1, j = o.p_j[k] - 1;
+            const double dvx[2] = {o.vx[2 * i] - o.vx[2 * j], o.vx[2 * i + 1] - o.vx[2 * j + 1]};
+            const double w1 = dvx[0] * o.dwdx[2 * k], w4 = dvx[1] * o.dwdx[2 * k + 1];
+            const double v_ij = w1 + w4;
+            o.drhodt[i] = o.drhodt[i] + o.mass[j] * v_ij;
+            o.drhodt[j] = o.drhodt[j] + o.mass[i] * v_ij;
+        }
+    }
+    for (int i = 0; i < n; ++i) {
+        const double dhsmldt = -o.hsml[i] * o.drhodt[i] / 2.0 / o.rho[i];   // dim = 2
+        o.hsml[i] = o.hsml[i] + dhsmldt * o.dt;
+        if (o.hsml[i] < 0.0) o.hsml[i] = o.hsml[i] - dhsmldt * o.dt;
+    }
+}
+
 // smoothing_length.f90:118-145 (Marquis_hsml); sle = 0 keeps hsml.
 void smoothing_length(Orc &o) {
+    if (o.P.sle == 1) { benz_hsml(o); return; }
     if (o.P.sle != 2) return;
     for (int i = 0; i < o.ntotal; ++i) {
         o.hsml[i] = std::sqrt(o.mass[i] / o.rho[i]) * (double)o.P.hsml_multiplicity;
@@ -715,14 +836,14 @@ void clamp_A(Orc &o) {
     for (int i = 0; i < o.ntotal; ++i) if (o.A[i] > 1.0) o.A[i] = 1.0;
 }
 
-// time_integration.f90:263-390 (predictor_corrector).
+// time_integration.f90:155-282 (predictor_corrector).
 void predictor_corrector(Orc &o) {
     const int n = o.ntotal;
     const double dt = o.dt;
     std::vector<double> x1(o.x.begin(), o.x.begin() + 2 * n), vx1(o.vx.begin(), o.vx.begin() + 2 * n);
     std::vector<double> h1(o.h.begin(), o.h.begin() + n), A1(o.A.begin(), o.A.begin() + n);
     std::vector<double> rho1(o.rho.begin(), o.rho.begin() + n);
-    single_step(o);                                                  // :312
+    single_step(o);                                                  // :204
     for (int k = 0; k < 2 * n; ++k) {
         o.x[k] = o.x[k] + o.dxdt[k] * dt / 2.0;
         o.vx[k] = o.vx[k] + o.dvxdt[k] * dt / 2.0;
@@ -733,9 +854,12 @@ void predictor_corrector(Orc &o) {
     }
     clamp_A(o);
     density(o);
+    if (o.P.den_alg == 2)                                            // :220-223
+        for (int i = 0; i < n; ++i) o.rho[i] = o.rho[i] + o.drhodt[i] * dt / 2.0;
     mass_evolution(o);
-    single_step(o);                                                  // :341
-    std::vector<double> x12(2 * n), vx12(2 * n), h12(n), A12(n);
+    sound_speed(o);
+    single_step(o);                                                  // :233
+    std::vector<double> x12(2 * n), vx12(2 * n), h12(n), A12(n), rho12(n);
     for (int k = 0; k < 2 * n; ++k) {
         x12[k] = x1[k] + o.dxdt[k] * dt / 2.0;
         vx12[k] = vx1[k] + o.dvxdt[k] * dt / 2.0;
@@ -744,7 +868,9 @@ void predictor_corrector(Orc &o) {
         h12[i] = h1[i] + o.dhdt[i] * dt / 2.0;
         A12[i] = A1[i] + o.dAdt[i] * dt / 2.0;
     }
-    density(o);                                                      // :350
+    density(o);                                                      // :242
+    if (o.P.den_alg == 2)                                            // :245-247
+        for (int i = 0; i < n; ++i) rho12[i] = rho1[i] + o.drhodt[i] * dt / 2.0;
     for (int k = 0; k < 2 * n; ++k) {
         o.x[k] = 2.0 * x12[k] - x1[k];
         o.vx[k] = 2.0 * vx12[k] - vx1[k];
@@ -755,7 +881,10 @@ void predictor_corrector(Orc &o) {
     }
     clamp_A(o);
     density(o);
+    if (o.P.den_alg == 2)                                            // :265-267
+        for (int i = 0; i < n; ++i) o.rho[i] = 2.0 * rho12[i] - rho1[i];
     mass_evolution(o);
+    sound_speed(o);
     smoothing_length(o);
     time_step(o);
 }
@@ -775,7 +904,10 @@ void euler_scheme(Orc &o) {
     }
     clamp_A(o);
     density(o);
+    if (o.P.den_alg == 2)                                            // :131-133
+        for (int i = 0; i < n; ++i) o.rho[i] = o.rho[i] + o.drhodt[i] * dt;
     mass_evolution(o);
+    sound_speed(o);
     smoothing_length(o);
     time_step(o);
 }
@@ -786,7 +918,8 @@ void leapfrog_scheme(Orc &o) {
     const double dt = o.dt;
     std::vector<double> x1(o.x.begin(), o.x.begin() + 2 * n), vx1(o.vx.begin(), o.vx.begin() + 2 * n);
     std::vector<double> h1(o.h.begin(), o.h.begin() + n), A1(o.A.begin(), o.A.begin() + n);
-    single_step(o);                                                  // :321
+    std::vector<double> rho1(o.rho.begin(), o.rho.begin() + n);
+    single_step(o);                                                  // :330
     for (int k = 0; k < 2 * n; ++k) {
         o.x[k] = o.x[k] + o.dxdt[k] * dt / 2;
         o.vx[k] = o.vx[k] + o.dvxdt[k] * dt / 2;
@@ -797,8 +930,11 @@ void leapfrog_scheme(Orc &o) {
     }
     clamp_A(o);
     density(o);
+    if (o.P.den_alg == 2)                                            // :347-349
+        for (int i = 0; i < n; ++i) o.rho[i] = o.rho[i] + o.drhodt[i] * dt / 2;
     mass_evolution(o);
-    single_step(o);                                                  // :351
+    sound_speed(o);
+    single_step(o);                                                  // :358
     for (int k = 0; k < 2 * n; ++k) {
         o.vx[k] = vx1[k] + o.dvxdt[k] * dt;
         o.x[k] = x1[k] + (vx1[k] + o.dxdt[k]) * dt / 2;
@@ -809,12 +945,20 @@ void leapfrog_scheme(Orc &o) {
     }
     clamp_A(o);
     density(o);
+    if (o.P.den_alg == 2)                                            // :375-377
+        for (int i = 0; i < n; ++i) o.rho[i] = rho1[i] + o.drhodt[i] * dt;
     mass_evolution(o);
+    sound_speed(o);
     smoothing_length(o);
     time_step(o);
 }
 
 int fail(Orc *o, int code, const char *msg) { o->err = msg; return code; }
+
+bool normals_ok(const Orc &o) {
+    return !(o.P.bfa == 2 && o.P.boundary_pressure && o.ntotalb > 0 &&
+             o.b_normal.size() != 2 * (size_t)o.ntotalb);
+}
 
 }  // namespace
 
@@ -863,6 +1007,7 @@ int orc_set_state(void *hh, int n, const double *x, const double *vx, const doub
     o->dvxdt.assign(2 * (size_t)n, 0.0); o->dxdt.assign(2 * (size_t)n, 0.0);
     o->dAdt.assign(n, 0.0); o->dhdt.assign(n, 0.0); o->drhodt.assign(n, 0.0);
     o->kernel_zero.assign(n, 0.0);
+    o->b_normal.clear();
     for (auto *v : {&o->eps11, &o->eps12, &o->eps22, &o->zeta, &o->eta, &o->sig11, &o->sig12, &o->sig22})
         v->assign(n, 0.0);
     o->dt = dt; o->current_time = t;
@@ -870,8 +1015,19 @@ int orc_set_state(void *hh, int n, const double *x, const double *vx, const doub
     for (int i = 0; i < n; ++i) mh = std::max(mh, hsml[i]);
     o->max_hsml = (o->P.max_hsml > 0.0) ? o->P.max_hsml : mh * 10.0;  // initialize.f90:191
     o->nip = o->bnip = 0;
+    sound_speed(*o);                                                   // initialize.f90:200
     return 0;
 }
+
+// b_normal(2, nb) of the walls (boundaries.f90:232-287), read by bf_Wang.
+int orc_set_wall_normals(void *hh, int nb, const double *bn) {
+    Orc *o = (Orc *)hh;
+    if (nb != o->ntotalb) return fail(o, SIMP_ERR_BADARG, "set_wall_normals: ntotalb differs from the state's walls");
+    o->b_normal.assign(bn, bn + 2 * (size_t)nb);
+    return 0;
+}
+
+
 
 int orc_get_state(void *hh, double *x, double *vx, double *mass, double *rho, double *hsml,
                   double *A, double *h, double *dt, double *t) {
@@ -928,6 +1084,7 @@ int orc_interaction_stats(void *hh, int *maxip, int *minip, long long *sumip, in
 
 int orc_single_step(void *hh, double t, double *dxdt, double *dvxdt, double *dhdt, double *dAdt) {
     Orc *o = (Orc *)hh;
+    if (!normals_ok(*o)) return fail(o, SIMP_ERR_STATE, "bfa = 2 needs the wall normals");
     o->current_time = t;
     single_step(*o);
     const int n = o->ntotal;
@@ -961,11 +1118,12 @@ int orc_sum_density(void *hh, int k0_mode, double *rho_out) {
     return 0;
 }
 
-// time_integration.f90:146-181 for nsteps iterations.
+// time_integration.f90:38-71 for nsteps iterations.
 int orc_step(void *hh, int nsteps, double *t, double *dt) {
     Orc *o = (Orc *)hh;
+    if (!normals_ok(*o)) return fail(o, SIMP_ERR_STATE, "bfa = 2 needs the wall normals");
     for (int s = 0; s < nsteps && !o->bad; ++s) {
-        if (o->P.int_algorithm == 1) euler_scheme(*o);              // time_integration.f90:46-53
+        if (o->P.int_algorithm == 1) euler_scheme(*o);              // time_integration.f90:47-55
         else if (o->P.int_algorithm == 3) leapfrog_scheme(*o);
         else predictor_corrector(*o);
         o->itimestep += 1;
@@ -995,6 +1153,14 @@ double orc_boundary_w(const simp_params *P, double br) {
     Orc o; o.P = *P; o.scale_h = scale_h_of(P->skf);
     o.hsml_ij.assign(1, P->b_length);
     return boundary_w(o, br, 1);
+}
+
+// factor * dW/dq of the boundary kernel at distance br (hsml_ij = b_length
+// for the Wendland C6 factor, as orc_boundary_w).
+double orc_boundary_fdwdq(const simp_params *P, double br) {
+    Orc o; o.P = *P; o.scale_h = scale_h_of(P->skf);
+    o.hsml_ij.assign(1, P->b_length);
+    return boundary_fdwdq(o, br, 1);
 }
 
 }  // extern "C"

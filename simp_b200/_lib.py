@@ -28,6 +28,7 @@ SIGNATURES = {
                                   _i32, _dp, _dp, _ip]),
     "simp_gpu_batch_remove": (_i32, [_vp, _i32]),
     "simp_gpu_set_forcing": (_i32, [_vp, ctypes.POINTER(SimpForcing)]),
+    "simp_gpu_set_wall_normals": (_i32, [_vp, _i32, _dp]),
     "simp_gpu_batch_get_state": (_i32, [_vp, _i32, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
     "simp_gpu_batch_info": (_i32, [_vp, _i32, _ip, ctypes.POINTER(ctypes.c_int64), _ip]),
     "simp_gpu_set_state": (_i32, [_vp, _i32, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _i32, _dp, _dp,
@@ -50,6 +51,14 @@ SIGNATURES = {
     "simp_gpu_kernel_times": (_i32, [_vp, _dp, _i32, ctypes.POINTER(ctypes.c_int64)]),
     "simp_gpu_last_error": (ctypes.c_char_p, [_vp]),
     "simp_gpu_version": (ctypes.c_char_p, []),
+    # snapshot files (host code; no device needed except for simp_gpu_write_output)
+    "simp_csv_create_output": (_i32, [ctypes.c_char_p]),
+    "simp_gpu_write_output": (_i32, [_vp, ctypes.c_char_p]),
+    "simp_csv_append_snapshot": (_i32, [ctypes.c_char_p, _i32, _i32, ctypes.c_double] + [_dp] * 13),
+    "simp_csv_write_walls": (_i32, [ctypes.c_char_p, _i32, _dp, _dp]),
+    "simp_csv_read_snapshot": (_i32, [ctypes.c_char_p, _i32, _i32, _ip, _ip, _dp] + [_dp] * 7),
+    "simp_csv_read_walls": (_i32, [ctypes.c_char_p, _i32, _ip, _dp, _dp]),
+    "simp_csv_last_error": (ctypes.c_char_p, []),
     # include/simp_serve.h
     "simp_server_create": (_i32, [ctypes.POINTER(SimpParams), ctypes.POINTER(ServerConfig), ctypes.POINTER(_vp)]),
     "simp_server_destroy": (_i32, [_vp]),

@@ -48,6 +48,7 @@ class Basin:
     params: SimpParams
     steps: int = 0
     meta: dict = field(default_factory=dict)
+    bn: np.ndarray | None = None   # wall normals b_normal(2, nb), into the ice
 
     @property
     def n(self) -> int:
@@ -80,20 +81,24 @@ def _wall_line(p0, p1, spacing):
 
 
 def _walls(L: float, dx: float, b_length: float, sides: str):
+    """Wall particles of the requested sides and their unit normals, which
+    point into the ice as the reference's b_normal does
+    (boundaries.f90:232-287)."""
     s = b_length / 3.0
     lo, hi = -0.5 * dx, L + 0.5 * dx
-    segs = []
-    if "+x" in sides:
-        segs.append(_wall_line((hi, lo), (hi, hi), s))
-    if "-x" in sides:
-        segs.append(_wall_line((lo, lo), (lo, hi), s))
-    if "+y" in sides:
-        segs.append(_wall_line((lo, hi), (hi, hi), s))
-    if "-y" in sides:
-        segs.append(_wall_line((lo, lo), (hi, lo), s))
+    segs, normals = [], []
+    for side, p0, p1, nrm in (("+x", (hi, lo), (hi, hi), (-1.0, 0.0)),
+                              ("-x", (lo, lo), (lo, hi), (1.0, 0.0)),
+                              ("+y", (lo, hi), (hi, hi), (0.0, -1.0)),
+                              ("-y", (lo, lo), (hi, lo), (0.0, 1.0))):
+        if side in sides:
+            w = _wall_line(p0, p1, s)
+            segs.append(w)
+            normals.append(np.tile(nrm, (w.shape[0], 1)))
     if not segs:
-        return np.zeros((0, 2))
-    return np.ascontiguousarray(np.concatenate(segs, axis=0))
+        return np.zeros((0, 2)), np.zeros((0, 2))
+    return (np.ascontiguousarray(np.concatenate(segs, axis=0)),
+            np.ascontiguousarray(np.concatenate(normals, axis=0)))
 
 
 def make_basin(nside: int, dx: float, seed: int, *, name: str = "basin",
@@ -111,10 +116,10 @@ def make_basin(nside: int, dx: float, seed: int, *, name: str = "basin",
     mass = rho * dx * dx
     hsml = np.full(n, 2.4 * dx)
     prm = basin_params(dx, skf=skf, dt=dt, wind=wind, precision=precision, vortex=vortex)
-    xb = _walls(L, dx, prm.b_length, walls)
+    xb, bn = _walls(L, dx, prm.b_length, walls)
     massb = np.full(xb.shape[0], mass.sum() / n)
     return Basin(name=name, dx=dx, L=L, x=x, vx=np.zeros((n, 2)), mass=mass,
-                 rho=rho, hsml=hsml, A=AA, h=hh, xb=xb, massb=massb,
+                 rho=rho, hsml=hsml, A=AA, h=hh, xb=xb, massb=massb, bn=bn,
                  params=prm, steps=steps, meta={"seed": seed, "nside": nside})
 
 

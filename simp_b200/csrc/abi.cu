@@ -144,6 +144,12 @@ Phys make_phys(const simp_params &p, double max_hsml) {
     P.zeta_max = p.zeta_max;
     P.eta_max = p.eta_max;
     P.mu = tan(p.phi * kPi / 180.0);   // data_variables.f90:180
+    P.bfa = p.bfa;
+    P.boundary_friction = p.boundary_friction;
+    P.kappa_t = p.kappa_t;
+    P.xi = p.xi;
+    P.Y = p.Y;
+    P.nu = p.nu;
     return P;
 }
 
@@ -151,18 +157,19 @@ int check_params(simp_ctx *c, const simp_params &p, bool batch) {
     auto bad = [&](const char *what) { return simp_fail(c, SIMP_ERR_BADARG, std::string("unsupported switch: ") + what); };
     if (p.int_algorithm < 1 || p.int_algorithm > 3) return bad("int_algorithm (1 Euler, 2 predictor-corrector, 3 leap-frog)");
     if (p.nnps_algorithm != 1 && p.nnps_algorithm != 2) return bad("nnps_algorithm (1 or 2)");
-    if (p.sle != 0 && p.sle != 2) return bad("sle (0 or 2)");
+    if (p.sle < 0 || p.sle > 2) return bad("sle (0, 1 or 2)");
     if (p.tse != 0 && p.tse != 2) return bad("tse (0 or 2)");
     if (p.rheology != 1 && p.rheology != 2) return bad("rheology (1 elliptical, 2 Mohr-Coulomb)");
     if (p.eos_alg < 1 || p.eos_alg > 3) return bad("eos_alg (1, 2 or 3)");
     if (p.pa_sph != 1 && p.pa_sph != 2) return bad("pa_sph (1 or 2)");
     if (!skf_known(p.skf)) return bad("skf (1 to 9)");
-    if (p.den_alg != 3) return bad("den_alg (3 in the step; the summation density is simp_gpu_sum_density)");
-    if (p.bfa != 1) return bad("bfa (only 1, Monaghan)");
-    if (p.boundary_friction) return bad("boundary_friction");
+    if (p.den_alg != 2 && p.den_alg != 3)
+        return bad("den_alg (2 or 3 in the step; the summation density is simp_gpu_sum_density)");
+    if (p.bfa < 1 || p.bfa > 3) return bad("bfa (1 Monaghan, 2 Wang, 3 Marquis)");
+    if (p.bfa == 2 && batch) return bad("bfa = 2 (wall normals) in a batch");
     if (p.precision != SIMP_PREC_FP64 && p.precision != SIMP_PREC_MIXED) return bad("precision (0 FP64, 1 mixed)");
     if (!(p.e > 0.0) || !(p.rho_ice > 0.0) || !(p.b_length > 0.0)) return bad("material constants");
-    if (batch && (p.tse != 0 || p.sle == 2)) return bad("batches need a fixed dt (tse = 0) and fixed hsml (sle = 0)");
+    if (batch && (p.tse != 0 || p.sle != 0)) return bad("batches need a fixed dt (tse = 0) and fixed hsml (sle = 0)");
     return SIMP_OK;
 }
 
@@ -178,14 +185,14 @@ void free_all(simp_ctx *c) {
     void *ptrs[] = {c->s0.x, c->s0.y, c->s0.vx, c->s0.vy, c->s0.m, c->s0.rho, c->s0.mor, c->s0.h,
                     c->s0.A, c->s0.hs, c->s1.x, c->s1.y, c->s1.vx, c->s1.vy, c->s1.rho, c->s1.mor,
                     c->s1.h, c->s1.A, c->mass1, c->xr, c->yr, c->xl, c->yl, c->cell, c->id, c->pinst,
-                    c->tau11, c->tau12, c->tau22, c->div, c->diag, c->rates, c->bx, c->by, c->bm,
+                    c->tau11, c->tau12, c->tau22, c->div, c->diag, c->rates, c->bx, c->by, c->bm, c->bnx, c->bny,
                     c->bid, c->binst, c->bcell, c->bcell_start, c->cell_start, c->cnt, c->perm, c->tmp,
                     c->itmp, c->scan_tmp, c->sc, c->pair_cnt, c->bpair_cnt, c->pair_buf_i,
                     c->pair_buf_j, c->pair_buf_r, c->pair_buf_h, c->nbr, c->nbr_count,
                     c->pair_j, c->pair_count, c->nbr_tmp, c->s0.hsf,
                     c->inst_dev, c->row_map, c->chunk_cnt, c->chunk_off, c->chunks, c->s0.xy, c->s0.vxy,
                     c->s0.pf, c->s0.mm, c->s0.hmm, c->s1.xy, c->s1.vxy, c->s1.pf, c->s1.mm, c->s1.hmm,
-                    c->tau_a, c->tau_b, c->tau_q, c->pair_dw};
+                    c->tau_a, c->tau_b, c->tau_q, c->pair_dw, c->drhodt};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->sc_host) cudaFreeHost(c->sc_host);
@@ -197,10 +204,11 @@ void free_all(simp_ctx *c) {
     if (c->stream) cudaStreamDestroy(c->stream);
 }
 
-void invalidate_graph(simp_ctx *c) {
-    if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
-    c->step_graph = nullptr;
-}
+// The step graph captured kernel arguments that changed (sizes, grid,
+// physics): the next step re-captures it and updates the instantiated graph
+// in place when the kernels are the same ones (a new state of the same
+// basin), else instantiates it anew.
+void invalidate_graph(simp_ctx *c) { c->graph_stale = true; }
 
 // Verlet-list skin: the parameter when given, else 10% of max(hsml).
 double list_skin(const simp_ctx *c, double hmax) {
@@ -307,7 +315,7 @@ int layout(simp_ctx *c) {
     for (int q = 0; q < c->max_inst; ++q) table[q] = c->insts[q].active ? c->insts[q].I : Inst{};
     SIMP_CUDA(c, cudaMemcpyAsync(c->inst_dev, table.data(), sizeof(Inst) * c->max_inst, cudaMemcpyHostToDevice, s));
     // walls of every active instance, sorted by cell key (stable)
-    struct W { int key, slot, local; double x, y, m; };
+    struct W { int key, slot, local; double x, y, m, nx, ny; };
     std::vector<W> ws;
     for (int q = 0; q < c->max_inst; ++q) {
         const InstHost &h = c->insts[q];
@@ -317,17 +325,21 @@ int layout(simp_ctx *c) {
             const double xb = h.xb[2 * b], yb = h.xb[2 * b + 1];
             const int cx = clampi((int)std::floor((xb - I.x0) * I.inv_cs), 0, I.ncx - 1);
             const int cy = clampi((int)std::floor((yb - I.y0) * I.inv_cs), 0, I.ncy - 1);
-            ws.push_back({I.base + cy * I.ncx + cx, q, b, xb, yb, h.massb[b]});
+            const bool hn = h.bn.size() == 2 * (size_t)h.nb;
+            ws.push_back({I.base + cy * I.ncx + cx, q, b, xb, yb, h.massb[b], hn ? h.bn[2 * b] : 0.0,
+                          hn ? h.bn[2 * b + 1] : 0.0});
         }
     }
     std::stable_sort(ws.begin(), ws.end(), [](const W &a, const W &b) { return a.key < b.key; });
     const int nb = (int)ws.size();
-    std::vector<double> hx(nb), hy(nb), hm(nb);
+    std::vector<double> hx(nb), hy(nb), hm(nb), hnx(nb), hny(nb);
     std::vector<int> hid(nb), hinst(nb), hcell(nb), start((size_t)base + 1, 0);
     for (int k = 0; k < nb; ++k) {
         hx[k] = ws[k].x;
         hy[k] = ws[k].y;
         hm[k] = ws[k].m;
+        hnx[k] = ws[k].nx;
+        hny[k] = ws[k].ny;
         hid[k] = ws[k].local;
         hinst[k] = ws[k].slot;
         hcell[k] = ws[k].key;
@@ -338,6 +350,10 @@ int layout(simp_ctx *c) {
         SIMP_CUDA(c, cudaMemcpyAsync(c->bx, hx.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, s));
         SIMP_CUDA(c, cudaMemcpyAsync(c->by, hy.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, s));
         SIMP_CUDA(c, cudaMemcpyAsync(c->bm, hm.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, s));
+        if (c->bnx) {
+            SIMP_CUDA(c, cudaMemcpyAsync(c->bnx, hnx.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, s));
+            SIMP_CUDA(c, cudaMemcpyAsync(c->bny, hny.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, s));
+        }
         SIMP_CUDA(c, cudaMemcpyAsync(c->bid, hid.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, s));
         SIMP_CUDA(c, cudaMemcpyAsync(c->binst, hinst.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, s));
         SIMP_CUDA(c, cudaMemcpyAsync(c->bcell, hcell.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, s));
@@ -534,26 +550,33 @@ void enqueue_step(simp_ctx *c, bool diag, bool prof) {
     auto mark = [&](int k) {
         if (prof) cudaEventRecordWithFlags(c->prof_ev[k], c->stream, cudaEventRecordExternal);
     };
+    // continuity density (den_alg 2) and Benz hsml (sle 1) add a density-rate
+    // pass after an update (timed with the stress pass before it)
+    const bool den2 = c->prm.den_alg == 2, benz = c->prm.sle == 1;
     mark(0);
     if (c->prm.int_algorithm == 1) {
         // euler_scheme (time_integration.f90:86-148): one right-hand side
         launch_kinematic(c, c->s0, diag);
         mark(1);
         launch_stress(c, c->s0, c->s0, EPI_EULER);
+        if (den2 || benz) launch_density_rate(c, c->s0, c->s1, den2 ? 2 : 0, true);
         mark(2);
         launch_copy_s1_to_s0(c);
         mark(3);
         mark(4);
     } else {
-        // predictor_corrector (:263-390) or leapfrog_scheme (:289-391): the
+        // predictor_corrector (:155-282) or leapfrog_scheme (:289-391): the
         // same first half step, a different final update
+        const bool leap = c->prm.int_algorithm == 3;
         launch_kinematic(c, c->s0, false);
         mark(1);
         launch_stress(c, c->s0, c->s0, EPI_PREDICT);
+        if (den2) launch_density_rate(c, c->s0, c->s1, 1, false);
         mark(2);
         launch_kinematic(c, c->s1, diag);
         mark(3);
-        launch_stress(c, c->s1, c->s0, c->prm.int_algorithm == 3 ? EPI_LEAP : EPI_CORRECT);
+        launch_stress(c, c->s1, c->s0, leap ? EPI_LEAP : EPI_CORRECT);
+        if (leap ? (den2 || benz) : benz) launch_density_rate(c, c->s1, c->s0, (leap && den2) ? 2 : 0, true);
         mark(4);
     }
     launch_step_finish(c);
@@ -562,8 +585,8 @@ void enqueue_step(simp_ctx *c, bool diag, bool prof) {
 
 int ensure_graph(simp_ctx *c, bool diag) {
     const bool prof = c->profile;
-    if (c->step_graph && c->graph_diag == diag && c->graph_profiled == prof) return SIMP_OK;
-    invalidate_graph(c);
+    const bool same_kind = c->step_graph && c->graph_diag == diag && c->graph_profiled == prof;
+    if (same_kind && !c->graph_stale) return SIMP_OK;
     if (prof && !c->prof_ev[0])
         for (auto &e : c->prof_ev) SIMP_CUDA(c, cudaEventCreate(&e));
     cudaGraph_t g = nullptr;
@@ -574,19 +597,31 @@ int ensure_graph(simp_ctx *c, bool diag) {
     c->graph_kernels = c->launches - before;   // captured, not yet launched
     c->launches = before;
     if (e != cudaSuccess) return simp_cuda_check(c, e, "cudaStreamEndCapture");
+    if (same_kind) {
+        cudaGraphExecUpdateResultInfo info{};
+        if (cudaGraphExecUpdate(c->step_graph, g, &info) == cudaSuccess) {
+            cudaGraphDestroy(g);
+            c->graph_stale = false;
+            return SIMP_OK;
+        }
+        cudaGetLastError();   // (a different topology: instantiate below)
+    }
+    if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+    c->step_graph = nullptr;
     e = cudaGraphInstantiate(&c->step_graph, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return simp_cuda_check(c, e, "cudaGraphInstantiate");
     c->graph_diag = diag;
     c->graph_profiled = prof;
+    c->graph_stale = false;
     return SIMP_OK;
 }
 
 // A single basin whose hsml grew 5% past the size its grid was built for
-// (sle = 2) gets a new grid; until then the stencil radius covers it.
+// (sle = 1, 2) gets a new grid; until then the stencil radius covers it.
 int maybe_regrid(simp_ctx *c, bool *done) {
     *done = false;
-    if (c->max_inst != 1 || !c->insts[0].active || c->prm.sle != 2) return SIMP_OK;
+    if (c->max_inst != 1 || !c->insts[0].active || c->prm.sle == 0) return SIMP_OK;
     InstHost &h = c->insts[0];
     Inst I{};
     TRY(read_inst(c, 0, &I));
@@ -689,11 +724,16 @@ int create(const simp_params *params, int32_t maxn, int32_t maxnb, int32_t max_i
     TRY(dalloc(c, &c->id, M));
     TRY(dalloc(c, &c->pinst, M));
     TRY(dalloc(c, &c->perm, M));
-    TRY(dalloc(c, &c->tmp, 14 * MX));
+    TRY(dalloc(c, &c->tmp, 15 * MX));
+    if (c->prm.sle == 1 && c->prm.den_alg != 2) TRY(dalloc(c, &c->drhodt, M));
     TRY(dalloc(c, &c->itmp, 5 * MX));
     TRY(dalloc(c, &c->bx, MB));
     TRY(dalloc(c, &c->by, MB));
     TRY(dalloc(c, &c->bm, MB));
+    if (c->prm.bfa == 2) {
+        TRY(dalloc(c, &c->bnx, MB));
+        TRY(dalloc(c, &c->bny, MB));
+    }
     TRY(dalloc(c, &c->bid, MB));
     TRY(dalloc(c, &c->binst, MB));
     TRY(dalloc(c, &c->bcell, MB));
@@ -735,6 +775,17 @@ simp_forcing forcing_of(const simp_params &p) {
 
 namespace simp {
 
+// bf_Wang reads b_normal (boundary_force.f90:146-147), which the reference
+// sets with the walls (boundaries.f90:232-287): a basin with walls needs
+// them before its first right-hand side.
+int check_normals(simp_ctx *c) {
+    if (c->prm.bfa != 2 || !c->prm.boundary_pressure) return SIMP_OK;
+    const InstHost &h = c->insts[0];
+    if (h.active && h.nb > 0 && h.bn.size() != 2 * (size_t)h.nb)
+        return simp_fail(c, SIMP_ERR_STATE, "bfa = 2 needs the wall normals (simp_gpu_set_wall_normals)");
+    return SIMP_OK;
+}
+
 // Device bytes per unit of maxn of a context with these parameters (the
 // allocations of create() below, with room for its cell lists).
 double bytes_per_particle(const simp_params &p) {
@@ -748,7 +799,8 @@ double bytes_per_particle(const simp_params &p) {
     b += kMaxPairs * 4.0 + 4.0;                               // pair lists
     b += mixed ? kDwRows * 8.0 : 0.0;                         // kept kernel gradients
     b += 9 * 8.0 + 4 * 8.0;                                   // diagnostics, rates
-    b += 4 * 4.0 + 14 * 8.0 + 5 * 4.0 + 4.0;                  // sort keys, scratch
+    if (p.sle == 1 && p.den_alg != 2) b += 8.0;               // Benz's kept drhodt
+    b += 4 * 4.0 + 15 * 8.0 + 5 * 4.0 + 4.0;                  // sort keys, scratch
     b += 16.0 / kMinTileThreads + 48.0;                       // chunks, cell lists (worst case)
     return b;
 }
@@ -759,6 +811,7 @@ int step_enqueue(simp_ctx *c, int nsteps) {
     if (!c->have_state) return simp_fail(c, SIMP_ERR_STATE, "step before set_state");
     cudaStream_t s = c->stream;
     if (c->n == 0 || nsteps == 0) return SIMP_OK;   // (an empty batch)
+    TRY(check_normals(c));
     bool regridded = false;
     TRY(maybe_regrid(c, &regridded));
     launch_reset_stats(c);
@@ -887,6 +940,9 @@ void simp_params_reference_default(simp_params *p) {
     p->zeta_max = 0.0;   // data_variables.f90:154 declares them without a value
     p->eta_max = 0.0;
     p->phi = 45.0;       // data_variables.f90:159
+    p->xi = (double)0.5225f;   // default-real literals (data_variables.f90:158, 175)
+    p->Y = 1.0e9;
+    p->nu = (double)0.3f;
 }
 
 int32_t simp_gpu_create(const simp_params *params, int32_t maxn, int32_t maxnb, simp_ctx **out) {
@@ -945,6 +1001,7 @@ int32_t simp_gpu_set_state(simp_ctx *c, int32_t ntotal, const double *x, const d
     sc.list_scan = 1;
     SIMP_CUDA(c, cudaMemcpyAsync(c->sc, c->sc_host, sizeof(Scalars), cudaMemcpyHostToDevice, c->stream));
     SIMP_CUDA(c, cudaMemsetAsync(c->inst_dev, 0, sizeof(Inst), c->stream));
+    if (c->drhodt) SIMP_CUDA(c, cudaMemsetAsync(c->drhodt, 0, sizeof(double) * (size_t)c->maxn, c->stream));
     c->have_state = false;
     TRY(add_instance(c, 0, forcing_of(c->prm), ntotal, x, vx, mass, rho, hsml, A, h, ntotalb, xb, massb,
                      current_time));
@@ -975,6 +1032,18 @@ int32_t simp_gpu_batch_add(simp_ctx *c, const simp_forcing *forcing, int32_t nto
     TRY(add_instance(c, q, *forcing, ntotal, x, vx, mass, rho, hsml, A, h, ntotalb, xb, massb, 0.0));
     c->have_state = true;
     *slot = q;
+    return SIMP_OK;
+}
+
+int32_t simp_gpu_set_wall_normals(simp_ctx *c, int32_t ntotalb, const double *b_normal) {
+    if (!c) return SIMP_ERR_BADARG;
+    if (c->max_inst != 1) return simp_fail(c, SIMP_ERR_BADARG, "set_wall_normals is for single-basin contexts");
+    InstHost &h = c->insts[0];
+    if (!c->have_state || !h.active) return simp_fail(c, SIMP_ERR_STATE, "set_wall_normals before set_state");
+    if (ntotalb != h.nb || (ntotalb > 0 && !b_normal))
+        return simp_fail(c, SIMP_ERR_BADARG, "set_wall_normals: ntotalb differs from the state's walls");
+    h.bn.assign(b_normal, b_normal + 2 * (size_t)ntotalb);
+    if (c->bnx) TRY(layout(c));
     return SIMP_OK;
 }
 
@@ -1060,6 +1129,25 @@ int32_t simp_gpu_get_diag(simp_ctx *c, double *eps11, double *eps12, double *eps
     return SIMP_OK;
 }
 
+int32_t simp_gpu_write_output(simp_ctx *c, const char *folder) {
+    if (!c) return SIMP_ERR_BADARG;
+    if (!c->have_state || c->max_inst != 1) return simp_fail(c, SIMP_ERR_STATE, "write_output needs a single basin with state");
+    const InstHost &h = c->insts[0];
+    const size_t n = (size_t)h.n;
+    std::vector<double> xv(4 * n), f(5 * n), dg(9 * n);
+    double t = 0.0;
+    TRY(simp_gpu_get_state(c, xv.data(), xv.data() + 2 * n, f.data(), nullptr, f.data() + n, f.data() + 2 * n,
+                           f.data() + 3 * n, nullptr, &t));
+    double *d[9];
+    for (int k = 0; k < 9; ++k) d[k] = dg.data() + (size_t)k * n;
+    TRY(simp_gpu_get_diag(c, d[0], d[1], d[2], d[3], d[4], d[5], d[6], d[7], d[8]));
+    const int rc = simp_csv_append_snapshot(folder, h.n, h.nb, t, xv.data(), xv.data() + 2 * n, f.data(), d[5],
+                                            f.data() + n, f.data() + 2 * n, f.data() + 3 * n, d[0], d[1], d[2],
+                                            d[6], d[7], d[8]);
+    if (rc) return simp_fail(c, rc, simp_csv_last_error());
+    return SIMP_OK;
+}
+
 int32_t simp_gpu_nnps(simp_ctx *c, int32_t *nip, int32_t *p_i, int32_t *p_j, double *r_ij,
                       double *hsml_ij, int32_t cap, int32_t *bnip, int32_t *bp_i, int32_t *bp_j,
                       double *br_ij, int32_t bcap) {
@@ -1084,6 +1172,7 @@ int32_t simp_gpu_single_step(simp_ctx *c, double current_time, double *dxdt, dou
                              double *dhdt, double *dAdt) {
     if (!c) return SIMP_ERR_BADARG;
     if (!c->have_state || c->max_inst != 1) return simp_fail(c, SIMP_ERR_STATE, "single_step needs a single basin with state");
+    TRY(check_normals(c));
     cudaStream_t s = c->stream;
     k_set_time0<<<1, 1, 0, s>>>(c->sc, c->inst_dev, current_time);
     c->launches += 1;
@@ -1111,7 +1200,7 @@ int32_t simp_gpu_sum_density(simp_ctx *c, double *rho_out) {
     return SIMP_OK;
 }
 
-// time_integration.f90:146-181 for nsteps iterations of every basin.  Each
+// time_integration.f90:38-71 for nsteps iterations of every basin.  Each
 // basin is re-sorted into its grid every kSortEvery of its own steps; in
 // between the device-side stencil radius keeps the cell list exact.
 int32_t simp_gpu_step(simp_ctx *c, int32_t nsteps, double *current_time, double *dt) {

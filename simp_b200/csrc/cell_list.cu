@@ -185,7 +185,7 @@ __global__ void k_cell_sort(int ncells, const int *__restrict__ start, int *__re
     }
 }
 
-constexpr int kGathered = 12;
+constexpr int kGathered = 13;   // (the last one only with Benz's kept drhodt)
 struct Gather {
     const double *src[kGathered];
     double *dst[kGathered];
@@ -212,7 +212,8 @@ __global__ void k_gather(int kept, int from, DueMask due, const int *__restrict_
     if (k >= kept || !moves(from, due, pinst_in, k)) return;
     const int o = perm[k];
 #pragma unroll
-    for (int a = 0; a < kGathered; ++a) gd.dst[a][k] = gd.src[a][o];
+    for (int a = 0; a < kGathered; ++a)
+        if (gd.src[a]) gd.dst[a][k] = gd.src[a][o];
     cell_out[k] = key[o];
     id_out[k] = id_in[o];
     pinst_out[k] = pinst_in[o];
@@ -277,7 +278,8 @@ __global__ void k_put_back(int kept, int from, DueMask due, Gather gd, State s, 
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= kept || !moves(from, due, pinst, k)) return;
 #pragma unroll
-    for (int a = 0; a < kGathered; ++a) const_cast<double *>(gd.src[a])[k] = gd.dst[a][k];
+    for (int a = 0; a < kGathered; ++a)
+        if (gd.src[a]) const_cast<double *>(gd.src[a])[k] = gd.dst[a][k];
     id[k] = id_new[k];
     pinst[k] = pinst_new[k];
     refresh_views(s, k);
@@ -347,7 +349,7 @@ int rebuild(simp_ctx *c, const DueMask &due, int from, bool new_lists) {
         if (c->total_cells > 0)
             k_cell_sort<<<nblk(c->total_cells, 128), 128, 0, s>>>(c->total_cells, c->cell_start, c->perm, c->id);
         double *srcs[kGathered] = {c->s0.x, c->s0.y, c->s0.vx, c->s0.vy, c->s0.m, c->s0.rho,
-                                   c->s0.mor, c->s0.h, c->s0.A, c->s0.hs, c->xr, c->yr};
+                                   c->s0.mor, c->s0.h, c->s0.A, c->s0.hs, c->xr, c->yr, c->drhodt};
         Gather gd;
         for (int a = 0; a < kGathered; ++a) {
             gd.src[a] = srcs[a];
@@ -360,7 +362,7 @@ int rebuild(simp_ctx *c, const DueMask &due, int from, bool new_lists) {
             c->launches += 1;
             if (keep_lists) {
                 NbrList nl{c->nbr, c->nbr_count, c->xl, c->yl, c->maxn};
-                double *xl_new = c->tmp + 12 * MX, *yl_new = c->tmp + 13 * MX;
+                double *xl_new = c->tmp + 13 * MX, *yl_new = c->tmp + 14 * MX;
                 k_remap_lists<<<nblk(kept, 128), 128, 0, s>>>(kept, from, due, c->pinst, c->perm, inv, n, nl,
                                                               c->nbr_tmp, cnt_new, xl_new, yl_new);
                 k_put_back_lists<<<nblk(kept, B), B, 0, s>>>(kept, from, due, c->pinst, nl, c->nbr_tmp, cnt_new,

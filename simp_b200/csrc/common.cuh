@@ -165,6 +165,8 @@ struct Phys {
     double vortex_x, vortex_y, vortex_umax, vortex_radius;
     double max_hsml;
     double zeta_max, eta_max, mu;   // Mohr-Coulomb caps and tan(phi)
+    int bfa, boundary_friction;     // boundary force algorithm and its friction branch
+    double kappa_t, xi, Y, nu;      // friction parameters; Young modulus and Poisson ratio
 };
 
 // Interaction-count bookkeeping for nnps.f90:613-670.
@@ -399,6 +401,63 @@ __device__ __forceinline__ double boundary_w(const Phys &P, double br, double hs
             return 0.0;
         }
     }
+}
+
+// factor * dW/dq of the boundary kernel at q = br / b_length * scale_h
+// (boundary_kernel.f90: b_Quadratic :111-112, b_Gaussian :182-184,
+// b_quintic_spline :257-274, b_Wendland_C2 :348-349, b_Wendland_C4
+// :422-423, b_Wendland_C6 :495-496; the cubic as its kernel's derivative).
+// The kernel gradient is then bdwdx = -(f dW/dq) / b_length * (bdx / br) *
+// scale_h, with bdx = xb - x_i.
+__device__ __forceinline__ double boundary_fdwdq(const Phys &P, double br, double hs_i) {
+    const double sh = (double)P.scale_h;
+    const double q = br / P.b_length * sh;
+    const double shb = sh / P.b_length, s2 = shb * shb;
+    switch (P.skf) {
+        case SIMP_SKF_QUADRATIC:
+            return (2.0 / kPi) * s2 * (0.375 * q - 0.75);
+        case SIMP_SKF_GAUSSIAN:
+        case SIMP_SKF_MARQUIS:
+        case SIMP_SKF_MARQUIS2:
+            return (1.0 / kPi) * s2 * (-2.0 * q * exp(-(q * q)));
+        case SIMP_SKF_QUINTIC: {
+            const double f = (15.0 / (478.0 * kPi)) * s2;
+            const double u3 = 3.0 - q, u2 = 2.0 - q, u1 = 1.0 - q;
+            const double p3 = (u3 * u3) * (u3 * u3), p2 = (u2 * u2) * (u2 * u2), p1 = (u1 * u1) * (u1 * u1);
+            if (q <= 1.0) return f * (-5.0 * p3 + 30.0 * p2 - 75.0 * p1);
+            if (q <= 2.0) return f * (-5.0 * p3 + 30.0 * p2);
+            if (q <= 3.0) return f * (-5.0 * p3);
+            return 0.0;
+        }
+        case SIMP_SKF_WENDLAND_C2: {
+            const double q2 = q * q;
+            return (3.0 / (2.0 * kPi)) * s2 * (20.0 * (q2 * q2 - 3.0 * (q2 * q) + 3.0 * q2 - q));
+        }
+        case SIMP_SKF_WENDLAND_C4: {
+            const double om = 1.0 - q, om2 = om * om;
+            return (3.0 / kPi) * s2 * ((-56.0 * q) * (5.0 * q + 1.0) * (om2 * om2 * om));
+        }
+        case SIMP_SKF_WENDLAND_C6: {
+            const double shh = sh / hs_i;
+            const double factor = (78.0 / (7.0 * kPi)) * (shh * shh);
+            const double om = 1.0 - q;
+            const double om2 = om * om, om4 = om2 * om2;
+            return factor * ((-22.0 * q) * (om4 * om2 * om) * ((16.0 * q + 7.0) * q + 1.0));
+        }
+        default: {
+            const double factor = (15.0 / (7.0 * kPi)) * s2;
+            if (q <= 1.0) return factor * (1.5 * q * q - 2.0 * q);
+            if (q <= 2.0) { const double u = 2.0 - q; return factor * (-0.5 * u * u); }
+            return 0.0;
+        }
+    }
+}
+
+// Sound speed c_yang (sound_speed.f90:54-55), evaluated from the current
+// density: the reference refreshes c after every density update
+// (initialize.f90:200, time_integration.f90:140, 230, 274, 355, 383).
+__device__ __forceinline__ double sound_speed(const Phys &P, double rho) {
+    return sqrt(P.Y * (1.0 - P.nu) / (rho * (1.0 + P.nu) * (1.0 - 2.0 * P.nu)));
 }
 
 // Wind at a particle of an instance: uniform (the reference hard-codes one,

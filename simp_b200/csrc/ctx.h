@@ -20,6 +20,7 @@ struct InstHost {
     long long steps_since_sort = 0;
     long long steps_done = 0;
     std::vector<double> xb, massb; // its walls (re-binned when the layout changes)
+    std::vector<double> bn;        // their normals b_normal(2, nb) (bf_Wang), empty until set
 };
 
 struct simp_ctx {
@@ -45,6 +46,7 @@ struct simp_ctx {
     // particle state sets (device, cell order)
     simp::State s0{}, s1{};
     double *mass1 = nullptr;       // half-step mass when the mass update is on
+    double *drhodt = nullptr;      // Benz hsml without con_density: the reference's drhodt, kept across steps
     double *xr = nullptr, *yr = nullptr;  // sort positions (updated when the instance is re-sorted)
     double *xl = nullptr, *yl = nullptr;  // positions where each Verlet list was built
     int *cell = nullptr;           // sort-time cell key per particle
@@ -68,6 +70,7 @@ struct simp_ctx {
     double *rates = nullptr;       // 4 * maxn
     // wall particles, sorted by cell key
     double *bx = nullptr, *by = nullptr, *bm = nullptr;
+    double *bnx = nullptr, *bny = nullptr;   // wall normals (bfa = 2 only)
     int *bid = nullptr;            // local wall index within its instance
     int *binst = nullptr;          // instance slot of each wall particle
     int *bcell = nullptr;          // cell key per wall slot
@@ -89,7 +92,7 @@ struct simp_ctx {
     // rebuild scratch
     int *cnt = nullptr;            // per-cell counters (cell_cap)
     int *perm = nullptr;           // maxn
-    double *tmp = nullptr;         // 14 * max(maxn, maxnb) doubles reorder scratch
+    double *tmp = nullptr;         // 15 * max(maxn, maxnb) doubles reorder scratch
     int *itmp = nullptr;           // 5 * max(maxn, maxnb) ints
     void *scan_tmp = nullptr;
     size_t scan_tmp_bytes = 0;
@@ -104,6 +107,7 @@ struct simp_ctx {
     size_t pair_buf_cap = 0;
     // step graph
     cudaGraphExec_t step_graph = nullptr;
+    bool graph_stale = false;      // captured arguments changed since the last capture
     bool graph_diag = false;
     bool graph_profiled = false;
     long long graph_kernels = 0;   // kernels per replay
@@ -139,10 +143,14 @@ size_t scan_tmp_bytes(int n);
 // passes.cu
 // stress-pass epilogues: the rates (single_step), the predictor half step
 // and the corrector (predictor_corrector), the Euler step, the leap-frog
-// second half (time_integration.f90:86-148, 263-390, 289-391)
+// second half (time_integration.f90:86-148, 155-282, 289-391)
 enum EpiMode : int { EPI_RATES = 0, EPI_PREDICT = 1, EPI_CORRECT = 2, EPI_EULER = 3, EPI_LEAP = 4 };
 void launch_kinematic(simp_ctx *c, const State &s, bool diag);
 void launch_stress(simp_ctx *c, const State &nb, const State &own, EpiMode mode);
+// drho/dt over the last right-hand side's pairs with the updated velocities
+// (con_density, Benz_hsml): rho_upd 0 none, 1 half step, 2 full step; tail:
+// the step's final hsml, its bounds and the VP dt
+void launch_density_rate(simp_ctx *c, const State &g, const State &v, int rho_upd, bool tail);
 void launch_step_finish(simp_ctx *c);
 void launch_copy_s1_to_s0(simp_ctx *c);
 void launch_reset_stats(simp_ctx *c);

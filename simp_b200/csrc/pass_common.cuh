@@ -22,7 +22,7 @@
 //   a_i = rho_i / (rho_ice h_i) sum_j m_j (tau_i + tau_j) . grad W_ij
 //         - sum_walls F_b / rho_i + wind + water drag
 //   followed by one of three epilogues: the rates (single_step), the
-//   predictor half step (time_integration.f90:314-338) or the corrector and
+//   predictor half step (time_integration.f90:204-227) or the corrector and
 //   final update (:343-388).
 //
 // Each pair is evaluated from both sides (gather form, no atomics on the
@@ -405,6 +405,7 @@ struct StressArgs {
     const int *pinst;
     const int *cell;
     const double *bx, *by, *bm;
+    const double *bnx, *bny;   // wall normals (bfa = 2)
     const int *bstart;
     int nb;
     Phys P;
@@ -517,7 +518,7 @@ __device__ __forceinline__ void block_bounds(Scalars *sc, unsigned active, unsig
 // The last block of a stress pass to finish decides whether the next
 // kinematic pass rebuilds the Verlet lists: when the fastest particle moved
 // 3/4 of the skin since they were built (lists are then complete only for
-// particles that moved less than skin / 4), or when hsml changes (sle = 2).
+// particles that moved less than skin / 4), or when hsml changes (sle 1, 2).
 // Threadfence reduction; no block waits on another.  Every block of the
 // grid calls it once, with all its threads.
 __device__ __forceinline__ void lists_block_done(const StressArgs &a) {
@@ -531,7 +532,7 @@ __device__ __forceinline__ void lists_block_done(const StressArgs &a) {
     if (last && threadIdx.x == 0) {
         __threadfence();
         const double dl = sqrt(bitsd(atomicAdd(&a.sc->dlist2_bits, 0ull)));
-        const bool stale = (a.P.sle == 2) || !(dl < 0.75 * a.sc->skin);
+        const bool stale = (a.P.sle != 0) || !(dl < 0.75 * a.sc->skin);
         a.sc->list_scan = stale ? 1 : 0;
         a.sc->blocks_done = 0u;
     }
@@ -552,26 +553,63 @@ __device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool l
     const double fi = (P.pa_sph == 2) ? 1.0 / P.rho_ice / hh : rho / P.rho_ice / hh;
     double ax = fi * fma(a.tau11[i], Sx, fma(a.tau12[i], Sy, Tx));
     double ay = fi * fma(a.tau12[i], Sx, fma(a.tau22[i], Sy, Ty));
-    // boundary force (bf_Monaghan normal component, boundary_force.f90:78-82)
-    if (P.boundary_pressure && a.nb > 0 && !dead) {
+    // boundary force, boundary_kernel.f90:5-45 calling boundary_force.f90
+    // once per wall pair (bfa 1 bf_Monaghan :38-102, 2 bf_Wang :109-176,
+    // 3 bf_Marquis :183-225)
+    const double vxi = s.vx[i], vyi = s.vy[i];
+    if ((P.boundary_pressure || P.boundary_friction) && a.nb > 0 && !dead) {
         const Grid g = inst_grid(I, a.cell_start);
         const double bl = I.b_length;
         const int Rb = wall_radius(I.dmax2_bits, g, bl);
         const BinRule bb = make_bin_rule(I.bs, xi, yi, bl);
-        double fx = 0.0, fy = 0.0;
+        const double sh = (double)P.scale_h;
+        const double dt = a.sc->dt;
+        const double csnd = P.boundary_friction ? sound_speed(P, rho) : 0.0;
+        double fx = 0.0, fy = 0.0;   // sum of F_b (Monaghan), applied as -F_b / rho
+        double gx = 0.0, gy = 0.0;   // acceleration terms added as they are
         cnt += for_each_wall(a.bx, a.by, a.bstart, g, ci, Rb, bb, xi, yi, bl,
                              [&](int b, double bdx, double bdy, double d) {
-                                 const double bw = boundary_w(P, d, hi);
-                                 const double mb = a.bm[b];
-                                 const double coef = P.kappa_n * bw * 2.0 * mb / ((mi + mb) * (d * d));
-                                 fx += coef * bdx;
-                                 fy += coef * bdy;
+                                 if (P.bfa == 1) {
+                                     const double mb = a.bm[b];
+                                     if (P.boundary_pressure) {
+                                         const double bw = boundary_w(P, d, hi);
+                                         const double coef = P.kappa_n * bw * 2.0 * mb / ((mi + mb) * (d * d));
+                                         fx += coef * bdx;
+                                         fy += coef * bdy;
+                                     }
+                                     if (P.boundary_friction) {   // :85-100
+                                         const double t = boundary_fdwdq(P, d, hi) / bl;
+                                         const double bwx = -(t * (bdx / d) * sh), bwy = -(t * (bdy / d) * sh);
+                                         const double v_r = vxi * bdx + vyi * bdy;
+                                         const double pi_aj = P.kappa_t * csnd * v_r / d / rho;
+                                         gx += (-1.0 * mb * pi_aj * bwx) / rho;
+                                         gy += (-1.0 * mb * pi_aj * bwy) / rho;
+                                     }
+                                 } else if (P.bfa == 2) {
+                                     if (P.boundary_pressure) {   // :146-172
+                                         const double nx = a.bnx[b], ny = a.bny[b];
+                                         const double v1 = nx * vxi + ny * vyi;
+                                         double v2 = sqrt(vxi * vxi + vyi * vyi) - v1;
+                                         const double F1 = mi * v1 / dt;
+                                         double F2 = mi * v2 / dt;
+                                         if (P.boundary_friction && fabs(v2) > fabs(P.xi * v1)) {
+                                             v2 = v2 * P.xi * fabs(F1 / F2);
+                                             F2 = mi * v2 / dt;
+                                         }
+                                         gx += F1 * nx + F2 * ny;
+                                         gy += F1 * ny - F2 * nx;
+                                     }
+                                 } else if (!P.boundary_pressure && P.boundary_friction) {   // :212-222
+                                     gx -= vxi * (1.0 - d / bl);
+                                     gy -= vyi * (1.0 - d / bl);
+                                 }
                              });
         ax -= fx / rho;
         ay -= fy / rho;
+        ax += gx;
+        ay += gy;
     }
     // drag, wind_forcing.f90:35-51 and water_drag.f90:35-53 (off at t <= 0)
-    const double vxi = s.vx[i], vyi = s.vy[i];
     const double tnow = I.t;
     if (P.wind_force && tnow > 0.0) {
         double wu, wv;
@@ -607,7 +645,7 @@ __device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool l
     const double x0 = b.x[i], y0 = b.y[i], vx0 = b.vx[i], vy0 = b.vy[i], h0 = b.h[i], A0 = b.A[i];
     double xn, yn, vxn, vyn, hn, An;
     if (a.mode == EPI_PREDICT) {
-        // time_integration.f90:315-323 (and the leap-frog's first half, :323-332)
+        // time_integration.f90:207-215 (and the leap-frog's first half, :333-341)
         xn = x0 + vxi * dt / 2.0;
         yn = y0 + vyi * dt / 2.0;
         vxn = vx0 + ax * dt / 2.0;
@@ -615,7 +653,7 @@ __device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool l
         hn = h0 + dhdt * dt / 2.0;
         An = A0 + dAdt * dt / 2.0;
     } else if (a.mode == EPI_EULER) {
-        // euler_scheme, time_integration.f90:110-117
+        // euler_scheme, time_integration.f90:117-125
         xn = x0 + vxi * dt;
         yn = y0 + vyi * dt;
         vxn = vx0 + ax * dt;
@@ -623,7 +661,7 @@ __device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool l
         hn = h0 + dhdt * dt;
         An = A0 + dAdt * dt;
     } else if (a.mode == EPI_LEAP) {
-        // leapfrog_scheme, time_integration.f90:356-364 (vx0: the step-start
+        // leapfrog_scheme, time_integration.f90:361-369 (vx0: the step-start
         // velocity, vxi: the half-step one)
         vxn = vx0 + ax * dt;
         vyn = vy0 + ay * dt;
@@ -632,7 +670,7 @@ __device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool l
         yn = y0 + (vy0 + vyi) * dt / 2.0;
         An = A0 + dAdt * dt;
     } else {
-        // time_integration.f90:344-367
+        // time_integration.f90:236-259
         const double x12 = x0 + vxi * dt / 2.0, y12 = y0 + vyi * dt / 2.0;
         const double vx12 = vx0 + ax * dt / 2.0, vy12 = vy0 + ay * dt / 2.0;
         const double h12 = h0 + dhdt * dt / 2.0, A12 = A0 + dAdt * dt / 2.0;
@@ -644,18 +682,35 @@ __device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool l
         An = 2.0 * A12 - A0;
     }
     if (An > 1.0) An = 1.0;
-    const double rhon = hn * P.rho_ice;                       // density.f90:192
+    // the step's last update: hsml, VP time step (after the corrector, the
+    // Euler step or the leap-frog's second half).  `tail_later`: a
+    // density-rate pass (k_density_rate) follows and does them, because the
+    // final density (con_density) or Benz's hsml needs the updated
+    // velocities of the neighbours.
+    const bool final_update = a.mode == EPI_CORRECT || a.mode == EPI_EULER || a.mode == EPI_LEAP;
+    const bool den2 = P.den_alg == 2;
+    const bool tail_later = final_update && ((den2 && a.mode != EPI_CORRECT) || P.sle == 1);
+    double rhon;
+    if (!den2) {
+        rhon = hn * P.rho_ice;                                // density.f90:192
+    } else if (a.mode == EPI_CORRECT) {
+        // time_integration.f90:242-266: drho/dt of the corrector's density
+        // call (half-step velocities and pairs) is the negated divergence
+        // sum of this right-hand side
+        const double r0 = b.rho[i];
+        const double r12 = r0 + (-dv) * dt / 2.0;
+        rhon = 2.0 * r12 - r0;
+    } else {
+        rhon = b.rho[i];   // rho_1, until k_density_rate adds drho/dt dt
+    }
     double mn = b.m[i];
     const double hs_old = b.hs[i];
     if (P.sle != 2 && P.mass_from_area) {                     // mass_evolution.f90:66-69
         const double ar = kPi * ((P.alpha * hs_old) * (P.alpha * hs_old));
         mn = P.rho_ice * An * hn * ar;
     }
-    // the step's last update: hsml, VP time step (after the corrector, the
-    // Euler step or the leap-frog's second half)
-    const bool final_update = a.mode == EPI_CORRECT || a.mode == EPI_EULER || a.mode == EPI_LEAP;
     double hsn = hs_old;
-    if (final_update && P.sle == 2) {                         // smoothing_length.f90:136-142
+    if (final_update && !tail_later && P.sle == 2) {          // smoothing_length.f90:136-142
         hsn = sqrt(mn / rhon) * (double)P.hsml_multiplicity;
         if (hsn > P.max_hsml) hsn = P.max_hsml;
     }
@@ -671,8 +726,10 @@ __device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool l
         dl2 = dxl * dxl + dyl * dyl;
         if (!live || !isfinite(dl2)) dl2 = 0.0;
     }
+    // (dead lanes contribute neutral bounds: in place updates, the particle
+    // they mirror may already have been written by its own thread)
     double xa = fmax(fabs(xn), fabs(yn));
-    if (!isfinite(xa)) xa = 0.0;
+    if (!live || !isfinite(xa)) xa = 0.0;
     const bool bad = !(isfinite(xn) && isfinite(yn) && isfinite(vxn) && isfinite(vyn) &&
                        isfinite(hn) && isfinite(An));
     if (live && bad) {
@@ -697,21 +754,23 @@ __device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool l
         o.pf[i] = make_float4((float)xn, (float)yn, hsf, 0.0f);
         if (o.hmm) o.hmm[i] = make_float4(hsf, (float)mn, (float)morn, 0.0f);
         else o.mm[i] = make_double2(mn, morn);
-        if (final_update && P.sle == 2) a.hs_next[i] = hsn;
+        if (final_update && !tail_later && P.sle == 2) a.hs_next[i] = hsn;
     }
     // this step's bounds, one block-wide reduction
-    const bool corr = final_update;
+    const bool corr = final_update && !tail_later;
     unsigned active = 1u | (lists ? 2u : 0u) | 4u;
     unsigned long long v[kBounds] = {(unsigned long long)(live ? cnt : 0), dbits(dl2), dbits(xa), ~0ull, 0ull,
                                      ~0ull};
     if (corr && P.sle == 2) {                                   // smoothing_length.f90:136-142
         active |= 8u | 16u;
-        v[3] = dbits(hsn);
-        v[4] = dbits(hsn);
+        if (live) {
+            v[3] = dbits(hsn);
+            v[4] = dbits(hsn);
+        }
     }
     if (corr && P.tse == 2) {                                   // time_step.f90:155
         active |= 32u;
-        v[5] = dbits(P.rho_ice * (hsn * hsn) * P.delta_min / (P.P_star * (1.0 + P.k_t)));
+        if (live) v[5] = dbits(P.rho_ice * (hsn * hsn) * P.delta_min / (P.P_star * (1.0 + P.k_t)));
     }
     block_bounds(a.sc, active, v);
     if (lists) lists_block_done(a);

@@ -156,7 +156,115 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksStress) k_stress(StressArgs 
                   true);
 }
 
-// New hsml of the next step (sle = 2) and its FP32 copy.
+// Density rate drho/dt_i = sum_j m_j (v_i - v_j) . grad_i W_ij over the
+// pairs of the right-hand side just evaluated, with the velocities the
+// integrator has just written: con_density (density.f90:107-165, called
+// after each update, time_integration.f90:128-133, 218-223, 344-349, 372-377)
+// and the same sum in Benz_hsml (smoothing_length.f90:62-80).  The pair
+// geometry and hsml are those of the right-hand side's state (the reference
+// reuses that right-hand side's p_i, p_j and dwdx); the masses are the
+// current ones at the call: the right-hand side's for con_density (called
+// before mass_evolution), the updated ones for Benz_hsml's own sum (called
+// after it).  The sum is FP64 in both precision forms.
+//   rho_upd: 0 none, 1 rho = rho_1 + drho/dt dt / 2, 2 rho = rho_1 + drho/dt dt;
+//   tail: the step's final hsml (Benz, or Marquis with the new density),
+//   its bounds and the VP time step, which the stress epilogue left out.
+struct DensArgs {
+    State g;             // right-hand side state (positions, hsml, masses)
+    State v;             // updated state: velocities in, rho and views out
+    const double *mj;    // neighbour masses of the sum
+    const double *rho1;  // step-start density
+    double *acc;         // Benz's drhodt when den_alg != 2 (kept across steps)
+    double *hs_next;
+    PairList pl;
+    const int *cell_start, *cell, *pinst;
+    const Inst *inst;
+    Scalars *sc;
+    Phys P;
+    int n, rho_upd, tail;
+};
+
+__global__ void __launch_bounds__(kBlock) k_density_rate(DensArgs a) {
+    const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i0 < a.n;
+    const int i = live ? i0 : a.n - 1;   // dead lanes mirror the last particle for the reductions
+    const State &g = a.g;
+    const Phys &P = a.P;
+    const Inst &I = a.inst[a.pinst[i]];
+    const bool dead = (I.flags & FLAG_NONFINITE) != 0;
+    const double xi = g.x[i], yi = g.y[i], hi = g.hs[i];
+    const double inv_hi = 1.0 / hi;
+    const double vxi = a.v.vx[i], vyi = a.v.vy[i];
+    Sum<double> r;
+    auto add = [&](int j) {
+        const double2 q = g.xy[j];
+        const PairGeom<double> pg = pair_geom<double, false>(P, xi - q.x, yi - q.y, hi, inv_hi, g.hs[j]);
+        const double2 v = a.v.vxy[j];
+        const double dvx = vxi - v.x, dvy = vyi - v.y;
+        r.madd(a.mj[j], fma(dvx, pg.gfac * pg.dx, dvy * (pg.gfac * pg.dy)));
+    };
+    const int cnt = a.pl.count[i];
+    if (dead) {
+    } else if (cnt <= kMaxPairs) {
+#pragma unroll 4
+        for (int k = 0; k < cnt; ++k) add(a.pl.pj[(size_t)k * a.pl.stride + i]);
+    } else {
+        // (more pairs than the list holds: the cell stencil of the
+        // right-hand side's positions, whose bounds the instance keeps)
+        const PairCtx pc = pair_ctx(g, a.sc, I, a.cell_start, i);
+        for_stencil(pc.g, i, a.cell[i], stencil_radius(pc.hmax, pc.dmax2_bits, pc.g, 0.0), [&](int j) {
+            if (is_pair(g, pc, j)) add(j);
+        });
+    }
+    const double drhodt = r.get();
+    const double dt = a.sc->dt;
+    const State &o = a.v;
+    double rhon = o.rho[i];
+    if (a.rho_upd && live) {
+        rhon = (a.rho_upd == 1) ? a.rho1[i] + drhodt * dt / 2.0 : a.rho1[i] + drhodt * dt;
+        o.rho[i] = rhon;
+        o.mor[i] = o.m[i] / rhon;
+        refresh_views(o, i);
+    }
+    if (!a.tail) return;
+    const double hs_old = g.hs[i];
+    double hsn = hs_old;
+    if (P.sle == 1) {
+        // Benz_hsml, smoothing_length.f90:82-94.  Without con_density the
+        // reference adds to its drhodt array, never cleared: kept per
+        // particle across steps (and re-sorts) here.
+        double d = drhodt;
+        if (a.acc) {
+            d = a.acc[i] + drhodt;
+            if (live) a.acc[i] = d;
+        }
+        const double dhs = -hs_old * d / 2.0 / rhon;
+        hsn = hs_old + dhs * dt;
+        if (hsn < 0.0) hsn = hsn - dhs * dt;
+    } else if (P.sle == 2) {                                   // smoothing_length.f90:136-142
+        hsn = sqrt(o.m[i] / rhon) * (double)P.hsml_multiplicity;
+        if (hsn > P.max_hsml) hsn = P.max_hsml;
+    }
+    if (live && P.sle != 0) a.hs_next[i] = hsn;
+    // (dead lanes contribute neutral values: the particle they mirror may
+    // already have been updated by its own thread)
+    unsigned active = 0u;
+    unsigned long long v[kBounds] = {0ull, 0ull, 0ull, ~0ull, 0ull, ~0ull};
+    if (P.sle != 0) {
+        active |= 8u | 16u;
+        if (live) {
+            v[3] = dbits(hsn);
+            v[4] = dbits(hsn);
+        }
+    }
+    if (P.tse == 2) {                                          // time_step.f90:155
+        active |= 32u;
+        if (live) v[5] = dbits(P.rho_ice * (hsn * hsn) * P.delta_min / (P.P_star * (1.0 + P.k_t)));
+    }
+    block_bounds(a.sc, active, v);
+}
+
+// New hsml of the next step (sle = 1, 2) and its FP32 copy.
 __global__ void k_commit_hsml(int n, const double *__restrict__ hs_next, State s0) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -169,9 +277,9 @@ __global__ void k_commit_hsml(int n, const double *__restrict__ hs_next, State s
 }
 
 // End of a predictor-corrector step: time_step's new dt, current_time += dt
-// (time_integration.f90:179, using the dt computed at the end of the step),
+// (time_integration.f90:71, using the dt computed at the end of the step),
 // and the new hsml bounds.
-// (One basin per context when tse = 2 or sle = 2: instance 0 carries its
+// (One basin per context when tse = 2 or sle != 0: instance 0 carries its
 // hsml bounds.)  Every instance's current_time advances by the same dt.
 constexpr int kFinishThreads = 256;
 __global__ void __launch_bounds__(kFinishThreads) k_step_finish(Scalars *sc, Inst *inst, int ninst, int tse,
@@ -184,7 +292,7 @@ __global__ void __launch_bounds__(kFinishThreads) k_step_finish(Scalars *sc, Ins
         }
         dt = sc->dt;
         sc->t = sc->t + dt;
-        if (sle == 2) {
+        if (sle != 0) {
             sc->hmin = bitsd(sc->acc_hmin);
             sc->hmax = fmax(sc->hmax, bitsd(sc->acc_hmax));
             sc->bs = 2.0 * sc->hmin;
@@ -301,6 +409,8 @@ void launch_stress(simp_ctx *c, const State &rhs, const State &base, EpiMode mod
     a.bx = c->bx;
     a.by = c->by;
     a.bm = c->bm;
+    a.bnx = c->bnx;
+    a.bny = c->bny;
     a.bstart = c->bcell_start;
     a.nb = c->nb;
     a.P = c->phys;
@@ -331,8 +441,30 @@ void launch_stress(simp_ctx *c, const State &rhs, const State &base, EpiMode mod
     c->launches += 1;
 }
 
+void launch_density_rate(simp_ctx *c, const State &g, const State &v, int rho_upd, bool tail) {
+    DensArgs a{};
+    a.g = g;
+    a.v = v;
+    a.rho1 = c->s0.rho;
+    a.acc = c->drhodt;
+    a.mj = c->drhodt ? v.m : g.m;
+    a.hs_next = c->tmp;
+    a.pl = pair_list(c);
+    a.cell_start = c->cell_start;
+    a.cell = c->cell;
+    a.pinst = c->pinst;
+    a.inst = c->inst_dev;
+    a.sc = c->sc;
+    a.P = c->phys;
+    a.n = c->n;
+    a.rho_upd = rho_upd;
+    a.tail = tail ? 1 : 0;
+    k_density_rate<<<nblk(c->n, kBlock), kBlock, 0, c->stream>>>(a);
+    c->launches += 1;
+}
+
 void launch_step_finish(simp_ctx *c) {
-    if (c->prm.sle == 2) {
+    if (c->prm.sle != 0) {
         k_commit_hsml<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->n, c->tmp, c->s0);
         c->launches += 1;
     }

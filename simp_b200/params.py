@@ -45,6 +45,7 @@ _DBL_FIELDS = [
     "vortex_x", "vortex_y", "vortex_umax", "vortex_radius",
     "dt", "max_hsml", "skin",
     "zeta_max", "eta_max", "phi",
+    "xi", "Y", "nu",
 ]
 
 
@@ -158,6 +159,9 @@ def reference_default() -> SimpParams:
     p.zeta_max = 0.0          # data_variables.f90:154, declared without a value
     p.eta_max = 0.0
     p.phi = 45.0              # data_variables.f90:159 (mu = tan(phi pi / 180.), :180)
+    p.xi = _real4(0.5225)     # data_variables.f90:175, a default-real literal
+    p.Y = 1.0e9               # :157
+    p.nu = _real4(0.3)        # :158
     return p
 
 

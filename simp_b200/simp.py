@@ -3,7 +3,7 @@
 The reference drives its physics through argument-less subroutines on module
 globals: NNPS (neighbor/nnps.f90:5), single_step (integration/single_step.f90:5),
 density (phy_quantities/density.f90:5), predictor_corrector and the
-time_integration loop (integration/time_integration.f90:146-181, 263-390).
+time_integration loop (integration/time_integration.f90:38-71, 155-282).
 ``Simp`` holds those globals resident on the GPU and offers the same
 operations under the same names.  Errors the reference turns into a STOP
 banner raise ``SimpError`` carrying the banner text and the status code.
@@ -89,6 +89,8 @@ class Simp:
         prm = b.params if params is None else params
         s = cls(prm, maxn or b.n, max(b.nb, 1))
         s.set_state(b.x, b.vx, b.mass, b.rho, b.hsml, b.A, b.h, b.xb, b.massb, prm.dt, 0.0)
+        if prm.bfa == 2 and b.nb > 0 and getattr(b, "bn", None) is not None:
+            s.set_wall_normals(b.bn)
         return s
 
     # -- state ------------------------------------------------------------
@@ -113,6 +115,15 @@ class Simp:
                                               ctypes.byref(dt), ctypes.byref(t)))
         out["dt"], out["current_time"] = dt.value, t.value
         return out
+
+    def write_output(self, folder: str):
+        """Appends a snapshot to the reference's output files (output.f90:61-78)."""
+        self._chk(self.lib.simp_gpu_write_output(self.h, str(folder).encode()))
+
+    def set_wall_normals(self, b_normal: np.ndarray):
+        """b_normal(2, ntotalb) of the walls (Wang boundary force, bfa = 2)."""
+        bn = np.ascontiguousarray(b_normal, dtype=np.float64).reshape(-1, 2)
+        self._chk(self.lib.simp_gpu_set_wall_normals(self.h, bn.shape[0], _lib.dptr(bn)))
 
     def set_forcing(self, forcing: SimpForcing):
         """Wind of this basin (and of later set_state calls)."""

@@ -11,8 +11,8 @@ import pytest
 from helpers import assert_same_pairs, rel_l2, smooth_velocity
 from simp_b200 import basins
 from simp_b200.params import SKF_WENDLAND_C6
-from simp_b200.simp import (SIMP_ERR_IND_INT, SIMP_ERR_MAXN, SIMP_ERR_PAIR_CAP, Simp,
-                            SimpError)
+from simp_b200.simp import (SIMP_ERR_BADARG, SIMP_ERR_IND_INT, SIMP_ERR_MAXN, SIMP_ERR_PAIR_CAP,
+                            SIMP_ERR_STATE, Simp, SimpError)
 
 pytestmark = pytest.mark.gpu
 
@@ -260,6 +260,21 @@ VARIANTS = {
     "stress_2": dict(pa_sph=2),
     "euler": dict(int_algorithm=1),
     "leapfrog": dict(int_algorithm=3),
+    # continuity density (density.f90:107-165) under each integrator
+    "con_density": dict(den_alg=2),
+    "con_density_euler": dict(den_alg=2, int_algorithm=1),
+    "con_density_leapfrog": dict(den_alg=2, int_algorithm=3),
+    # Benz hsml (smoothing_length.f90:40-111): with the diagnostic density
+    # its drhodt accumulates over the steps; with con_density it does not
+    "benz_hsml": dict(sle=1),
+    "benz_hsml_euler": dict(sle=1, int_algorithm=1),
+    "benz_hsml_leapfrog": dict(sle=1, int_algorithm=3, tse=2),
+    "benz_con_density": dict(sle=1, den_alg=2, tse=2),
+    "benz_con_density_euler": dict(sle=1, den_alg=2, int_algorithm=1),
+    "benz_mass_from_area": dict(sle=1, mass_from_area=1),
+    # Marquis hsml from the continuity density (after the density pass)
+    "marquis_con_density": dict(sle=2, den_alg=2),
+    "marquis_con_density_leapfrog": dict(sle=2, den_alg=2, int_algorithm=3),
 }
 
 
@@ -281,6 +296,73 @@ def test_switch_variants_against_oracle(gpu_lib, oracle_mod, name):
     g2.time_integration(10)
     o2.step(10)
     sg, so = g2.get_state(), o2.get_state()
-    for k in ("x", "vx", "h", "A", "rho"):
+    for k in ("x", "vx", "h", "A", "rho", "hsml"):
         assert rel_l2(sg[k], so[k]) < 1e-9, (k, rel_l2(sg[k], so[k]))
     assert sg["current_time"] == pytest.approx(so["current_time"])
+    if prm.sle != 0 or prm.den_alg == 2:
+        # the variant is live: hsml or rho moved away from their start
+        moved = sg["hsml"] if prm.sle != 0 else sg["rho"]
+        start = b.hsml if prm.sle != 0 else b.rho
+        assert not np.array_equal(moved, start)
+
+
+# Boundary force variants (boundary_force.f90): basin walled on four sides,
+# moving into its walls.  The Wang force adds m_i v / dt per wall pair to an
+# acceleration, as the reference does, so its trajectories run away: it is
+# checked on one right-hand side.
+BOUNDARY = {
+    "monaghan_friction": (dict(boundary_friction=1), 10),
+    "monaghan_friction_c6": (dict(boundary_friction=1, skf=6), 10),
+    "wang": (dict(bfa=2), 0),
+    "wang_friction": (dict(bfa=2, boundary_friction=1), 0),
+    "marquis_pressure": (dict(bfa=3), 10),
+    # (its friction decelerates by up to 1/s per wall pair: explicit steps of
+    # 1 s overshoot, as they would in the reference)
+    "marquis_friction": (dict(bfa=3, boundary_pressure=0, boundary_friction=1, dt=1e-2), 10),
+}
+
+
+def _walled_basin():
+    b = basins.make_basin(50, 2000.0, 11, walls="+x-x+y-y")
+    b.vx = smooth_velocity(b.x, b.L, amp=0.3, seed=41)
+    b.h = b.h * np.linspace(0.9, 1.1, b.n)
+    b.rho = b.h * 900.0
+    return b
+
+
+@pytest.mark.parametrize("name", sorted(BOUNDARY))
+def test_boundary_force_variants_against_oracle(gpu_lib, oracle_mod, name):
+    b = _walled_basin()
+    kw, nsteps = BOUNDARY[name]
+    prm = _variant(b, **kw)
+    g, o = _pair(b, oracle_mod, prm)
+    rg, ro = g.single_step(3600.0), o.single_step(3600.0)
+    for k in ("dvxdt", "dhdt", "dAdt"):
+        assert rel_l2(rg[k], ro[k]) < TOL_RHS, (k, rel_l2(rg[k], ro[k]))
+    if prm.bfa == 3 and prm.boundary_pressure:
+        # bf_Marquis with the pressure switch on returns at once: no wall force
+        q = _variant(b, **dict(kw, boundary_pressure=0))
+        r0 = Simp.from_basin(b, q).single_step(3600.0)
+        assert np.array_equal(rg["dvxdt"], r0["dvxdt"])
+    if nsteps:
+        g2, o2 = _pair(b, oracle_mod, prm)
+        g2.time_integration(nsteps)
+        o2.step(nsteps)
+        sg, so = g2.get_state(), o2.get_state()
+        for k in ("x", "vx", "h", "A", "rho"):
+            assert rel_l2(sg[k], so[k]) < 1e-9, (k, rel_l2(sg[k], so[k]))
+
+
+def test_wang_force_needs_wall_normals(gpu_lib):
+    b = _walled_basin()
+    prm = _variant(b, bfa=2)
+    g = Simp(prm, b.n, b.nb)
+    g.set_state(b.x, b.vx, b.mass, b.rho, b.hsml, b.A, b.h, b.xb, b.massb, prm.dt, 0.0)
+    with pytest.raises(SimpError) as ex:
+        g.time_integration(1)
+    assert ex.value.code == SIMP_ERR_STATE
+    with pytest.raises(SimpError) as ex:
+        g.set_wall_normals(b.bn[:-1])
+    assert ex.value.code == SIMP_ERR_BADARG
+    g.set_wall_normals(b.bn)
+    g.single_step(3600.0)

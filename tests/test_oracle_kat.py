@@ -161,6 +161,89 @@ def test_mass_is_conserved(oracle_mod):
     assert np.array_equal(o.get_state()["mass"], b.mass)
 
 
+@pytest.mark.parametrize("skf", sorted(KERNELS))
+def test_boundary_kernel_gradient_is_derivative(oracle_mod, skf):
+    """bdwdx of each boundary kernel is the derivative of its bw
+    (boundary_kernel.f90): factor dW/dq against a central difference."""
+    p = _params(skf)
+    sh = KERNELS[skf][1]
+    bl = p.b_length
+    # (8 points: none on the piecewise kernels' knots q = 1, 2, where the
+    # single-precision literals of the cubic leave a 1e-8 step in bw)
+    for br in np.linspace(0.07, 0.93, 8) * bl:
+        e = 1e-6 * bl
+        num = (oracle_mod.boundary_w(p, br + e) - oracle_mod.boundary_w(p, br - e)) / (2 * e) * bl / sh
+        got = oracle_mod.boundary_fdwdq(p, br)
+        assert got == pytest.approx(num, rel=1e-5, abs=1e-7 * abs(oracle_mod.boundary_w(p, 0.0))), (skf, br)
+
+
+def _stepped(oracle_mod, b, nsteps=1, **kw):
+    p = b.params.copy()
+    for k, v in kw.items():
+        setattr(p, k, v)
+    o = oracle_mod.Oracle.from_basin(b, p)
+    o.step(nsteps)
+    return o.get_state()
+
+
+@pytest.mark.parametrize("int_algorithm", [1, 2, 3])
+def test_con_density_keeps_density_under_translation(oracle_mod, int_algorithm):
+    """con_density: a uniform velocity gives drho/dt = 0 exactly, whatever
+    the integrator (density.f90:107-165)."""
+    b = basins.make_basin(30, 2000.0, 5, walls="")
+    b.vx[:] = (0.3, -0.1)
+    st = _stepped(oracle_mod, b, 2, den_alg=2, int_algorithm=int_algorithm)
+    assert np.array_equal(st["rho"], b.rho)
+    assert not np.array_equal(st["x"], b.x)
+
+
+def _dilating(eps):
+    b = basins.make_basin(40, 2000.0, 9, walls="")
+    c = 0.5 * b.L
+    b.vx = np.ascontiguousarray(eps * (b.x - c))
+    inner = np.all(np.abs(b.x - c) < 0.3 * b.L, axis=1)
+    return b, inner
+
+
+@pytest.mark.parametrize("int_algorithm", [1, 2, 3])
+def test_con_density_uniform_dilatation(oracle_mod, int_algorithm):
+    """v = eps (x - c) has div v = 2 eps: away from the free edges the SPH
+    continuity equation gives drho/dt = -2 eps rho to the kernel's
+    discretisation error (a jittered lattice, cubic spline)."""
+    eps, dt = 1.0e-4, 1.0e-6
+    b, inner = _dilating(eps)
+    st = _stepped(oracle_mod, b, 1, den_alg=2, int_algorithm=int_algorithm, dt=dt)
+    ratio = ((st["rho"] - b.rho) / dt / (-2.0 * eps * b.rho))[inner]
+    assert np.all(np.abs(ratio - 1.0) < 0.05)          # (a 5% jitter of the lattice)
+    assert abs(np.mean(ratio) - 1.0) < 0.015
+
+
+def test_benz_hsml_follows_density(oracle_mod):
+    """Benz_hsml with con_density: dh/dt = -hsml drho/dt / (2 rho) = eps hsml
+    for the dilatation (smoothing_length.f90:82-94)."""
+    eps, dt = 1.0e-4, 1.0e-6
+    b, inner = _dilating(eps)
+    st = _stepped(oracle_mod, b, 1, den_alg=2, sle=1, int_algorithm=1, dt=dt)
+    ratio = ((st["hsml"] - b.hsml) / dt / (eps * b.hsml))[inner]
+    assert np.all(np.abs(ratio - 1.0) < 0.05)
+    assert abs(np.mean(ratio) - 1.0) < 0.015
+
+
+def test_benz_hsml_accumulates_without_con_density(oracle_mod):
+    """Without con_density, Benz_hsml adds each step's pair sum to drhodt,
+    which nothing clears (smoothing_length.f90:62-80): in a steady
+    dilatation the second step changes hsml about twice as much as the
+    first.  With con_density the two changes are about equal."""
+    eps, dt = 1.0e-4, 1.0e-6
+    b, inner = _dilating(eps)
+    for den_alg, ratio in ((3, 2.0), (2, 1.0)):
+        s1 = _stepped(oracle_mod, b, 1, den_alg=den_alg, sle=1, int_algorithm=1, dt=dt)
+        s2 = _stepped(oracle_mod, b, 2, den_alg=den_alg, sle=1, int_algorithm=1, dt=dt)
+        d1 = (s1["hsml"] - b.hsml)[inner]
+        d2 = (s2["hsml"] - s1["hsml"])[inner]
+        assert np.allclose(d2 / d1, ratio, rtol=0.01), den_alg
+
+
 def test_reference_default_literals():
     """Default-real literals of data_variables.f90 keep single precision."""
     p = reference_default()
