@@ -101,6 +101,44 @@ __global__ void k_set_time0(Scalars *sc, Inst *inst, double t) {
     inst[0].t = t;
 }
 
+// Extents and validity of an uploaded basin [off, off + n): per block
+// xmin, -xmax, ymin, -ymax, hmin, -hmax (all minima), and the counts of
+// non-positive hsml / rho / h and of non-finite positions.
+constexpr int kRedBlocks = 296;
+constexpr int kRedVals = 8;
+__global__ void __launch_bounds__(256) k_extents(int n, int off, State s, double *part) {
+    double v[kRedVals] = {INFINITY, INFINITY, INFINITY, INFINITY, INFINITY, INFINITY, 0.0, 0.0};
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int i = off + k;
+        const double x = s.x[i], y = s.y[i], hs = s.hs[i];
+        v[0] = fmin(v[0], x);
+        v[1] = fmin(v[1], -x);
+        v[2] = fmin(v[2], y);
+        v[3] = fmin(v[3], -y);
+        v[4] = fmin(v[4], hs);
+        v[5] = fmin(v[5], -hs);
+        if (!(hs > 0.0) || !(s.rho[i] > 0.0) || !(s.h[i] > 0.0)) v[6] += 1.0;
+        if (!isfinite(x) || !isfinite(y)) v[7] += 1.0;
+    }
+    __shared__ double red[kRedVals][8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < kRedVals; ++q) {
+        for (int o = 16; o > 0; o >>= 1) {
+            const double t = __shfl_xor_sync(0xffffffffu, v[q], o);
+            v[q] = (q < 6) ? fmin(v[q], t) : v[q] + t;
+        }
+        if (lane == 0) red[q][w] = v[q];
+    }
+    __syncthreads();
+    if (threadIdx.x < kRedVals) {
+        const int q = threadIdx.x;
+        double r = red[q][0];
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) r = (q < 6) ? fmin(r, red[q][k]) : r + red[q][k];
+        part[blockIdx.x * kRedVals + q] = r;
+    }
+}
+
 __global__ void k_grow_xabs(Scalars *sc, double xa) {
     atomicMax(&sc->xabs_bits, (unsigned long long)__double_as_longlong(xa));
 }
@@ -192,10 +230,11 @@ void free_all(simp_ctx *c) {
                     c->pair_j, c->pair_count, c->nbr_tmp, c->s0.hsf,
                     c->inst_dev, c->row_map, c->chunk_cnt, c->chunk_off, c->chunks, c->s0.xy, c->s0.vxy,
                     c->s0.pf, c->s0.mm, c->s0.hmm, c->s1.xy, c->s1.vxy, c->s1.pf, c->s1.mm, c->s1.hmm,
-                    c->tau_a, c->tau_b, c->tau_q, c->pair_dw, c->drhodt};
+                    c->tau_a, c->tau_b, c->tau_q, c->pair_dw, c->drhodt, c->red_dev};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->sc_host) cudaFreeHost(c->sc_host);
+    if (c->red_host) cudaFreeHost(c->red_host);
     if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
     for (cudaEvent_t e : c->prof_ev)
         if (e) cudaEventDestroy(e);
@@ -372,10 +411,11 @@ DueMask mask_of(int slot) {
     return m;
 }
 
-// Appends one basin's particles after the current ones and sorts it in.
-int add_instance(simp_ctx *c, int slot, const simp_forcing &f, int n, const double *x, const double *vx,
-                 const double *mass, const double *rho, const double *hsml, const double *A,
-                 const double *h, int nb, const double *xb, const double *massb, double t0) {
+// Uploads one basin's particles to [c->n, c->n + n) (nothing else changes
+// until add_instance takes them) and reduces their extents on the device.
+int stage_instance(simp_ctx *c, int n, const double *x, const double *vx, const double *mass,
+                   const double *rho, const double *hsml, const double *A, const double *h, int nb,
+                   const double *xb, const double *massb, Extents *e) {
     if (n < 1 || nb < 0 || !x || !vx || !mass || !rho || !hsml || !A || !h || (nb > 0 && (!xb || !massb)))
         return simp_fail(c, SIMP_ERR_BADARG, "bad sizes or null arrays");
     if (c->n + n > c->maxn)
@@ -388,18 +428,51 @@ int add_instance(simp_ctx *c, int slot, const simp_forcing &f, int n, const doub
                          "allowed. (boundaries.f90:296-303)");
     if (c->id_stride && n >= c->id_stride)
         return simp_fail(c, SIMP_ERR_BADARG, "a basin of a batch holds at most 2,097,151 particles");
-    double xmin = x[0], xmax = x[0], ymin = x[1], ymax = x[1], hmin = hsml[0], hmax = hsml[0];
-    for (int i = 0; i < n; ++i) {
-        xmin = std::min(xmin, x[2 * i]);
-        xmax = std::max(xmax, x[2 * i]);
-        ymin = std::min(ymin, x[2 * i + 1]);
-        ymax = std::max(ymax, x[2 * i + 1]);
-        hmin = std::min(hmin, hsml[i]);
-        hmax = std::max(hmax, hsml[i]);
-        if (!(hsml[i] > 0.0) || !(rho[i] > 0.0) || !(h[i] > 0.0))
-            return simp_fail(c, SIMP_ERR_BADARG, "hsml, rho and h must be positive");
-    }
+    cudaStream_t s = c->stream;
+    const int off = c->n;
+    const size_t N = (size_t)n;
+    double *stage = c->tmp;
+    SIMP_CUDA(c, cudaMemcpyAsync(stage, x, sizeof(double) * 2 * N, cudaMemcpyHostToDevice, s));
+    SIMP_CUDA(c, cudaMemcpyAsync(stage + 2 * N, vx, sizeof(double) * 2 * N, cudaMemcpyHostToDevice, s));
+    k_deinterleave<<<nblk(n, kB), kB, 0, s>>>(n, stage, c->s0.x + off, c->s0.y + off);
+    k_deinterleave<<<nblk(n, kB), kB, 0, s>>>(n, stage + 2 * N, c->s0.vx + off, c->s0.vy + off);
+    SIMP_CUDA(c, cudaMemcpyAsync(c->s0.m + off, mass, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    SIMP_CUDA(c, cudaMemcpyAsync(c->s0.rho + off, rho, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    SIMP_CUDA(c, cudaMemcpyAsync(c->s0.hs + off, hsml, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    SIMP_CUDA(c, cudaMemcpyAsync(c->s0.A + off, A, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    SIMP_CUDA(c, cudaMemcpyAsync(c->s0.h + off, h, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    const int rb = std::min(kRedBlocks, nblk(n, 256));
+    k_extents<<<rb, 256, 0, s>>>(n, off, c->s0, c->red_dev);
+    c->launches += 3;
+    SIMP_CUDA(c, cudaGetLastError());
+    SIMP_CUDA(c, cudaMemcpyAsync(c->red_host, c->red_dev, sizeof(double) * kRedVals * rb, cudaMemcpyDeviceToHost, s));
+    SIMP_CUDA(c, cudaStreamSynchronize(s));
+    double v[kRedVals] = {INFINITY, INFINITY, INFINITY, INFINITY, INFINITY, INFINITY, 0.0, 0.0};
+    for (int b = 0; b < rb; ++b)
+        for (int q = 0; q < kRedVals; ++q) {
+            const double t = c->red_host[b * kRedVals + q];
+            v[q] = (q < 6) ? std::min(v[q], t) : v[q] + t;
+        }
+    if (v[6] > 0.0) return simp_fail(c, SIMP_ERR_BADARG, "hsml, rho and h must be positive");
+    e->n = n;
+    e->xmin = v[0];
+    e->xmax = -v[1];
+    e->ymin = v[2];
+    e->ymax = -v[3];
+    e->hmin = v[4];
+    e->hmax = -v[5];
+    e->finite = v[7] == 0.0;
+    return SIMP_OK;
+}
+
+// Appends the staged basin after the current particles and sorts it in.
+int add_instance(simp_ctx *c, int slot, const simp_forcing &f, const Extents &e, int nb, const double *xb,
+                 const double *massb, double t0) {
+    const int n = e.n;
+    double xmin = e.xmin, xmax = e.xmax, ymin = e.ymin, ymax = e.ymax;
+    const double hmin = e.hmin, hmax = e.hmax;
     const double pxa = std::max(std::max(std::fabs(xmin), std::fabs(xmax)), std::max(std::fabs(ymin), std::fabs(ymax)));
+    if (!e.finite) return simp_fail(c, SIMP_ERR_BADARG, "non-finite positions");
     for (int b = 0; b < nb; ++b) {
         xmin = std::min(xmin, xb[2 * b]);
         xmax = std::max(xmax, xb[2 * b]);
@@ -434,24 +507,13 @@ int add_instance(simp_ctx *c, int slot, const simp_forcing &f, int n, const doub
     I.bs = 2.0 * hmin;
     I.dmax2_bits = 0ull;
     I.flags = 0;
-    // particle arrays at [off, off + n)
+    // particle arrays at [off, off + n), staged by stage_instance
     cudaStream_t s = c->stream;
     const int off = c->n;
-    const size_t N = (size_t)n;
-    double *stage = c->tmp;
-    SIMP_CUDA(c, cudaMemcpyAsync(stage, x, sizeof(double) * 2 * N, cudaMemcpyHostToDevice, s));
-    SIMP_CUDA(c, cudaMemcpyAsync(stage + 2 * N, vx, sizeof(double) * 2 * N, cudaMemcpyHostToDevice, s));
-    k_deinterleave<<<nblk(n, kB), kB, 0, s>>>(n, stage, c->s0.x + off, c->s0.y + off);
-    k_deinterleave<<<nblk(n, kB), kB, 0, s>>>(n, stage + 2 * N, c->s0.vx + off, c->s0.vy + off);
-    SIMP_CUDA(c, cudaMemcpyAsync(c->s0.m + off, mass, sizeof(double) * N, cudaMemcpyHostToDevice, s));
-    SIMP_CUDA(c, cudaMemcpyAsync(c->s0.rho + off, rho, sizeof(double) * N, cudaMemcpyHostToDevice, s));
-    SIMP_CUDA(c, cudaMemcpyAsync(c->s0.hs + off, hsml, sizeof(double) * N, cudaMemcpyHostToDevice, s));
-    SIMP_CUDA(c, cudaMemcpyAsync(c->s0.A + off, A, sizeof(double) * N, cudaMemcpyHostToDevice, s));
-    SIMP_CUDA(c, cudaMemcpyAsync(c->s0.h + off, h, sizeof(double) * N, cudaMemcpyHostToDevice, s));
     k_init_new<<<nblk(n, kB), kB, 0, s>>>(n, off, ih.id_base, slot, c->id, c->pinst, c->s0, c->xr, c->yr,
                                           c->nbr_count);
     k_grow_xabs<<<1, 1, 0, s>>>(c->sc, pxa);
-    c->launches += 4;
+    c->launches += 2;
     SIMP_CUDA(c, cudaGetLastError());
     c->n += n;
     // the new basin's keys come last: only its own range is sorted, and the
@@ -738,6 +800,9 @@ int create(const simp_params *params, int32_t maxn, int32_t maxnb, int32_t max_i
     TRY(dalloc(c, &c->binst, MB));
     TRY(dalloc(c, &c->bcell, MB));
     TRY(dalloc(c, &c->sc, 1));
+    TRY(dalloc(c, &c->red_dev, (size_t)kRedBlocks * kRedVals));
+    if (cudaMallocHost((void **)&c->red_host, sizeof(double) * kRedBlocks * kRedVals) != cudaSuccess)
+        return simp_fail(c, SIMP_ERR_NOMEM, "pinned host allocation failed");
     TRY(dalloc(c, &c->pair_cnt, M + 1));
     TRY(dalloc(c, &c->bpair_cnt, MB + 1));
     TRY(dalloc(c, &c->inst_dev, (size_t)max_inst));
@@ -978,18 +1043,18 @@ int32_t simp_gpu_set_state(simp_ctx *c, int32_t ntotal, const double *x, const d
                          "The number of boundary particles generated is higher than the maximum "
                          "allowed. (boundaries.f90:296-303)");
     if (ntotal < 1) return simp_fail(c, SIMP_ERR_BADARG, "set_state: bad sizes or null arrays");
-    double hmax = hsml[0];
-    for (int i = 0; i < ntotal; ++i) hmax = std::max(hmax, hsml[i]);
+    reset_all(c);
+    c->have_state = false;
+    Extents e{};
+    TRY(stage_instance(c, ntotal, x, vx, mass, rho, hsml, A, h, ntotalb, xb, massb, &e));
+    const double hmax = e.hmax, hmin = e.hmin;
     const double max_hsml = (c->prm.max_hsml > 0.0) ? c->prm.max_hsml : hmax * 10.0;  // initialize.f90:191
     c->phys = make_phys(c->prm, max_hsml);
-    reset_all(c);
     // global scalars of the run
     Scalars &sc = *c->sc_host;
     std::memset(&sc, 0, sizeof(Scalars));
     sc.dt = dt;
     sc.t = current_time;
-    double hmin = hsml[0];
-    for (int i = 0; i < ntotal; ++i) hmin = std::min(hmin, hsml[i]);
     sc.hmin = hmin;
     sc.hmax = hmax;
     sc.bs = 2.0 * hmin;
@@ -1002,9 +1067,7 @@ int32_t simp_gpu_set_state(simp_ctx *c, int32_t ntotal, const double *x, const d
     SIMP_CUDA(c, cudaMemcpyAsync(c->sc, c->sc_host, sizeof(Scalars), cudaMemcpyHostToDevice, c->stream));
     SIMP_CUDA(c, cudaMemsetAsync(c->inst_dev, 0, sizeof(Inst), c->stream));
     if (c->drhodt) SIMP_CUDA(c, cudaMemsetAsync(c->drhodt, 0, sizeof(double) * (size_t)c->maxn, c->stream));
-    c->have_state = false;
-    TRY(add_instance(c, 0, forcing_of(c->prm), ntotal, x, vx, mass, rho, hsml, A, h, ntotalb, xb, massb,
-                     current_time));
+    TRY(add_instance(c, 0, forcing_of(c->prm), e, ntotalb, xb, massb, current_time));
     c->have_state = true;
     return SIMP_OK;
 }
@@ -1019,17 +1082,18 @@ int32_t simp_gpu_batch_add(simp_ctx *c, const simp_forcing *forcing, int32_t nto
     for (int k = 0; k < c->max_inst; ++k)
         if (!c->insts[k].active) { q = k; break; }
     if (q < 0) return simp_fail(c, SIMP_ERR_MAXN, "no free slot in the batch");
+    Extents e{};
+    TRY(stage_instance(c, ntotal, x, vx, mass, rho, hsml, A, h, ntotalb, xb, massb, &e));
     if (!c->have_state) {
         // first basin: physics constants and the list skin
-        double hmax = 0.0;
-        for (int i = 0; i < ntotal && hsml; ++i) hmax = std::max(hmax, hsml[i]);
+        const double hmax = e.hmax;
         c->phys = make_phys(c->prm, c->prm.max_hsml > 0.0 ? c->prm.max_hsml : 10.0 * hmax);
         TRY(read_scalars(c));
         c->sc_host->skin = list_skin(c, hmax);
         c->sc_host->dt = c->prm.dt;
         SIMP_CUDA(c, cudaMemcpyAsync(c->sc, c->sc_host, sizeof(Scalars), cudaMemcpyHostToDevice, c->stream));
     }
-    TRY(add_instance(c, q, *forcing, ntotal, x, vx, mass, rho, hsml, A, h, ntotalb, xb, massb, 0.0));
+    TRY(add_instance(c, q, *forcing, e, ntotalb, xb, massb, 0.0));
     c->have_state = true;
     *slot = q;
     return SIMP_OK;

@@ -23,6 +23,13 @@ struct InstHost {
     std::vector<double> bn;        // their normals b_normal(2, nb) (bf_Wang), empty until set
 };
 
+// Extents of a basin staged for admission, reduced on the device.
+struct Extents {
+    int n;
+    double xmin, xmax, ymin, ymax, hmin, hmax;
+    bool finite;
+};
+
 struct simp_ctx {
     simp_params prm{};
     simp::Phys phys{};
@@ -47,6 +54,8 @@ struct simp_ctx {
     simp::State s0{}, s1{};
     double *mass1 = nullptr;       // half-step mass when the mass update is on
     double *drhodt = nullptr;      // Benz hsml without con_density: the reference's drhodt, kept across steps
+    double *red_dev = nullptr;     // per-block extents of a basin being admitted
+    double *red_host = nullptr;    // (pinned copy)
     double *xr = nullptr, *yr = nullptr;  // sort positions (updated when the instance is re-sorted)
     double *xl = nullptr, *yl = nullptr;  // positions where each Verlet list was built
     int *cell = nullptr;           // sort-time cell key per particle
