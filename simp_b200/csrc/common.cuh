@@ -227,10 +227,20 @@ __device__ __forceinline__ float klog(float v) { return logf(v); }
 constexpr double kLog2Real4 = 0.693147182464599609375;
 constexpr double kMarquis2C1 = 10.0, kMarquis2C2 = 50.0;   // kernel.f90:602-603
 
-template <class T, bool WANT_W>
+// Kernel choice of a pass: SKF when the pass is compiled for one kernel
+// (the cubic spline and the reference default, Wendland C6), else the
+// runtime switch (SKF = 0).
+template <int SKF>
+__host__ __device__ constexpr int skf_of(int runtime) { return SKF ? SKF : runtime; }
+// The kernels with their own compiled pair passes.
+__host__ __device__ constexpr int skf_compiled(int skf) {
+    return (skf == SIMP_SKF_CUBIC || skf == SIMP_SKF_WENDLAND_C6) ? skf : 0;
+}
+
+template <class T, bool WANT_W, int SKF = 0>
 __device__ __forceinline__ void kernel_wg(int skf, T q, T shh, T inv_h, T *w, T *gq) {
     const T s2 = shh * shh;
-    switch (skf) {
+    switch (skf_of<SKF>(skf)) {
         case SIMP_SKF_QUADRATIC: {   // kernel.f90:269-276
             const T f = (T)(2.0 / kPi) * s2;
             if (WANT_W) *w = f * fma(T(0.1875) * q, q, fma(T(-0.75), q, T(0.75)));
@@ -358,11 +368,12 @@ __device__ __forceinline__ double kernel_zero(const Phys &P, double hij) {
 // the boundary-pair index), for which the particle's own hsml stands here
 // (identical whenever hsml is uniform).  Cubic: b_Quadratic's form with the
 // cubic spline, support b_length, scale_h = 2.
+template <int SKF = 0>
 __device__ __forceinline__ double boundary_w(const Phys &P, double br, double hs_i) {
     const double sh = (double)P.scale_h;
     const double q = br / P.b_length * sh;
     const double shb = sh / P.b_length, s2 = shb * shb;
-    switch (P.skf) {
+    switch (skf_of<SKF>(P.skf)) {
         case SIMP_SKF_QUADRATIC:
             return (2.0 / kPi) * s2 * (0.1875 * q * q - 0.75 * q + 0.75);
         case SIMP_SKF_GAUSSIAN:
@@ -409,11 +420,12 @@ __device__ __forceinline__ double boundary_w(const Phys &P, double br, double hs
 // :422-423, b_Wendland_C6 :495-496; the cubic as its kernel's derivative).
 // The kernel gradient is then bdwdx = -(f dW/dq) / b_length * (bdx / br) *
 // scale_h, with bdx = xb - x_i.
+template <int SKF = 0>
 __device__ __forceinline__ double boundary_fdwdq(const Phys &P, double br, double hs_i) {
     const double sh = (double)P.scale_h;
     const double q = br / P.b_length * sh;
     const double shb = sh / P.b_length, s2 = shb * shb;
-    switch (P.skf) {
+    switch (skf_of<SKF>(P.skf)) {
         case SIMP_SKF_QUADRATIC:
             return (2.0 / kPi) * s2 * (0.375 * q - 0.75);
         case SIMP_SKF_GAUSSIAN:

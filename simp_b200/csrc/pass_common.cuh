@@ -87,7 +87,7 @@ struct PairGeom {
 // dx, dy: x_i - x_j (differences of the FP64 positions, rounded to T);
 // hi, inv_hi, hj: the smoothing lengths in T (the FP32 copies in the mixed
 // form).
-template <class T, bool WANT_W>
+template <class T, bool WANT_W, int SKF = 0>
 __device__ __forceinline__ PairGeom<T> pair_geom(const Phys &P, T dx, T dy, T hi, T inv_hi, T hj) {
     PairGeom<T> g;
     g.dx = dx;
@@ -100,7 +100,7 @@ __device__ __forceinline__ PairGeom<T> pair_geom(const Phys &P, T dx, T dy, T hi
     const T shh = sh * inv_h;
     const T q = r * shh;
     T gq, w = 0;
-    kernel_wg<T, WANT_W>(P.skf, q, shh, inv_h, &w, &gq);
+    kernel_wg<T, WANT_W, SKF>(P.skf, q, shh, inv_h, &w, &gq);
     if (WANT_W) g.w = w;
     g.gfac = gq * shh * rs;
     return g;
@@ -544,6 +544,7 @@ __device__ __forceinline__ void lists_block_done(const StressArgs &a) {
 // Called by every thread of the block (dead lanes with live = false).
 // `lists`: the Verlet-list implementation (displacement since the lists
 // were built, and the last block's rebuild decision).
+template <int SKF>
 __device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool live, int ki, const Inst &I,
                                               bool dead, double xi, double yi, double hi, int ci, double Sx,
                                               double Sy, double Tx, double Ty, int cnt, bool lists) {
@@ -572,13 +573,13 @@ __device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool l
                                  if (P.bfa == 1) {
                                      const double mb = a.bm[b];
                                      if (P.boundary_pressure) {
-                                         const double bw = boundary_w(P, d, hi);
+                                         const double bw = boundary_w<SKF>(P, d, hi);
                                          const double coef = P.kappa_n * bw * 2.0 * mb / ((mi + mb) * (d * d));
                                          fx += coef * bdx;
                                          fy += coef * bdy;
                                      }
                                      if (P.boundary_friction) {   // :85-100
-                                         const double t = boundary_fdwdq(P, d, hi) / bl;
+                                         const double t = boundary_fdwdq<SKF>(P, d, hi) / bl;
                                          const double bwx = -(t * (bdx / d) * sh), bwy = -(t * (bdy / d) * sh);
                                          const double v_r = vxi * bdx + vyi * bdy;
                                          const double pi_aj = P.kappa_t * csnd * v_r / d / rho;

@@ -14,13 +14,14 @@ namespace {
 using namespace pass;
 
 constexpr int kBlock = 128;
-// minimum resident blocks per SM (register caps 73 and 64): more warps in
-// flight to hide the latency of the neighbour gathers
+// minimum resident blocks per SM (register caps 102 and 73), measured at
+// cfg2 FP64 against 4..8: the kinematic pass keeps its pair math in
+// registers, the stress pass trades some for warps in flight
 #ifndef SIMP_KIN_MIN_BLOCKS
-#define SIMP_KIN_MIN_BLOCKS 7
+#define SIMP_KIN_MIN_BLOCKS 5
 #endif
 #ifndef SIMP_STRESS_MIN_BLOCKS
-#define SIMP_STRESS_MIN_BLOCKS 8
+#define SIMP_STRESS_MIN_BLOCKS 7
 #endif
 constexpr int kMinBlocksKin = SIMP_KIN_MIN_BLOCKS;
 constexpr int kMinBlocksStress = SIMP_STRESS_MIN_BLOCKS;
@@ -29,7 +30,7 @@ constexpr int kMinBlocksStress = SIMP_STRESS_MIN_BLOCKS;
 // the resident blocks comes out of the L1 cache that serves the gathers.
 constexpr int kGatherSlots = 24;
 
-template <class T>
+template <class T, int SKF>
 __global__ void __launch_bounds__(kBlock, kMinBlocksKin) k_kinematic(KinArgs a) {
     __shared__ int s_list[kGatherSlots * kBlock];
     const int t = threadIdx.x;
@@ -58,7 +59,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksKin) k_kinematic(KinArgs a) 
             if (done + k < kMaxPairs) a.pl.pj[(size_t)(done + k) * a.pl.stride + i] = j;
             const double2 q = s.xy[j], v = s.vxy[j];
             const KinNb<T> nb = Nb<T>::kin(s, j);
-            const PairGeom<T> pg = pair_geom<T, false>(P, (T)(xi - q.x), (T)(yi - q.y), hiT, inv_hiT, nb.h);
+            const PairGeom<T> pg = pair_geom<T, false, SKF>(P, (T)(xi - q.x), (T)(yi - q.y), hiT, inv_hiT, nb.h);
             const T dwx = pg.gfac * pg.dx, dwy = pg.gfac * pg.dy;
             if (dwr && done + k < kDwRows) dwr[(size_t)(done + k) * a.pl.stride + i] = Vec2<T>::make(dwx, dwy);
             ks.add(dwx, dwy, (T)(vxi - v.x), (T)(vyi - v.y), nb.m, nb.mor);
@@ -106,7 +107,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksKin) k_kinematic(KinArgs a) 
     kin_rheology(a, i, -ks.dv.get(), -ks.g1.get(), -ks.g2.get(), -ks.g3.get(), -ks.g4.get());
 }
 
-template <class T>
+template <class T, int SKF>
 __global__ void __launch_bounds__(kBlock, kMinBlocksStress) k_stress(StressArgs a) {
     const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
     const bool live = i0 < a.n;
@@ -124,7 +125,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksStress) k_stress(StressArgs 
     auto accumulate = [&](int j) {
         const double2 q = s.xy[j];
         const StressNb<T> nb = Nb<T>::stress(s, a.rec, j);
-        const PairGeom<T> pg = pair_geom<T, false>(P, (T)(xi - q.x), (T)(yi - q.y), hiT, inv_hiT, nb.h);
+        const PairGeom<T> pg = pair_geom<T, false, SKF>(P, (T)(xi - q.x), (T)(yi - q.y), hiT, inv_hiT, nb.h);
         ss.add(pg.gfac * pg.dx, pg.gfac * pg.dy, nb.m, nb.t11, nb.t12, nb.t22);
     };
     int cnt = a.pl.count[i];
@@ -152,8 +153,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksStress) k_stress(StressArgs 
             ++cnt;
         });
     }
-    stress_finish(a, i, live, ki, I, dead, xi, yi, hi, ci, ss.sx.get(), ss.sy.get(), ss.tx.get(), ss.ty.get(), cnt,
-                  true);
+    stress_finish<SKF>(a, i, live, ki, I, dead, xi, yi, hi, ci, ss.sx.get(), ss.sy.get(), ss.tx.get(), ss.ty.get(),
+                       cnt, true);
 }
 
 // Density rate drho/dt_i = sum_j m_j (v_i - v_j) . grad_i W_ij over the
@@ -390,10 +391,21 @@ void launch_kinematic(simp_ctx *c, const State &s, bool diag) {
         launch_kinematic_tiled(c, a);
         return;
     }
-    if (c->prm.precision == SIMP_PREC_MIXED)
-        k_kinematic<float><<<nblk(c->n, kBlock), kBlock, 0, c->stream>>>(a);
-    else
-        k_kinematic<double><<<nblk(c->n, kBlock), kBlock, 0, c->stream>>>(a);
+    const bool mixed = c->prm.precision == SIMP_PREC_MIXED;
+    const int g = nblk(c->n, kBlock);
+    switch (skf_compiled(c->prm.skf)) {
+        case SIMP_SKF_CUBIC:
+            if (mixed) k_kinematic<float, SIMP_SKF_CUBIC><<<g, kBlock, 0, c->stream>>>(a);
+            else k_kinematic<double, SIMP_SKF_CUBIC><<<g, kBlock, 0, c->stream>>>(a);
+            break;
+        case SIMP_SKF_WENDLAND_C6:
+            if (mixed) k_kinematic<float, SIMP_SKF_WENDLAND_C6><<<g, kBlock, 0, c->stream>>>(a);
+            else k_kinematic<double, SIMP_SKF_WENDLAND_C6><<<g, kBlock, 0, c->stream>>>(a);
+            break;
+        default:
+            if (mixed) k_kinematic<float, 0><<<g, kBlock, 0, c->stream>>>(a);
+            else k_kinematic<double, 0><<<g, kBlock, 0, c->stream>>>(a);
+    }
     c->launches += 1;
 }
 
@@ -434,10 +446,21 @@ void launch_stress(simp_ctx *c, const State &rhs, const State &base, EpiMode mod
         launch_stress_tiled(c, a);
         return;
     }
-    if (c->prm.precision == SIMP_PREC_MIXED)
-        k_stress<float><<<nblk(c->n, kBlock), kBlock, 0, c->stream>>>(a);
-    else
-        k_stress<double><<<nblk(c->n, kBlock), kBlock, 0, c->stream>>>(a);
+    const bool mixed = c->prm.precision == SIMP_PREC_MIXED;
+    const int g = nblk(c->n, kBlock);
+    switch (skf_compiled(c->prm.skf)) {
+        case SIMP_SKF_CUBIC:
+            if (mixed) k_stress<float, SIMP_SKF_CUBIC><<<g, kBlock, 0, c->stream>>>(a);
+            else k_stress<double, SIMP_SKF_CUBIC><<<g, kBlock, 0, c->stream>>>(a);
+            break;
+        case SIMP_SKF_WENDLAND_C6:
+            if (mixed) k_stress<float, SIMP_SKF_WENDLAND_C6><<<g, kBlock, 0, c->stream>>>(a);
+            else k_stress<double, SIMP_SKF_WENDLAND_C6><<<g, kBlock, 0, c->stream>>>(a);
+            break;
+        default:
+            if (mixed) k_stress<float, 0><<<g, kBlock, 0, c->stream>>>(a);
+            else k_stress<double, 0><<<g, kBlock, 0, c->stream>>>(a);
+    }
     c->launches += 1;
 }
 

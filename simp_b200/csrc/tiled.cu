@@ -167,7 +167,7 @@ __device__ __forceinline__ KinTile<T> kin_tile(unsigned char *base, int cap) {
 // rule applies): the exact FP64 test then runs with the pair math.
 constexpr unsigned short kExact = 0x8000;
 
-template <class T>
+template <class T, int SKF>
 __global__ void __launch_bounds__(kMaxTileThreads) k_kin_tiled(KinArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ Halo h;
@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(kMaxTileThreads) k_kin_tiled(KinArgs a) {
     // row: the pair's position in the particle's pair list (its kernel
     // gradient is kept for the stress pass when row < kDwRows)
     auto pair_terms = [&](int row, double xj, double yj, T hj, double vxj, double vyj, T mj, T mrj) {
-        const PairGeom<T> pg = pair_geom<T, false>(P, (T)(xi - xj), (T)(yi - yj), hiT, inv_hiT, hj);
+        const PairGeom<T> pg = pair_geom<T, false, SKF>(P, (T)(xi - xj), (T)(yi - yj), hiT, inv_hiT, hj);
         const T dwx = pg.gfac * pg.dx, dwy = pg.gfac * pg.dy;
         if (dwr && row < kDwRows) dwr[(size_t)row * pl.stride + i] = Vec2<T>::make(dwx, dwy);
         ks.add(dwx, dwy, (T)(vxi - vxj), (T)(vyi - vyj), mj, mrj);
@@ -383,7 +383,7 @@ __device__ __forceinline__ StressTile<T> stress_tile(unsigned char *base, int ca
     return t;
 }
 
-template <class T>
+template <class T, int SKF>
 __global__ void __launch_bounds__(kMaxTileThreads) k_stress_tiled(StressArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ Halo h;
@@ -423,7 +423,7 @@ __global__ void __launch_bounds__(kMaxTileThreads) k_stress_tiled(StressArgs a) 
     StressSums<T> ss;
     const T hiT = Nb<T>::h(s, i), inv_hiT = (T)inv_hi;
     auto terms = [&](double xj, double yj, T hj, T mj, T t11, T t12, T t22) {
-        const PairGeom<T> pg = pair_geom<T, false>(P, (T)(xi - xj), (T)(yi - yj), hiT, inv_hiT, hj);
+        const PairGeom<T> pg = pair_geom<T, false, SKF>(P, (T)(xi - xj), (T)(yi - yj), hiT, inv_hiT, hj);
         ss.add(pg.gfac * pg.dx, pg.gfac * pg.dy, mj, t11, t12, t22);
     };
     auto global_terms = [&](int j) {
@@ -468,7 +468,7 @@ __global__ void __launch_bounds__(kMaxTileThreads) k_stress_tiled(StressArgs a) 
             ++cnt;
         });
     }
-    stress_finish(a, i, live, ch.q, I, dead, xi, yi, hi, ci, ss.sx.get(), ss.sy.get(), ss.tx.get(), ss.ty.get(),
+    stress_finish<SKF>(a, i, live, ch.q, I, dead, xi, yi, hi, ci, ss.sx.get(), ss.sy.get(), ss.tx.get(), ss.ty.get(),
                   cnt, true);
 }
 
@@ -494,6 +494,37 @@ void build_chunks(simp_ctx *c) {
     c->launches += 2 + kScanKernels;
 }
 
+template <class T, int SKF>
+cudaError_t set_tile_smem(size_t kb, size_t sb) {
+    cudaError_t e = cudaFuncSetAttribute(k_kin_tiled<T, SKF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kb);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_stress_tiled<T, SKF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
+    return e;
+}
+
+template <class T, int SKF>
+void launch_tiled(simp_ctx *c, int pass, int grid, size_t sm, const KinArgs *ka, const StressArgs *sa) {
+    if (pass == 0) k_kin_tiled<T, SKF><<<grid, c->tile_threads, sm, c->stream>>>(*ka);
+    else k_stress_tiled<T, SKF><<<grid, c->tile_threads, sm, c->stream>>>(*sa);
+}
+
+void launch_tiled_any(simp_ctx *c, int pass, int grid, size_t sm, const KinArgs *ka, const StressArgs *sa) {
+    const bool mixed = c->prm.precision == SIMP_PREC_MIXED;
+    switch (skf_compiled(c->prm.skf)) {
+        case SIMP_SKF_CUBIC:
+            if (mixed) launch_tiled<float, SIMP_SKF_CUBIC>(c, pass, grid, sm, ka, sa);
+            else launch_tiled<double, SIMP_SKF_CUBIC>(c, pass, grid, sm, ka, sa);
+            break;
+        case SIMP_SKF_WENDLAND_C6:
+            if (mixed) launch_tiled<float, SIMP_SKF_WENDLAND_C6>(c, pass, grid, sm, ka, sa);
+            else launch_tiled<double, SIMP_SKF_WENDLAND_C6>(c, pass, grid, sm, ka, sa);
+            break;
+        default:
+            if (mixed) launch_tiled<float, 0>(c, pass, grid, sm, ka, sa);
+            else launch_tiled<double, 0>(c, pass, grid, sm, ka, sa);
+    }
+}
+
 size_t tiled_smem_bytes(int precision, int pass, int cap, int threads) {
     if (pass == 0)
         return precision == SIMP_PREC_MIXED ? kin_smem_bytes<float>(cap, threads)
@@ -505,14 +536,17 @@ int tiled_configure(simp_ctx *c) {
     const size_t kb = tiled_smem_bytes(c->prm.precision, 0, c->tile_cap, c->tile_threads);
     const size_t sb = tiled_smem_bytes(c->prm.precision, 1, c->tile_cap, c->tile_threads);
     cudaError_t e;
-    if (c->prm.precision == SIMP_PREC_MIXED) {
-        e = cudaFuncSetAttribute(k_kin_tiled<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kb);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_stress_tiled<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
-    } else {
-        e = cudaFuncSetAttribute(k_kin_tiled<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kb);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_stress_tiled<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
+    const bool mixed = c->prm.precision == SIMP_PREC_MIXED;
+    switch (skf_compiled(c->prm.skf)) {
+        case SIMP_SKF_CUBIC:
+            e = mixed ? set_tile_smem<float, SIMP_SKF_CUBIC>(kb, sb) : set_tile_smem<double, SIMP_SKF_CUBIC>(kb, sb);
+            break;
+        case SIMP_SKF_WENDLAND_C6:
+            e = mixed ? set_tile_smem<float, SIMP_SKF_WENDLAND_C6>(kb, sb)
+                      : set_tile_smem<double, SIMP_SKF_WENDLAND_C6>(kb, sb);
+            break;
+        default:
+            e = mixed ? set_tile_smem<float, 0>(kb, sb) : set_tile_smem<double, 0>(kb, sb);
     }
     if (e != cudaSuccess) return simp_cuda_check(c, e, "cudaFuncSetAttribute (tile shared memory)");
     return SIMP_OK;
@@ -525,10 +559,7 @@ void launch_kinematic_tiled(simp_ctx *c, const KinArgs &a0) {
     a.cap = c->tile_cap;
     const int grid = chunk_bound(c);
     const size_t sm = tiled_smem_bytes(c->prm.precision, 0, c->tile_cap, c->tile_threads);
-    if (c->prm.precision == SIMP_PREC_MIXED)
-        k_kin_tiled<float><<<grid, c->tile_threads, sm, c->stream>>>(a);
-    else
-        k_kin_tiled<double><<<grid, c->tile_threads, sm, c->stream>>>(a);
+    launch_tiled_any(c, 0, grid, sm, &a, nullptr);
     c->launches += 1;
 }
 
@@ -539,10 +570,7 @@ void launch_stress_tiled(simp_ctx *c, const StressArgs &a0) {
     a.cap = c->tile_cap;
     const int grid = chunk_bound(c);
     const size_t sm = tiled_smem_bytes(c->prm.precision, 1, c->tile_cap, c->tile_threads);
-    if (c->prm.precision == SIMP_PREC_MIXED)
-        k_stress_tiled<float><<<grid, c->tile_threads, sm, c->stream>>>(a);
-    else
-        k_stress_tiled<double><<<grid, c->tile_threads, sm, c->stream>>>(a);
+    launch_tiled_any(c, 1, grid, sm, nullptr, &a);
     c->launches += 1;
 }
 
