@@ -14,24 +14,37 @@ namespace {
 using namespace pass;
 
 constexpr int kBlock = 128;
-// minimum resident blocks per SM (register caps 102 and 73), measured at
-// cfg2 FP64 against 4..8: the kinematic pass keeps its pair math in
-// registers, the stress pass trades some for warps in flight
+// minimum resident blocks per SM, per precision form, measured against 4..8
+// (cfg2 FP64, cfg3 mixed): the FP64 kinematic pass keeps its pair math in
+// registers (cap 102), the FP32 passes and the FP64 stress pass trade
+// registers for warps in flight (caps 64 and 73)
 #ifndef SIMP_KIN_MIN_BLOCKS
 #define SIMP_KIN_MIN_BLOCKS 5
 #endif
 #ifndef SIMP_STRESS_MIN_BLOCKS
 #define SIMP_STRESS_MIN_BLOCKS 7
 #endif
-constexpr int kMinBlocksKin = SIMP_KIN_MIN_BLOCKS;
-constexpr int kMinBlocksStress = SIMP_STRESS_MIN_BLOCKS;
+#ifndef SIMP_KIN_MIN_BLOCKS_F32
+#define SIMP_KIN_MIN_BLOCKS_F32 8
+#endif
+#ifndef SIMP_STRESS_MIN_BLOCKS_F32
+#define SIMP_STRESS_MIN_BLOCKS_F32 8
+#endif
+template <class T>
+struct MinBlocks {
+    static constexpr int kin = SIMP_KIN_MIN_BLOCKS, stress = SIMP_STRESS_MIN_BLOCKS;
+};
+template <>
+struct MinBlocks<float> {
+    static constexpr int kin = SIMP_KIN_MIN_BLOCKS_F32, stress = SIMP_STRESS_MIN_BLOCKS_F32;
+};
 // per-thread pair list in shared memory: a typical particle's pairs fit;
 // a longer list is processed in batches.  Kept small: the shared memory of
 // the resident blocks comes out of the L1 cache that serves the gathers.
 constexpr int kGatherSlots = 24;
 
 template <class T, int SKF>
-__global__ void __launch_bounds__(kBlock, kMinBlocksKin) k_kinematic(KinArgs a) {
+__global__ void __launch_bounds__(kBlock, MinBlocks<T>::kin) k_kinematic(KinArgs a) {
     __shared__ int s_list[kGatherSlots * kBlock];
     const int t = threadIdx.x;
     const int i = blockIdx.x * blockDim.x + t;
@@ -108,7 +121,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksKin) k_kinematic(KinArgs a) 
 }
 
 template <class T, int SKF>
-__global__ void __launch_bounds__(kBlock, kMinBlocksStress) k_stress(StressArgs a) {
+__global__ void __launch_bounds__(kBlock, MinBlocks<T>::stress) k_stress(StressArgs a) {
     const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
     const bool live = i0 < a.n;
     const int i = live ? i0 : a.n - 1;   // dead lanes mirror the last particle for warp reductions
