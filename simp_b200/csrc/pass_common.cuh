@@ -139,24 +139,26 @@ __device__ __forceinline__ PairCtx pair_ctx(const State &s, const Scalars *sc, c
 
 // The reference criterion for candidate j, decided exactly: FP32 prefilter,
 // the FP64 test of nnps.f90:277-281 when undecided, then the bucket rule.
-__device__ __forceinline__ bool is_pair(const State &s, const PairCtx &p, int j) {
+// (f: candidate j's packed FP32 copy, already loaded; read when p.use_f32)
+__device__ __forceinline__ bool is_pair_with(const State &s, const PairCtx &p, int j, float4 f) {
     int dec = 2;
-    if (p.use_f32) {
-        const float4 f = s.pf[j];
-        dec = prefilter(p.xif - f.x, p.yif - f.y, 0.5f * (p.hif + f.z), p.margin);
-    }
+    if (p.use_f32) dec = prefilter(p.xif - f.x, p.yif - f.y, 0.5f * (p.hif + f.z), p.margin);
     if (dec == 0) return false;
     if (dec == 2 || p.br.on) {
-        const double2 q = s.xy[j];
+        const double2 q = __ldg(&s.xy[j]);
         const double xj = q.x, yj = q.y;
         if (dec == 2) {
             double r;
-            const double mh = __dmul_rn(__dadd_rn(p.hi, s.hs[j]), 0.5);
+            const double mh = __dmul_rn(__dadd_rn(p.hi, __ldg(&s.hs[j])), 0.5);
             if (!pair_test(__dsub_rn(p.xi, xj), __dsub_rn(p.yi, yj), mh, &r)) return false;
         }
         if (!bin_rule_ok(p.br, xj, yj)) return false;
     }
     return true;
+}
+
+__device__ __forceinline__ bool is_pair(const State &s, const PairCtx &p, int j) {
+    return is_pair_with(s, p, j, p.use_f32 ? __ldg(&s.pf[j]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f));
 }
 
 // Visits the cell-stencil candidates of particle i (cell order).
@@ -183,11 +185,48 @@ __device__ __forceinline__ void for_each_current_pair(const State &s, const NbrL
     const bool valid = (own + all) * (1.0 + 1e-9) < sc->skin;
     if (cnt >= 0 && cnt <= kMaxNbr && valid) {
         for (int k = 0; k < cnt; ++k) {
-            const int j = nl.nbr[(size_t)k * nl.stride + i];
+            const int j = __ldg(&nl.nbr[(size_t)k * nl.stride + i]);
             if (is_pair(s, p, j)) on_pair(j);
         }
     } else {
         for_stencil(p.g, i, ci, stencil_radius(p.hmax, p.dmax2_bits, p.g, 0.0), [&](int j) {
+            if (is_pair(s, p, j)) on_pair(j);
+        });
+    }
+}
+
+// The same, with the list candidates taken kBatch at a time: their list
+// entries, then their FP32 copies are loaded together, so one wait covers a
+// whole batch.  before_batch() runs ahead of each batch (at most kBatch
+// pairs follow it) and ahead of each stencil candidate.
+constexpr int kBatch = 4;
+template <class B, class F>
+__device__ __forceinline__ void for_each_current_pair_batched(const State &s, const NbrList &nl, const Scalars *sc,
+                                                              int i, int ci, const PairCtx &p, B &&before_batch,
+                                                              F &&on_pair) {
+    const int cnt = nl.count[i];
+    const double dxl = p.xi - nl.xl[i], dyl = p.yi - nl.yl[i];
+    const double own = sqrt(dxl * dxl + dyl * dyl);
+    const double all = sqrt(bitsd(sc->dlist2_bits));
+    const bool valid = (own + all) * (1.0 + 1e-9) < sc->skin;
+    if (cnt >= 0 && cnt <= kMaxNbr && valid) {
+        for (int k0 = 0; k0 < cnt; k0 += kBatch) {
+            before_batch();
+            int jj[kBatch];
+            float4 ff[kBatch];
+#pragma unroll
+            for (int u = 0; u < kBatch; ++u)
+                jj[u] = (k0 + u < cnt) ? __ldg(&nl.nbr[(size_t)(k0 + u) * nl.stride + i]) : -1;
+#pragma unroll
+            for (int u = 0; u < kBatch; ++u)
+                ff[u] = (jj[u] >= 0 && p.use_f32) ? __ldg(&s.pf[jj[u]]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+#pragma unroll
+            for (int u = 0; u < kBatch; ++u)
+                if (jj[u] >= 0 && is_pair_with(s, p, jj[u], ff[u])) on_pair(jj[u]);
+        }
+    } else {
+        for_stencil(p.g, i, ci, stencil_radius(p.hmax, p.dmax2_bits, p.g, 0.0), [&](int j) {
+            before_batch();
             if (is_pair(s, p, j)) on_pair(j);
         });
     }
@@ -216,15 +255,15 @@ template <>
 struct Nb<double> {
     static __device__ __forceinline__ double h(const State &s, int j) { return s.hs[j]; }
     static __device__ __forceinline__ KinNb<double> kin(const State &s, int j) {
-        const double2 q = s.mm[j];
-        return {s.hs[j], q.x, q.y};
+        const double2 q = __ldg(&s.mm[j]);
+        return {__ldg(&s.hs[j]), q.x, q.y};
     }
     static __device__ __forceinline__ StressNb<double> stress(const State &s, const TauRec &t, int j) {
-        const double2 a = t.ta[j], b = t.tb[j];
-        return {s.hs[j], b.y, a.x, a.y, b.x};
+        const double2 a = __ldg(&t.ta[j]), b = __ldg(&t.tb[j]);
+        return {__ldg(&s.hs[j]), b.y, a.x, a.y, b.x};
     }
     static __device__ __forceinline__ StressNb<double> stress_rec(const TauRec &t, int j) {
-        const double2 a = t.ta[j], b = t.tb[j];
+        const double2 a = __ldg(&t.ta[j]), b = __ldg(&t.tb[j]);
         return {0.0, b.y, a.x, a.y, b.x};
     }
 };
@@ -232,15 +271,15 @@ template <>
 struct Nb<float> {
     static __device__ __forceinline__ float h(const State &s, int j) { return s.hsf[j]; }
     static __device__ __forceinline__ KinNb<float> kin(const State &s, int j) {
-        const float4 q = s.hmm[j];
+        const float4 q = __ldg(&s.hmm[j]);
         return {q.x, q.y, q.z};
     }
     static __device__ __forceinline__ StressNb<float> stress(const State &s, const TauRec &t, int j) {
-        const float4 q = t.tq[j];
-        return {s.hsf[j], q.w, q.x, q.y, q.z};
+        const float4 q = __ldg(&t.tq[j]);
+        return {__ldg(&s.hsf[j]), q.w, q.x, q.y, q.z};
     }
     static __device__ __forceinline__ StressNb<float> stress_rec(const TauRec &t, int j) {
-        const float4 q = t.tq[j];
+        const float4 q = __ldg(&t.tq[j]);
         return {0.0f, q.w, q.x, q.y, q.z};
     }
 };

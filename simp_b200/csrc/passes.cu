@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<T>::kin) k_kinematic(KinArgs
         for (int k = 0; k < cnt; ++k) {
             const int j = s_list[k * kBlock + t];
             if (done + k < kMaxPairs) a.pl.pj[(size_t)(done + k) * a.pl.stride + i] = j;
-            const double2 q = s.xy[j], v = s.vxy[j];
+            const double2 q = __ldg(&s.xy[j]), v = __ldg(&s.vxy[j]);
             const KinNb<T> nb = Nb<T>::kin(s, j);
             const PairGeom<T> pg = pair_geom<T, false, SKF>(P, (T)(xi - q.x), (T)(yi - q.y), hiT, inv_hiT, nb.h);
             const T dwx = pg.gfac * pg.dx, dwy = pg.gfac * pg.dy;
@@ -113,7 +113,14 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<T>::kin) k_kinematic(KinArgs
         a.nl.xl[i] = xi;
         a.nl.yl[i] = yi;
     } else {
-        for_each_current_pair(s, a.nl, a.sc, i, a.cell[i], pc, on_pair);
+        // (room for a whole batch in the list before each batch)
+        for_each_current_pair_batched(s, a.nl, a.sc, i, a.cell[i], pc, [&]() {
+            if (cnt > kGatherSlots - kBatch) flush();
+        }, [&](int j) {
+            s_list[cnt * kBlock + t] = j;
+            ++npairs;
+            ++cnt;
+        });
     }
     flush();   // (also writes the stress pass's pair list, a coalesced row per k)
     a.pl.count[i] = npairs;
@@ -136,7 +143,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<T>::stress) k_stress(StressA
     StressSums<T> ss;
     const T hiT = Nb<T>::h(s, i), inv_hiT = (T)inv_hi;
     auto accumulate = [&](int j) {
-        const double2 q = s.xy[j];
+        const double2 q = __ldg(&s.xy[j]);
         const StressNb<T> nb = Nb<T>::stress(s, a.rec, j);
         const PairGeom<T> pg = pair_geom<T, false, SKF>(P, (T)(xi - q.x), (T)(yi - q.y), hiT, inv_hiT, nb.h);
         ss.add(pg.gfac * pg.dx, pg.gfac * pg.dy, nb.m, nb.t11, nb.t12, nb.t22);
@@ -148,14 +155,14 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<T>::stress) k_stress(StressA
 #pragma unroll 4
         for (int k = 0; k < cnt; ++k) {
             const size_t r = (size_t)k * a.pl.stride + i;
-            const typename Vec2<T>::type g = dwr[r];
-            const StressNb<T> nb = Nb<T>::stress_rec(a.rec, a.pl.pj[r]);
+            const typename Vec2<T>::type g = __ldg(&dwr[r]);
+            const StressNb<T> nb = Nb<T>::stress_rec(a.rec, __ldg(&a.pl.pj[r]));
             ss.add(g.x, g.y, nb.m, nb.t11, nb.t12, nb.t22);
         }
     } else if (cnt <= kMaxPairs) {
         // the kinematic pass of this right-hand side found the pairs
 #pragma unroll 4
-        for (int k = 0; k < cnt; ++k) accumulate(a.pl.pj[(size_t)k * a.pl.stride + i]);
+        for (int k = 0; k < cnt; ++k) accumulate(__ldg(&a.pl.pj[(size_t)k * a.pl.stride + i]));
     } else if (dead) {
         cnt = 0;
     } else {
