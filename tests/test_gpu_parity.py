@@ -222,6 +222,30 @@ def test_trajectory_fast_motion_rebuilds(gpu_lib, oracle_mod):
         assert_same_pairs(g.nnps(), o.nnps())
 
 
+def test_few_fast_particles_cross_the_lists(gpu_lib, oracle_mod):
+    """Nine particles at 30 m/s through a basin at rest: they leave the
+    Verlet skin (480 m) within a few steps while every other particle stays
+    put; the lists are rebuilt in time and every pair is still found."""
+    b = basins.cfg1()
+    b.vx = np.zeros_like(b.vx)
+    c = np.argsort(np.hypot(b.x[:, 0] - 0.5 * b.L, b.x[:, 1] - 0.5 * b.L))[:9]
+    b.vx[c] = (30.0, 12.0)
+    prm = b.params.copy()
+    prm.dt = 5.0
+    g, o = _pair(b, oracle_mod, prm)
+    for _ in range(3):
+        g.time_integration(4)
+        o.step(4)
+        sg, so = g.get_state(), o.get_state()
+        for k in ("x", "vx", "h"):
+            ref = b.x if k == "x" else 0.0
+            assert rel_l2(sg[k] - ref, so[k] - ref) < TOL_TRAJ_20, (k, rel_l2(sg[k] - ref, so[k] - ref))
+        o.set_state(sg["x"], sg["vx"], sg["mass"], sg["rho"], sg["hsml"], sg["A"], sg["h"],
+                    b.xb, b.massb, prm.dt, sg["current_time"])
+        assert_same_pairs(g.nnps(), o.nnps())
+    assert np.max(np.hypot(*(sg["x"][c] - b.x[c]).T)) > 480.0      # past the skin
+
+
 def test_trajectory_vp_timestep_and_marquis_hsml(gpu_lib, oracle_mod):
     """Reference default switches: sle = 2 (Marquis hsml), tse = 2 (VP dt),
     Wendland C6, mass from the lattice."""
