@@ -374,6 +374,7 @@ def run_forms(args, which):
             "particle_steps": sst["particle_steps"], "peak_resident_requests": sst["peak_resident_requests"],
             "peak_resident_particles": sst["peak_resident_particles"],
             "serial_fp64": ser, "speedup_vs_serial_fp64": served_value / ser["value"],
+            "time_split_s": {k: sst[k] for k in ("admit_s", "step_s", "retire_s") if k in sst},
             "spot_checks": spots}
     return out
 

@@ -83,7 +83,8 @@ typedef struct simp_params {
     int32_t nnps_algorithm;    /* 2 bucket search, 1 direct find (nnps.f90:21-30)       */
     int32_t sle;               /* 0 keep hsml, 1 Benz hsml, 2 Marquis hsml
                                   (smoothing_length.f90:24-30)                          */
-    int32_t tse;               /* 0 keep dt, 2 VP criterion (time_step.f90:132-157)     */
+    int32_t tse;               /* 0 keep dt, 1 Monaghan (time_step.f90:40-103, without
+                                  artificial viscosity), 2 VP criterion (:132-157)     */
     int32_t rheology;          /* 1 elliptical yield curve, 2 Mohr-Coulomb
                                   (bulk_viscosity.f90, shear_viscosity.f90)           */
     int32_t eos_alg;           /* 1 Hibler, 2 Gutfraind, 3 Kreyscher (eos.f90)         */

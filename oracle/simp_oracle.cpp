@@ -776,7 +776,7 @@ void density(Orc &o) {
 // sound_speed.f90:20-27 with c_yang :54-55: only when something reads c.
 void sound_speed(Orc &o) {
     const simp_params &P = o.P;
-    if (!P.boundary_friction) return;   // (artificial_visc is off; tse = 1 is not a path here)
+    if (!P.boundary_friction && P.tse != 1) return;   // (artificial_visc is off)
     for (int i = 0; i < o.ntotal; ++i)
         o.c[i] = std::pow(P.Y * (1 - P.nu) / (o.rho[i] * (1 + P.nu) * (1 - 2 * P.nu)), 0.5);
 }
@@ -821,8 +821,26 @@ void smoothing_length(Orc &o) {
     }
 }
 
+// time_step.f90:40-103 (Monaghan_time_step, artificial_visc off): the
+// force criterion from the last right-hand side's accelerations and the
+// CFL criterion from the sound speed.
+void monaghan_time_step(Orc &o) {
+    const int n = o.ntotal;
+    const double fF = 0.25;
+    double mf = 0.0, mc = 0.0;
+    for (int i = 0; i < n; ++i) {
+        const double acc = std::pow(p2(o.dvxdt[2 * i]) + p2(o.dvxdt[2 * i + 1]), 0.5);
+        const double a = o.hsml[i] / acc, c = o.hsml[i] / o.c[i];
+        mf = (i == 0) ? a : std::min(mf, a);
+        mc = (i == 0) ? c : std::min(mc, c);
+    }
+    const double dt_force = fF * std::pow(mf, 0.5);
+    o.dt = std::min(dt_force, mc);
+}
+
 // time_step.f90:132-157 (VP_time_step); tse = 0 keeps dt.
 void time_step(Orc &o) {
+    if (o.P.tse == 1) { monaghan_time_step(o); return; }
     if (o.P.tse != 2) return;
     double m = 0.0;
     for (int i = 0; i < o.ntotal; ++i) {

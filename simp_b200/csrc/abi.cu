@@ -196,7 +196,7 @@ int check_params(simp_ctx *c, const simp_params &p, bool batch) {
     if (p.int_algorithm < 1 || p.int_algorithm > 3) return bad("int_algorithm (1 Euler, 2 predictor-corrector, 3 leap-frog)");
     if (p.nnps_algorithm != 1 && p.nnps_algorithm != 2) return bad("nnps_algorithm (1 or 2)");
     if (p.sle < 0 || p.sle > 2) return bad("sle (0, 1 or 2)");
-    if (p.tse != 0 && p.tse != 2) return bad("tse (0 or 2)");
+    if (p.tse < 0 || p.tse > 2) return bad("tse (0 fixed, 1 Monaghan, 2 viscous-plastic)");
     if (p.rheology != 1 && p.rheology != 2) return bad("rheology (1 elliptical, 2 Mohr-Coulomb)");
     if (p.eos_alg < 1 || p.eos_alg > 3) return bad("eos_alg (1, 2 or 3)");
     if (p.pa_sph != 1 && p.pa_sph != 2) return bad("pa_sph (1 or 2)");

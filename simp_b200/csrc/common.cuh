@@ -472,6 +472,20 @@ __device__ __forceinline__ double sound_speed(const Phys &P, double rho) {
     return sqrt(P.Y * (1.0 - P.nu) / (rho * (1.0 + P.nu) * (1.0 - 2.0 * P.nu)));
 }
 
+// Time-step candidate of one particle (time_step.f90:132-157 VP_time_step;
+// :40-103 Monaghan_time_step without artificial viscosity, whose
+// dt = min(0.25 sqrt(min hsml / |a|), min hsml / c) is the min over the
+// particles of min(0.25 sqrt(hsml / |a|), hsml / c), sqrt being monotone).
+// hs: the new hsml, a2: |dv/dt|^2 of the last right-hand side, rho: the new
+// density (c_yang is refreshed from it before time_step).
+__device__ __forceinline__ double dt_candidate(const Phys &P, double hs, double a2, double rho) {
+    if (P.tse == 2) return P.rho_ice * (hs * hs) * P.delta_min / (P.P_star * (1.0 + P.k_t));
+    const double acc = sqrt(a2);
+    const double f = 0.25 * sqrt(hs / acc);
+    const double cfl = hs / sound_speed(P, rho);
+    return f < cfl ? f : cfl;
+}
+
 // Wind at a particle of an instance: uniform (the reference hard-codes one,
 // wind_forcing.f90:36-37) or a cyclonic vortex
 // U(r) = Umax (r/R) exp((1 - r^2/R^2)/2), counter-clockwise.

@@ -808,10 +808,11 @@ __device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool l
             v[4] = dbits(hsn);
         }
     }
-    if (corr && P.tse == 2) {                                   // time_step.f90:155
+    if (corr && P.tse != 0) {                                   // time_step.f90:20-26
         active |= 32u;
-        if (live) v[5] = dbits(P.rho_ice * (hsn * hsn) * P.delta_min / (P.P_star * (1.0 + P.k_t)));
+        if (live) v[5] = dbits(dt_candidate(P, hsn, ax * ax + ay * ay, rhon));
     }
+    if (tail_later && P.tse == 1 && live) a.rates[i] = ax * ax + ay * ay;   // for k_density_rate
     block_bounds(a.sc, active, v);
     if (lists) lists_block_done(a);
 }

@@ -196,6 +196,7 @@ struct DensArgs {
     const double *mj;    // neighbour masses of the sum
     const double *rho1;  // step-start density
     double *acc;         // Benz's drhodt when den_alg != 2 (kept across steps)
+    const double *a2;    // |dv/dt|^2 of the last right-hand side (tse = 1)
     double *hs_next;
     PairList pl;
     const int *cell_start, *cell, *pinst;
@@ -278,9 +279,9 @@ __global__ void __launch_bounds__(kBlock) k_density_rate(DensArgs a) {
             v[4] = dbits(hsn);
         }
     }
-    if (P.tse == 2) {                                          // time_step.f90:155
+    if (P.tse != 0) {                                          // time_step.f90:20-26
         active |= 32u;
-        if (live) v[5] = dbits(P.rho_ice * (hsn * hsn) * P.delta_min / (P.P_star * (1.0 + P.k_t)));
+        if (live) v[5] = dbits(dt_candidate(P, hsn, P.tse == 1 ? a.a2[i] : 0.0, rhon));
     }
     block_bounds(a.sc, active, v);
 }
@@ -307,7 +308,7 @@ __global__ void __launch_bounds__(kFinishThreads) k_step_finish(Scalars *sc, Ins
                                                                 int sle) {
     __shared__ double dt;
     if (threadIdx.x == 0) {
-        if (tse == 2) {
+        if (tse != 0) {
             sc->dt = bitsd(sc->acc_dt);
             sc->acc_dt = dbits(INFINITY);
         }
@@ -491,6 +492,7 @@ void launch_density_rate(simp_ctx *c, const State &g, const State &v, int rho_up
     a.rho1 = c->s0.rho;
     a.acc = c->drhodt;
     a.mj = c->drhodt ? v.m : g.m;
+    a.a2 = c->rates;
     a.hs_next = c->tmp;
     a.pl = pair_list(c);
     a.cell_start = c->cell_start;

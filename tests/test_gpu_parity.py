@@ -296,6 +296,9 @@ VARIANTS = {
     "benz_con_density": dict(sle=1, den_alg=2, tse=2),
     "benz_con_density_euler": dict(sle=1, den_alg=2, int_algorithm=1),
     "benz_mass_from_area": dict(sle=1, mass_from_area=1),
+    # Monaghan time step (time_step.f90:40-103): force and CFL criteria
+    "monaghan_dt": dict(tse=1),
+    "monaghan_dt_benz_euler": dict(tse=1, sle=1, int_algorithm=1),
     # Marquis hsml from the continuity density (after the density pass)
     "marquis_con_density": dict(sle=2, den_alg=2),
     "marquis_con_density_leapfrog": dict(sle=2, den_alg=2, int_algorithm=3),

@@ -244,6 +244,20 @@ def test_benz_hsml_accumulates_without_con_density(oracle_mod):
         assert np.allclose(d2 / d1, ratio, rtol=0.01), den_alg
 
 
+def test_monaghan_time_step_is_cfl_at_rest(oracle_mod):
+    """With no acceleration the force criterion is infinite and the time
+    step is min(hsml / c), c = (Y (1 - nu) / (rho (1 + nu) (1 - 2 nu)))^0.5
+    (time_step.f90:40-103, sound_speed.f90:54-55)."""
+    b = basins.make_basin(20, 2000.0, 3, walls="", wind=(0.0, 0.0))
+    p = b.params.copy()
+    p.tse = 1
+    o = oracle_mod.Oracle.from_basin(b, p)
+    o.step(1)
+    Y, nu = p.Y, p.nu
+    c = np.sqrt(Y * (1 - nu) / (b.rho * (1 + nu) * (1 - 2 * nu)))
+    assert o.get_state()["dt"] == pytest.approx(np.min(b.hsml / c), rel=1e-12)
+
+
 def test_reference_default_literals():
     """Default-real literals of data_variables.f90 keep single precision."""
     p = reference_default()
