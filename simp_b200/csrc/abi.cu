@@ -139,6 +139,12 @@ __global__ void __launch_bounds__(256) k_extents(int n, int off, State s, double
     }
 }
 
+// Wall particles per cell key (for their cell-start offsets).
+__global__ void k_count_walls(int nb, const int *__restrict__ key, int *__restrict__ cnt) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nb) atomicAdd(&cnt[key[k]], 1);
+}
+
 __global__ void k_grow_xabs(Scalars *sc, double xa) {
     atomicMax(&sc->xabs_bits, (unsigned long long)__double_as_longlong(xa));
 }
@@ -310,19 +316,24 @@ int layout(simp_ctx *c) {
     c->ninst = std::max(top, 1);
     const size_t need = (size_t)base + 2;
     if (need > c->cell_cap) {
+        // (grown at least twofold, from a reserve of maxn / 8 cells: a
+        // batch that admits basin after basin reallocates rarely; cudaFree
+        // waits for the device)
         cudaFree(c->cell_start);
         cudaFree(c->cnt);
         cudaFree(c->bcell_start);
-        cudaFree(c->scan_tmp);
         c->cell_start = c->cnt = c->bcell_start = nullptr;
-        c->scan_tmp = nullptr;
-        const size_t capn = need + need / 4;
+        const size_t capn = std::max(2 * need, std::max(2 * c->cell_cap, (size_t)c->maxn / 8 + 4096));
         TRY(dalloc(c, &c->cell_start, capn));
         TRY(dalloc(c, &c->cnt, capn));
         TRY(dalloc(c, &c->bcell_start, capn));
         const size_t sb = scan_tmp_bytes((int)std::max<size_t>(capn, (size_t)std::max(c->maxn, c->maxnb) + 1));
-        if (cudaMalloc(&c->scan_tmp, sb) != cudaSuccess) return simp_fail(c, SIMP_ERR_NOMEM, "device allocation failed");
-        c->scan_tmp_bytes = sb;
+        if (sb > c->scan_tmp_bytes) {
+            cudaFree(c->scan_tmp);
+            c->scan_tmp = nullptr;
+            if (cudaMalloc(&c->scan_tmp, sb) != cudaSuccess) return simp_fail(c, SIMP_ERR_NOMEM, "device allocation failed");
+            c->scan_tmp_bytes = sb;
+        }
         c->cell_cap = capn;
     }
     // cell rows of all instances, for the chunks of the tiled passes
@@ -339,7 +350,7 @@ int layout(simp_ctx *c) {
         c->row_map = nullptr;
         c->chunk_cnt = c->chunk_off = nullptr;
         c->chunks = nullptr;
-        const size_t rcap = rows.size() + rows.size() / 4 + 2;
+        const size_t rcap = std::max(2 * (rows.size() + 2), std::max(2 * c->row_cap, (size_t)4096));
         TRY(dalloc(c, &c->row_map, rcap));
         TRY(dalloc(c, &c->chunk_cnt, rcap));
         TRY(dalloc(c, &c->chunk_off, rcap));
@@ -353,38 +364,54 @@ int layout(simp_ctx *c) {
     std::vector<Inst> table(c->max_inst);
     for (int q = 0; q < c->max_inst; ++q) table[q] = c->insts[q].active ? c->insts[q].I : Inst{};
     SIMP_CUDA(c, cudaMemcpyAsync(c->inst_dev, table.data(), sizeof(Inst) * c->max_inst, cudaMemcpyHostToDevice, s));
-    // walls of every active instance, sorted by cell key (stable)
-    struct W { int key, slot, local; double x, y, m, nx, ny; };
-    std::vector<W> ws;
-    for (int q = 0; q < c->max_inst; ++q) {
-        const InstHost &h = c->insts[q];
-        if (!h.active) continue;
+    // walls of every active instance, sorted by cell key (stable): each
+    // instance's walls sorted by their local cell once per grid, then the
+    // instances in key-base order (their key ranges are disjoint)
+    int nb = 0;
+    for (int q : by_order) {
+        InstHost &h = c->insts[q];
         const Inst &I = h.I;
-        for (int b = 0; b < h.nb; ++b) {
-            const double xb = h.xb[2 * b], yb = h.xb[2 * b + 1];
-            const int cx = clampi((int)std::floor((xb - I.x0) * I.inv_cs), 0, I.ncx - 1);
-            const int cy = clampi((int)std::floor((yb - I.y0) * I.inv_cs), 0, I.ncy - 1);
-            const bool hn = h.bn.size() == 2 * (size_t)h.nb;
-            ws.push_back({I.base + cy * I.ncx + cx, q, b, xb, yb, h.massb[b], hn ? h.bn[2 * b] : 0.0,
-                          hn ? h.bn[2 * b + 1] : 0.0});
+        if (h.wall_grid_cs != I.cs || h.wall_grid_x0 != I.x0 || h.wall_grid_y0 != I.y0 ||
+            h.wall_key.size() != (size_t)h.nb) {
+            std::vector<std::pair<int, int>> kb((size_t)h.nb);
+            for (int b = 0; b < h.nb; ++b) {
+                const double xb = h.xb[2 * b], yb = h.xb[2 * b + 1];
+                const int cx = clampi((int)std::floor((xb - I.x0) * I.inv_cs), 0, I.ncx - 1);
+                const int cy = clampi((int)std::floor((yb - I.y0) * I.inv_cs), 0, I.ncy - 1);
+                kb[(size_t)b] = {cy * I.ncx + cx, b};
+            }
+            std::stable_sort(kb.begin(), kb.end(),
+                             [](const std::pair<int, int> &a, const std::pair<int, int> &b) { return a.first < b.first; });
+            h.wall_key.resize((size_t)h.nb);
+            h.wall_order.resize((size_t)h.nb);
+            for (int k = 0; k < h.nb; ++k) {
+                h.wall_key[(size_t)k] = kb[(size_t)k].first;
+                h.wall_order[(size_t)k] = kb[(size_t)k].second;
+            }
+            h.wall_grid_cs = I.cs;
+            h.wall_grid_x0 = I.x0;
+            h.wall_grid_y0 = I.y0;
+        }
+        nb += h.nb;
+    }
+    std::vector<double> hx(nb), hy(nb), hm(nb), hnx(nb), hny(nb);
+    std::vector<int> hid(nb), hinst(nb), hcell(nb);
+    int k = 0;
+    for (int q : by_order) {
+        const InstHost &h = c->insts[q];
+        const bool hn = h.bn.size() == 2 * (size_t)h.nb;
+        for (int e = 0; e < h.nb; ++e, ++k) {
+            const int b = h.wall_order[(size_t)e];
+            hx[k] = h.xb[2 * b];
+            hy[k] = h.xb[2 * b + 1];
+            hm[k] = h.massb[b];
+            hnx[k] = hn ? h.bn[2 * b] : 0.0;
+            hny[k] = hn ? h.bn[2 * b + 1] : 0.0;
+            hid[k] = b;
+            hinst[k] = q;
+            hcell[k] = h.I.base + h.wall_key[(size_t)e];
         }
     }
-    std::stable_sort(ws.begin(), ws.end(), [](const W &a, const W &b) { return a.key < b.key; });
-    const int nb = (int)ws.size();
-    std::vector<double> hx(nb), hy(nb), hm(nb), hnx(nb), hny(nb);
-    std::vector<int> hid(nb), hinst(nb), hcell(nb), start((size_t)base + 1, 0);
-    for (int k = 0; k < nb; ++k) {
-        hx[k] = ws[k].x;
-        hy[k] = ws[k].y;
-        hm[k] = ws[k].m;
-        hnx[k] = ws[k].nx;
-        hny[k] = ws[k].ny;
-        hid[k] = ws[k].local;
-        hinst[k] = ws[k].slot;
-        hcell[k] = ws[k].key;
-        start[ws[k].key + 1] += 1;
-    }
-    for (int k = 0; k < base; ++k) start[k + 1] += start[k];
     if (nb > 0) {
         SIMP_CUDA(c, cudaMemcpyAsync(c->bx, hx.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, s));
         SIMP_CUDA(c, cudaMemcpyAsync(c->by, hy.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, s));
@@ -397,8 +424,11 @@ int layout(simp_ctx *c) {
         SIMP_CUDA(c, cudaMemcpyAsync(c->binst, hinst.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, s));
         SIMP_CUDA(c, cudaMemcpyAsync(c->bcell, hcell.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, s));
     }
-    SIMP_CUDA(c, cudaMemcpyAsync(c->bcell_start, start.data(), sizeof(int) * ((size_t)base + 1),
-                                 cudaMemcpyHostToDevice, s));
+    // cell-start offsets of the walls, counted and scanned on the device
+    SIMP_CUDA(c, cudaMemsetAsync(c->cnt, 0, sizeof(int) * ((size_t)base + 1), s));
+    if (nb > 0) k_count_walls<<<nblk(nb, kB), kB, 0, s>>>(nb, c->bcell, c->cnt);
+    launch_scan_i32(c->cnt, c->bcell_start, base, c->scan_tmp, s);
+    c->launches += 1 + kScanKernels;
     SIMP_CUDA(c, cudaStreamSynchronize(s));
     c->nb = nb;
     invalidate_graph(c);

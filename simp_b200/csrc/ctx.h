@@ -21,6 +21,10 @@ struct InstHost {
     long long steps_done = 0;
     std::vector<double> xb, massb; // its walls (re-binned when the layout changes)
     std::vector<double> bn;        // their normals b_normal(2, nb) (bf_Wang), empty until set
+    // its walls in cell order: local cell keys and wall indices, for the
+    // grid (cs, x0, y0) they were binned on
+    std::vector<int> wall_key, wall_order;
+    double wall_grid_cs = 0.0, wall_grid_x0 = 0.0, wall_grid_y0 = 0.0;
 };
 
 // Extents of a basin staged for admission, reduced on the device.
