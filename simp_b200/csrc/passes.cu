@@ -101,13 +101,13 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<T>::kin) k_kinematic(KinArgs
         const float skinf = (float)skin, grow = 1.0f + pc.margin;
         int total = 0;
         for_stencil(pc.g, i, a.cell[i], stencil_radius(pc.hmax, pc.dmax2_bits, pc.g, pc.hmax + skin), [&](int j) {
-            const float4 f = s.pf[j];
+            const float4 f = __ldg(&s.pf[j]);
             const float dxf = pc.xif - f.x, dyf = pc.yif - f.y;
             const float lim = 0.5f * (pc.hif + f.z) + skinf;
             if (dxf * dxf + dyf * dyf > lim * lim * grow) return;
             if (total < kMaxNbr) a.nl.nbr[(size_t)total * a.nl.stride + i] = j;
             ++total;
-            if (is_pair(s, pc, j)) on_pair(j);
+            if (is_pair_with(s, pc, j, f)) on_pair(j);
         });
         a.nl.count[i] = total;
         a.nl.xl[i] = xi;
