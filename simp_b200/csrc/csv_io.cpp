@@ -148,25 +148,35 @@ std::string join(const char *folder, const char *name) {
     return p + name;
 }
 
-// Lines of a text file (without their newlines).
-int read_lines(const std::string &path, std::vector<std::string> *lines) {
+// Lines [first, first + count) of a text file (without their newlines;
+// count < 0: to the end), streamed: a file of many snapshots is never held
+// in memory whole.
+int read_lines(const std::string &path, std::vector<std::string> *lines, long long first = 0,
+               long long count = -1) {
     FILE *fp = std::fopen(path.c_str(), "r");
     if (!fp) return csv_fail(SIMP_ERR_BADARG, "cannot open " + path + ": " + std::strerror(errno));
     lines->clear();
     std::string cur;
+    long long line = 0;
+    const long long last = (count < 0) ? -1 : first + count;
     char buf[1 << 16];
     size_t got;
-    while ((got = std::fread(buf, 1, sizeof buf, fp)) > 0) {
+    bool done = false;
+    while (!done && (got = std::fread(buf, 1, sizeof buf, fp)) > 0) {
         for (size_t k = 0; k < got; ++k) {
             if (buf[k] == '\n') {
-                lines->push_back(cur);
+                if (line >= first) lines->push_back(cur);
                 cur.clear();
-            } else if (buf[k] != '\r') {
+                if (++line == last) {
+                    done = true;
+                    break;
+                }
+            } else if (buf[k] != '\r' && line >= first) {
                 cur.push_back(buf[k]);
             }
         }
     }
-    if (!cur.empty()) lines->push_back(cur);
+    if (!done && !cur.empty() && line >= first) lines->push_back(cur);
     std::fclose(fp);
     return SIMP_OK;
 }
@@ -287,14 +297,14 @@ int32_t simp_csv_read_snapshot(const char *folder, int32_t snapshot, int32_t cap
     if (n > cap)
         return csv_fail(SIMP_ERR_MAXN, "The number of particles read from the input file is higher than the "
                                        "maximum allowed. (initialize.f90:276-283)");
-    if ((rc = read_lines(join(folder, "particle_momentum.csv"), &mom))) return rc;
-    if ((rc = read_lines(join(folder, "particle_state.csv"), &st))) return rc;
-    if ((long long)mom.size() < first + n || (long long)st.size() < first + n)
+    if ((rc = read_lines(join(folder, "particle_momentum.csv"), &mom, first, n))) return rc;
+    if ((rc = read_lines(join(folder, "particle_state.csv"), &st, first, n))) return rc;
+    if ((long long)mom.size() < n || (long long)st.size() < n)
         return csv_fail(SIMP_ERR_BADARG, "read_snapshot: the particle files end before snapshot " +
                                              std::to_string(k));
     for (long long r = first; r < first + n; ++r) {
         double a[5], b[12];
-        if (parse_numbers(mom[(size_t)r], a, 5) != 5 || parse_numbers(st[(size_t)r], b, 12) != 12)
+        if (parse_numbers(mom[(size_t)(r - first)], a, 5) != 5 || parse_numbers(st[(size_t)(r - first)], b, 12) != 12)
             return csv_fail(SIMP_ERR_BADARG, "read_snapshot: short record at line " + std::to_string(r + 1));
         const long long i = (long long)a[0] - 1;
         if (i < 0 || i >= n || (long long)b[0] - 1 != i)
