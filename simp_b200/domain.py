@@ -111,6 +111,83 @@ def boundary_placing_1(bmap, bmap_resolution: float, b_length: float, bx_mingeom
     return xb, nrm
 
 
+def boundary_placing_2(bmap, bmap_resolution: float, b_length: float, bx_mingeom: float, by_maxgeom: float,
+                       max_hsml: float, hsml_multiplicity: int = 3, map_factor: float = 1.0,
+                       maxnb: int | None = None) -> np.ndarray:
+    """Walls of hsml_multiplicity lines, max(hsml) / hsml_multiplicity
+    apart and reaching into the land cell, on every land/ice edge, and on
+    the two edges of a land cell whose only ice neighbour is diagonal
+    (boundaries.f90:319-599).  No normals: the Wang force is not allowed with
+    these walls (boundaries.f90:76-83).  Map cells outside the map count as
+    land."""
+    bmap = np.asarray(bmap)
+    bx_numcell, by_numcell = bmap.shape
+    bppg = int(np.floor(bmap_resolution / (b_length / 3) + 0.5))
+    if bppg == 0:
+        raise DomainError("Boundary map resolution too high by comparison to the boundary particle resolution.")
+    spacing = max_hsml / hsml_multiplicity
+    half = f32(0.5) * f32(map_factor)
+    res = bmap_resolution
+    out = []
+
+    def ice(a, b):           # 1-based map indices
+        return 1 <= a <= bx_numcell and 1 <= b <= by_numcell and bmap[a - 1, b - 1] == 1
+
+    def lines(fx, fy):
+        for k in range(bppg):
+            t = (f32(k) + f32(0.5)) / f32(bppg)
+            for l in range(hsml_multiplicity):
+                out.append((fx(t, l), fy(t, l)))
+
+    def left(n, m):          # :339-350
+        lines(lambda t, l: bx_mingeom + float(f32(n) - half) * res - l * spacing,
+              lambda t, l: by_maxgeom + float(f32(-m + 1) + half - t) * res)
+
+    def right(n, m):         # :352-363
+        lines(lambda t, l: bx_mingeom + float(f32(n - 1) - half) * res + l * spacing,
+              lambda t, l: by_maxgeom + float(f32(-m + 1) + half - t) * res)
+
+    def up(n, m):            # :365-376
+        lines(lambda t, l: bx_mingeom + float(f32(n - 1) - half + t) * res,
+              lambda t, l: by_maxgeom + float(f32(-m) + half) * res + l * spacing)
+
+    def down(n, m):          # :378-389
+        lines(lambda t, l: bx_mingeom + float(f32(n - 1) - half + t) * res,
+              lambda t, l: by_maxgeom + float(f32(-m + 1) + half) * res - l * spacing)
+
+    for m in range(1, by_numcell + 1):
+        for n in range(1, bx_numcell + 1):
+            if bmap[n - 1, m - 1] != 0:
+                continue
+            if ice(n + 1, m):
+                left(n, m)
+            if ice(n - 1, m):
+                right(n, m)
+            if ice(n, m + 1):
+                up(n, m)
+            if ice(n, m - 1):
+                down(n, m)
+            # a diagonal ice neighbour only (:391-470 and :472-583)
+            if ice(n, m - 1) or ice(n, m + 1) or ice(n - 1, m) or ice(n + 1, m):
+                continue
+            if ice(n + 1, m - 1):
+                left(n, m)
+                down(n, m)
+            if ice(n - 1, m + 1):
+                right(n, m)
+                up(n, m)
+            if ice(n + 1, m + 1):
+                left(n, m)
+                up(n, m)
+            if ice(n - 1, m - 1):
+                down(n, m)
+                right(n, m)
+    xb = np.ascontiguousarray(np.array(out, dtype=np.float64).reshape(-1, 2))
+    if maxnb is not None and xb.shape[0] > maxnb:
+        raise DomainError("The number of boundary particles generated is higher than the maximum allowed.")
+    return xb
+
+
 def boundary_normal(xb, b_normal) -> np.ndarray:
     """Normals refitted from each wall particle and its two nearest wall
     neighbours (boundaries.f90:607-772), as the reference computes them for
@@ -164,16 +241,25 @@ def boundary_normal(xb, b_normal) -> np.ndarray:
 
 def basin_from_map(ice_map, map_resolution: float, resolution: float, x_mingeom: float, y_maxgeom: float,
                    params: SimpParams, bmap=None, bmap_resolution: float | None = None,
-                   map_factor: float = 1.0, name: str = "map_basin") -> Basin:
+                   map_factor: float = 1.0, b_setup: int = 1, name: str = "map_basin") -> Basin:
     """A basin of a map domain: the particles of particle_placing and, with a
     boundary map (the ice map itself when none is given), the walls of
-    boundary_placing_1 with massb = mean(mass) (boundaries.f90:52) and their
-    normals (refitted by boundary_normal when bfa = 2)."""
+    boundary_placing_1 (b_setup = 1) or boundary_placing_2 (b_setup = 2)
+    with massb = mean(mass) (boundaries.f90:52, 72), and the normals of
+    boundary_placing_1 (refitted by boundary_normal when bfa = 2)."""
     part = particle_placing(ice_map, map_resolution, resolution, x_mingeom, y_maxgeom,
                             params.hsml_multiplicity)
     bmap = np.asarray(ice_map if bmap is None else bmap)
     bres = map_resolution if bmap_resolution is None else bmap_resolution
-    xb, nrm = boundary_placing_1(bmap, bres, params.b_length, x_mingeom, y_maxgeom, map_factor)
+    if b_setup == 2:
+        if params.bfa == 2:
+            raise DomainError("The boundary force cannot be with bfa 2 if the boundary layer has multiple "
+                              "set of particles.")
+        xb = boundary_placing_2(bmap, bres, params.b_length, x_mingeom, y_maxgeom, float(part["hsml"].max()),
+                                params.hsml_multiplicity, map_factor)
+        nrm = np.zeros_like(xb)
+    else:
+        xb, nrm = boundary_placing_1(bmap, bres, params.b_length, x_mingeom, y_maxgeom, map_factor)
     if params.bfa == 2 and xb.shape[0] >= 3:
         nrm = boundary_normal(xb, nrm)
     n = part["x"].shape[0]

@@ -88,3 +88,33 @@ def test_map_basin_steps_in_the_oracle(oracle_mod):
     st = o.get_state()
     assert np.all(np.isfinite(st["x"])) and st["current_time"] == pytest.approx(3.0)
     assert b.nb > 0 and b.bn.shape == b.xb.shape
+
+
+def test_multilayer_walls():
+    """boundary_placing_2: hsml_multiplicity lines per edge, spaced
+    max(hsml) / hsml_multiplicity into the land; a land cell touching ice
+    only diagonally gets two edges."""
+    m = np.zeros((5, 5), dtype=np.int32)
+    m[1:4, 1:4] = 1
+    xb1, _ = domain.boundary_placing_1(m, 4000.0, 4000.0, 0.0, 50000.0)
+    xb2 = domain.boundary_placing_2(m, 4000.0, 4000.0, 0.0, 50000.0, max_hsml=3000.0, hsml_multiplicity=3)
+    # straight edges: 3 layers of the single-layer wall, plus the 4 corner
+    # cells (diagonal ice neighbour only): 2 edges x 3 wall particles x 3 layers each
+    assert xb2.shape[0] == 3 * xb1.shape[0] + 4 * 2 * 3 * 3
+    # the first layer of each edge is the single-layer wall
+    first = xb2[::3]
+    assert set(map(tuple, np.round(xb1, 6))) <= set(map(tuple, np.round(first, 6)))
+    # successive layers step 1000 m along one axis, away from the ice
+    # square's centre
+    c = np.array([2.0 * 4000.0, 50000.0 - 2.0 * 4000.0])
+    for a, b in ((0, 1), (1, 2)):
+        step = xb2[b::3] - xb2[a::3]
+        assert np.allclose(np.sort(np.abs(step), axis=1), [0.0, 1000.0])
+        assert np.all(np.abs(xb2[b::3] - c).sum(axis=1) > np.abs(xb2[a::3] - c).sum(axis=1))
+
+
+def test_multilayer_walls_refuse_wang_force():
+    prm = basin_params(1000.0)
+    prm.bfa = 2
+    with pytest.raises(domain.DomainError):
+        domain.basin_from_map(_lshape(), 4000.0, 1000.0, 0.0, 0.0, prm, b_setup=2)

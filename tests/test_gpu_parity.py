@@ -432,3 +432,25 @@ def test_map_domain_wang_force_with_refitted_normals(gpu_lib, oracle_mod):
     rg, ro = g.single_step(3600.0), o.single_step(3600.0)
     for k in ("dvxdt", "dhdt", "dAdt"):
         assert rel_l2(rg[k], ro[k]) < TOL_RHS, (k, rel_l2(rg[k], ro[k]))
+
+
+def test_map_domain_multilayer_walls_against_oracle(gpu_lib, oracle_mod):
+    """The same map with three-line walls (boundary_placing_2): more wall
+    pairs per particle; one right-hand side and 5 steps."""
+    from simp_b200 import domain
+    m = np.zeros((16, 12), dtype=np.int32)
+    m[1:15, 1:11] = 1
+    m[8:15, 1:6] = 0
+    prm = basins.basin_params(1000.0, dt=1.0, wind=(8.0, 3.0))
+    b = domain.basin_from_map(m, 4000.0, 1000.0, 10000.0, 150000.0, prm, b_setup=2)
+    b.vx = smooth_velocity(b.x, b.L, amp=0.3, seed=45)
+    g, o = _pair(b, oracle_mod)
+    rg, ro = g.single_step(3600.0), o.single_step(3600.0)
+    for k in ("dvxdt", "dhdt", "dAdt"):
+        assert rel_l2(rg[k], ro[k]) < TOL_RHS, (k, rel_l2(rg[k], ro[k]))
+    g2, o2 = _pair(b, oracle_mod)
+    g2.time_integration(5)
+    o2.step(5)
+    sg, so = g2.get_state(), o2.get_state()
+    for k in ("vx", "h"):
+        assert rel_l2(sg[k], so[k]) < 1e-9, (k, rel_l2(sg[k], so[k]))
