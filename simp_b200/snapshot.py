@@ -8,6 +8,8 @@ The formatting and parsing are host code inside libsimp_gpu.so; only
 """
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 
 from . import _lib
@@ -56,16 +58,16 @@ def particle_reading(folder: str, snapshot: int = -1, cap: int | None = None) ->
     """One snapshot of the particle files in SI units (x in m, vx in m/s,
     current_time in s), with rho = h rho_ice (the files hold no density)."""
     lib = _lib.load()
-    n, nb = _lib.ctypes.c_int32(), _lib.ctypes.c_int32()
-    t = _lib.ctypes.c_double()
-    _chk(lib.simp_csv_read_snapshot(_enc(folder), int(snapshot), 0, _lib.ctypes.byref(n), _lib.ctypes.byref(nb),
-                                    _lib.ctypes.byref(t), *([None] * 7)))
+    n, nb = ctypes.c_int32(), ctypes.c_int32()
+    t = ctypes.c_double()
+    _chk(lib.simp_csv_read_snapshot(_enc(folder), int(snapshot), 0, ctypes.byref(n), ctypes.byref(nb),
+                                    ctypes.byref(t), *([None] * 7)))
     out = {"x": np.zeros((n.value, 2)), "vx": np.zeros((n.value, 2))}
     for k in ("mass", "p", "hsml", "A", "h"):
         out[k] = np.zeros(n.value)
     cap = n.value if cap is None else int(cap)
-    _chk(lib.simp_csv_read_snapshot(_enc(folder), int(snapshot), cap, _lib.ctypes.byref(n), _lib.ctypes.byref(nb),
-                                    _lib.ctypes.byref(t),
+    _chk(lib.simp_csv_read_snapshot(_enc(folder), int(snapshot), cap, ctypes.byref(n), ctypes.byref(nb),
+                                    ctypes.byref(t),
                                     *[_lib.dptr(out[k]) for k in ("x", "vx", "mass", "p", "hsml", "A", "h")]))
     out["rho"] = out["h"] * RHO_ICE
     out["ntotalb"] = nb.value
@@ -76,9 +78,9 @@ def particle_reading(folder: str, snapshot: int = -1, cap: int | None = None) ->
 def boundary_reading(folder: str, cap: int | None = None) -> dict:
     """boundary_particles.csv in SI units."""
     lib = _lib.load()
-    nb = _lib.ctypes.c_int32()
-    _chk(lib.simp_csv_read_walls(_enc(folder), 0, _lib.ctypes.byref(nb), None, None))
+    nb = ctypes.c_int32()
+    _chk(lib.simp_csv_read_walls(_enc(folder), 0, ctypes.byref(nb), None, None))
     xb, massb = np.zeros((nb.value, 2)), np.zeros(nb.value)
     cap = nb.value if cap is None else int(cap)
-    _chk(lib.simp_csv_read_walls(_enc(folder), cap, _lib.ctypes.byref(nb), _lib.dptr(xb), _lib.dptr(massb)))
+    _chk(lib.simp_csv_read_walls(_enc(folder), cap, ctypes.byref(nb), _lib.dptr(xb), _lib.dptr(massb)))
     return {"xb": xb, "massb": massb}
