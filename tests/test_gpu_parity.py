@@ -454,3 +454,36 @@ def test_map_domain_multilayer_walls_against_oracle(gpu_lib, oracle_mod):
     sg, so = g2.get_state(), o2.get_state()
     for k in ("vx", "h"):
         assert rel_l2(sg[k], so[k]) < 1e-9, (k, rel_l2(sg[k], so[k]))
+
+
+def test_benz_drhodt_follows_particles_through_resorts(gpu_lib, oracle_mod):
+    """Benz hsml with the diagnostic density keeps the reference's
+    never-cleared drhodt per particle; 20 steps cross the re-sort at step 16,
+    which moves that array with the particles."""
+    b = basins.cfg1()
+    b.vx = smooth_velocity(b.x, b.L, amp=0.3, seed=46)
+    prm = _variant(b, sle=1)
+    g, o = _pair(b, oracle_mod, prm)
+    g.time_integration(20)
+    o.step(20)
+    sg, so = g.get_state(), o.get_state()
+    for k in ("hsml", "vx", "h"):
+        assert rel_l2(sg[k], so[k]) < TOL_TRAJ_20, (k, rel_l2(sg[k], so[k]))
+    assert not np.array_equal(sg["hsml"], b.hsml)
+
+
+def test_con_density_mixed_precision(gpu_lib):
+    """The continuity density in the mixed form against the plain form:
+    its density-rate pass is FP64 in both."""
+    from simp_b200.params import PREC_MIXED
+    b = basins.cfg1()
+    b.vx = smooth_velocity(b.x, b.L, amp=0.3, seed=47)
+    p64 = _variant(b, den_alg=2, dt=1e-3)
+    p32 = _variant(b, den_alg=2, dt=1e-3, precision=PREC_MIXED)
+    g64, g32 = Simp.from_basin(b, p64), Simp.from_basin(b, p32)
+    g64.time_integration(10)
+    g32.time_integration(10)
+    s64, s32 = g64.get_state(), g32.get_state()
+    for k in ("rho", "vx", "h"):
+        assert rel_l2(s32[k], s64[k]) < 1e-6, (k, rel_l2(s32[k], s64[k]))
+    assert not np.array_equal(s64["rho"], b.rho)
