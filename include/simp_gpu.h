@@ -293,11 +293,18 @@ SIMP_API void *simp_gpu_stream(simp_ctx *ctx);
 /* Implementation of the two pair passes (no reference counterpart):
  * SIMP_PASSES_TILED stages chunks of `threads` consecutive particles of a
  * cell row with their cell halo (at most `cap` particles) in shared memory;
- * SIMP_PASSES_GATHER gathers every particle's neighbours from HBM over
- * Verlet lists.  Both give the same bits.  threads: 64..256, a multiple of
- * 32; cap: a multiple of 4, within the shared memory of one block. */
+ * the gather forms gather every particle's neighbours from HBM over Verlet
+ * lists, with the kinematic pass as one kernel (SIMP_PASSES_GATHER_ONE) or
+ * as two, pair finding then pair sums over the stored pair list
+ * (SIMP_PASSES_GATHER_TWO); SIMP_PASSES_GATHER (the default) takes two
+ * kernels for plain FP64 contexts of up to 400,000 particles, else one.
+ * All give the same bits.  threads: 64..256, a multiple of 32; cap: a
+ * multiple of 4, within the shared memory of one block (both checked for
+ * every form). */
 #define SIMP_PASSES_GATHER 0
 #define SIMP_PASSES_TILED 1
+#define SIMP_PASSES_GATHER_ONE 2
+#define SIMP_PASSES_GATHER_TWO 3
 SIMP_API int32_t simp_gpu_set_passes(simp_ctx *ctx, int32_t impl, int32_t threads, int32_t cap);
 SIMP_API int32_t simp_gpu_get_passes(const simp_ctx *ctx, int32_t *impl, int32_t *threads, int32_t *cap);
 /* Times one right-hand side (both passes, no state change) of the current

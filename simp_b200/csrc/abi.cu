@@ -1305,7 +1305,7 @@ int32_t simp_gpu_step(simp_ctx *c, int32_t nsteps, double *current_time, double 
 
 int32_t simp_gpu_set_passes(simp_ctx *c, int32_t impl, int32_t threads, int32_t cap) {
     if (!c) return SIMP_ERR_BADARG;
-    if (impl != SIMP_PASSES_GATHER && impl != SIMP_PASSES_TILED)
+    if (impl < SIMP_PASSES_GATHER || impl > SIMP_PASSES_GATHER_TWO)
         return simp_fail(c, SIMP_ERR_BADARG, "unknown pair-pass implementation");
     if (threads < kMinTileThreads || threads > 256 || threads % 32 != 0 || cap < 64 || cap % 4 != 0 ||
         cap > 32767)
@@ -1367,7 +1367,8 @@ int32_t simp_gpu_autotune(simp_ctx *c, int32_t reps, double *ms_best) {
     const Cand cands[] = {
         {SIMP_PASSES_TILED, 128, 512},  {SIMP_PASSES_TILED, 128, 768},  {SIMP_PASSES_TILED, 128, 1024},
         {SIMP_PASSES_TILED, 256, 768},  {SIMP_PASSES_TILED, 256, 1024}, {SIMP_PASSES_TILED, 256, 1536},
-        {SIMP_PASSES_TILED, 64, 384},   {SIMP_PASSES_TILED, 64, 512},   {SIMP_PASSES_GATHER, 256, 1024}};
+        {SIMP_PASSES_TILED, 64, 384},   {SIMP_PASSES_TILED, 64, 512},   {SIMP_PASSES_GATHER_ONE, 256, 1024},
+        {SIMP_PASSES_GATHER_TWO, 256, 1024}};
     const Cand keep{c->pass_impl, c->tile_threads, c->tile_cap};
     Cand best = keep;
     double tbest = INFINITY;

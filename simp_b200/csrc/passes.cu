@@ -14,6 +14,16 @@ namespace {
 using namespace pass;
 
 constexpr int kBlock = 128;
+// Up to this many particles in a context the plain FP64 kinematic pass runs
+// as two kernels (k_find_pairs, k_kin_sums), above it as one (k_kinematic),
+// unless the context names one form (SIMP_PASSES_GATHER_ONE / _TWO).
+// The two-kernel pass writes and re-reads the pair list, which pays while
+// that round trip stays in L2.  Per pass, one kernel -> two (B200, basins of
+// the 500 m lattice): 147,456 particles 64.6 -> 55.1 us, 262,144 96.4 ->
+// 89.2, 409,600 143.0 -> 143.3, 524,176 170.5 -> 179.8, 1,048,576 305.7 ->
+// 343.9.  The mixed form always runs one kernel: on 1,048,576 particles the
+// two-kernel pass took 267 us against 241.
+constexpr int kSplitMaxParticles = 400000;
 // minimum resident blocks per SM, per precision form, measured against 4..8
 // (cfg2 FP64, cfg3 mixed): the FP64 kinematic pass keeps its pair math in
 // registers (cap 102), the FP32 passes and the FP64 stress pass trade
@@ -42,7 +52,12 @@ struct MinBlocks<float> {
 // a longer list is processed in batches.  Kept small: the shared memory of
 // the resident blocks comes out of the L1 cache that serves the gathers.
 constexpr int kGatherSlots = 24;
+#ifndef SIMP_FIND_MIN_BLOCKS
+#define SIMP_FIND_MIN_BLOCKS 8
+#endif
 
+// The kinematic pass in one kernel: candidates go into a per-thread list in
+// shared memory, then the pair arithmetic runs densely.
 template <class T, int SKF>
 __global__ void __launch_bounds__(kBlock, MinBlocks<T>::kin) k_kinematic(KinArgs a) {
     __shared__ int s_list[kGatherSlots * kBlock];
@@ -124,6 +139,93 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<T>::kin) k_kinematic(KinArgs
     }
     flush();   // (also writes the stress pass's pair list, a coalesced row per k)
     a.pl.count[i] = npairs;
+    kin_rheology(a, i, -ks.dv.get(), -ks.g1.get(), -ks.g2.get(), -ks.g3.get(), -ks.g4.get());
+}
+
+// The kinematic pass in two kernels.  k_find_pairs decides the exact pairs
+// of each particle (Verlet candidates, or the cell stencil when the lists
+// are rebuilt) and writes them as the pair list; it needs fewer registers
+// than the FP64 pair arithmetic, so more warps hide its gather latency.
+// k_kin_sums then does the pair arithmetic over those rows, in the order
+// they were found, the order of the one-kernel pass: both give bitwise the
+// same results.  launch_kinematic picks between them.
+__global__ void __launch_bounds__(kBlock, SIMP_FIND_MIN_BLOCKS) k_find_pairs(KinArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const State &s = a.s;
+    const Inst &I = a.inst[a.pinst[i]];
+    // a basin whose state turned non-finite is not searched any more (its
+    // stencil would span its whole grid); it is only carried until retired
+    const bool dead = (I.flags & FLAG_NONFINITE) != 0;
+    const PairCtx pc = pair_ctx(s, a.sc, I, a.cell_start, i);
+    int npairs = 0;
+    auto on_pair = [&](int j) {
+        if (npairs < kMaxPairs) a.pl.pj[(size_t)npairs * a.pl.stride + i] = j;
+        ++npairs;
+    };
+    if (a.sc->list_scan && i == 0) atomicExch(&a.sc->dlist2_bits, 0ull);
+    // (a particle of a newly admitted basin builds its list on its own)
+    const bool build = a.sc->list_scan || a.nl.count[i] < 0;
+    if (dead) {
+        if (build) {
+            a.nl.count[i] = 0;
+            a.nl.xl[i] = pc.xi;
+            a.nl.yl[i] = pc.yi;
+        }
+    } else if (build) {
+        // rebuild the Verlet list from the cell stencil: members are the
+        // candidates not certainly beyond mhsml + skin (FP32, with margin)
+        const double skin = a.sc->skin;
+        const float skinf = (float)skin, grow = 1.0f + pc.margin;
+        int total = 0;
+        for_stencil(pc.g, i, a.cell[i], stencil_radius(pc.hmax, pc.dmax2_bits, pc.g, pc.hmax + skin), [&](int j) {
+            const float4 f = __ldg(&s.pf[j]);
+            const float dxf = pc.xif - f.x, dyf = pc.yif - f.y;
+            const float lim = 0.5f * (pc.hif + f.z) + skinf;
+            if (dxf * dxf + dyf * dyf > lim * lim * grow) return;
+            if (total < kMaxNbr) a.nl.nbr[(size_t)total * a.nl.stride + i] = j;
+            ++total;
+            if (is_pair_with(s, pc, j, f)) on_pair(j);
+        });
+        a.nl.count[i] = total;
+        a.nl.xl[i] = pc.xi;
+        a.nl.yl[i] = pc.yi;
+    } else {
+        for_each_current_pair_batched(s, a.nl, a.sc, i, a.cell[i], pc, [] {}, on_pair);
+    }
+    a.pl.count[i] = npairs;
+}
+
+template <class T, int SKF>
+__global__ void __launch_bounds__(kBlock, MinBlocks<T>::kin) k_kin_sums(KinArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const State &s = a.s;
+    const Phys &P = a.P;
+    const double xi = s.x[i], yi = s.y[i], hi = s.hs[i];
+    const double vxi = s.vx[i], vyi = s.vy[i];
+    const double inv_hi = 1.0 / hi;
+    KinSums<T> ks;     // -div and the velocity gradient, negated
+    const T hiT = Nb<T>::h(s, i), inv_hiT = (T)inv_hi;
+    typename Vec2<T>::type *dwr = reinterpret_cast<typename Vec2<T>::type *>(a.dw);
+    auto pair = [&](int k, int j) {
+        const double2 q = __ldg(&s.xy[j]), v = __ldg(&s.vxy[j]);
+        const KinNb<T> nb = Nb<T>::kin(s, j);
+        const PairGeom<T> pg = pair_geom<T, false, SKF>(P, (T)(xi - q.x), (T)(yi - q.y), hiT, inv_hiT, nb.h);
+        const T dwx = pg.gfac * pg.dx, dwy = pg.gfac * pg.dy;
+        if (dwr && k < kDwRows) dwr[(size_t)k * a.pl.stride + i] = Vec2<T>::make(dwx, dwy);
+        ks.add(dwx, dwy, (T)(vxi - v.x), (T)(vyi - v.y), nb.m, nb.mor);
+    };
+    const int cnt = a.pl.count[i];
+    if (cnt <= kMaxPairs) {
+#pragma unroll 4
+        for (int k = 0; k < cnt; ++k) pair(k, __ldg(&a.pl.pj[(size_t)k * a.pl.stride + i]));
+    } else {
+        // more pairs than list rows: found again, in the same order
+        const PairCtx pc = pair_ctx(s, a.sc, a.inst[a.pinst[i]], a.cell_start, i);
+        int k = 0;
+        for_each_current_pair(s, a.nl, a.sc, i, a.cell[i], pc, [&](int j) { pair(k++, j); });
+    }
     kin_rheology(a, i, -ks.dv.get(), -ks.g1.get(), -ks.g2.get(), -ks.g3.get(), -ks.g4.get());
 }
 
@@ -412,22 +514,42 @@ void launch_kinematic(simp_ctx *c, const State &s, bool diag) {
         launch_kinematic_tiled(c, a);
         return;
     }
-    const bool mixed = c->prm.precision == SIMP_PREC_MIXED;
     const int g = nblk(c->n, kBlock);
+    const bool mixed = c->prm.precision == SIMP_PREC_MIXED;
+    const bool two = c->pass_impl == SIMP_PASSES_GATHER_TWO ||
+                     (c->pass_impl == SIMP_PASSES_GATHER && !mixed && c->n <= kSplitMaxParticles);
+    if (!two) {
+        switch (skf_compiled(c->prm.skf)) {
+            case SIMP_SKF_CUBIC:
+                if (mixed) k_kinematic<float, SIMP_SKF_CUBIC><<<g, kBlock, 0, c->stream>>>(a);
+                else k_kinematic<double, SIMP_SKF_CUBIC><<<g, kBlock, 0, c->stream>>>(a);
+                break;
+            case SIMP_SKF_WENDLAND_C6:
+                if (mixed) k_kinematic<float, SIMP_SKF_WENDLAND_C6><<<g, kBlock, 0, c->stream>>>(a);
+                else k_kinematic<double, SIMP_SKF_WENDLAND_C6><<<g, kBlock, 0, c->stream>>>(a);
+                break;
+            default:
+                if (mixed) k_kinematic<float, 0><<<g, kBlock, 0, c->stream>>>(a);
+                else k_kinematic<double, 0><<<g, kBlock, 0, c->stream>>>(a);
+        }
+        c->launches += 1;
+        return;
+    }
+    k_find_pairs<<<g, kBlock, 0, c->stream>>>(a);
     switch (skf_compiled(c->prm.skf)) {
         case SIMP_SKF_CUBIC:
-            if (mixed) k_kinematic<float, SIMP_SKF_CUBIC><<<g, kBlock, 0, c->stream>>>(a);
-            else k_kinematic<double, SIMP_SKF_CUBIC><<<g, kBlock, 0, c->stream>>>(a);
+            if (mixed) k_kin_sums<float, SIMP_SKF_CUBIC><<<g, kBlock, 0, c->stream>>>(a);
+            else k_kin_sums<double, SIMP_SKF_CUBIC><<<g, kBlock, 0, c->stream>>>(a);
             break;
         case SIMP_SKF_WENDLAND_C6:
-            if (mixed) k_kinematic<float, SIMP_SKF_WENDLAND_C6><<<g, kBlock, 0, c->stream>>>(a);
-            else k_kinematic<double, SIMP_SKF_WENDLAND_C6><<<g, kBlock, 0, c->stream>>>(a);
+            if (mixed) k_kin_sums<float, SIMP_SKF_WENDLAND_C6><<<g, kBlock, 0, c->stream>>>(a);
+            else k_kin_sums<double, SIMP_SKF_WENDLAND_C6><<<g, kBlock, 0, c->stream>>>(a);
             break;
         default:
-            if (mixed) k_kinematic<float, 0><<<g, kBlock, 0, c->stream>>>(a);
-            else k_kinematic<double, 0><<<g, kBlock, 0, c->stream>>>(a);
+            if (mixed) k_kin_sums<float, 0><<<g, kBlock, 0, c->stream>>>(a);
+            else k_kin_sums<double, 0><<<g, kBlock, 0, c->stream>>>(a);
     }
-    c->launches += 1;
+    c->launches += 2;
 }
 
 void launch_stress(simp_ctx *c, const State &rhs, const State &base, EpiMode mode) {

@@ -27,6 +27,12 @@ KERNELS = {1: ("quadratic", 2), 2: ("gaussian", 3), 3: ("quintic", 3), 4: ("wend
            9: ("cubic", 2)}
 PREC_FP64 = 0
 PREC_MIXED = 1
+
+# pair-pass implementations (include/simp_gpu.h, SIMP_PASSES_*)
+PASSES_GATHER = 0        # gathers; the kinematic pass's kernel count chosen by size
+PASSES_TILED = 1         # shared-memory tiles of a cell row with their halo
+PASSES_GATHER_ONE = 2    # gathers, kinematic pass as one kernel
+PASSES_GATHER_TWO = 3    # gathers, kinematic pass as pair finding + pair sums
 WIND_UNIFORM = 0
 WIND_VORTEX = 1
 

@@ -133,7 +133,9 @@ class Simp:
                 setattr(self.params, name, getattr(forcing, name))
 
     def set_passes(self, impl: int, threads: int = 256, cap: int = 1024):
-        """Pair-pass implementation: 0 per-particle gathers, 1 shared-memory tiles."""
+        """Pair-pass implementation (params.PASSES_*): 0 per-particle gathers
+        with the kinematic pass's form chosen by size, 1 shared-memory tiles,
+        2 gathers with a one-kernel kinematic pass, 3 with a two-kernel one."""
         self._chk(self.lib.simp_gpu_set_passes(self.h, int(impl), int(threads), int(cap)))
 
     def get_passes(self):
