@@ -38,7 +38,7 @@ def main():
     ap.add_argument("--chunk", type=int, default=0, help="steps per call (0: all in one call)")
     ap.add_argument("--precision", choices=("fp64", "mixed"), default=None,
                     help="override the workload's precision")
-    ap.add_argument("--passes", choices=("gather", "tiled"), default="gather",
+    ap.add_argument("--passes", choices=("gather", "tiled", "gather_one", "gather_two"), default="gather",
                     help="pair-pass implementation")
     ap.add_argument("--moving", action="store_true",
                     help="start from a smooth non-zero velocity field instead of rest")
@@ -50,7 +50,7 @@ def main():
     if args.precision:
         prm.precision = 1 if args.precision == "mixed" else 0
     sim = Simp.from_basin(b, prm)
-    sim.set_passes(1 if args.passes == "tiled" else 0)
+    sim.set_passes({"gather": 0, "tiled": 1, "gather_one": 2, "gather_two": 3}[args.passes])
     t0 = time.perf_counter()
     done = 0
     chunk = args.chunk or args.steps
