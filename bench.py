@@ -259,6 +259,9 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "kernel": names[top], "achieved": achieved, "peak": peak,
                          "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured" else "fallback",
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "fp64_pipe_frac": profile_traffic(names[top], "fp64_pipe_frac"),
+                         "fp64_pipe_source": "ncu sm__pipe_fp64_cycles_active of the pass (secondary roof), "
+                                             "profiles/pair_passes_cfg2_fp64.md",
                          "alg_bytes_per_launch": alg, "avg_launch_ms": avg_ms,
                          "step_alg_bytes_per_particle": roofline.STEP_BYTES_PER_PARTICLE,
                          "kernel_ms_per_step": {**{n: kernel_ms[k] / max(1, nst.value) for k, n in enumerate(names)},
@@ -379,12 +382,14 @@ def run_forms(args, which):
     return out
 
 
-def profile_traffic(kernel: str):
-    """DRAM bytes per launch from the committed ncu summary, if present."""
+def profile_traffic(kernel: str, key: str | None = None):
+    """DRAM bytes per launch (or, with key, another per-pass figure) from
+    the committed ncu summary, if present."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic_cfg2.txt")
     try:
         with open(p) as f:
-            v = json.load(f).get(kernel)
+            d = json.load(f)
+        v = (d.get(key) or {}).get(kernel) if key else d.get(kernel)
         return None if v is None else float(v)
     except Exception:
         return None
