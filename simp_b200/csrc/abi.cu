@@ -149,6 +149,90 @@ __global__ void k_grow_xabs(Scalars *sc, double xa) {
     atomicMax(&sc->xabs_bits, (unsigned long long)__double_as_longlong(xa));
 }
 
+// set_state of a state that continues the resident basin (the same
+// particles in the same caller order, the same hsml): the values go into
+// the particles' current places in cell order, so the sort, the cell lists
+// and the Verlet lists stay, and the displacement bounds grow as after a
+// step.  stage = [x,y interleaved | vx,vy interleaved | mass | rho | hsml |
+// A | h] in the caller's order.  Per block: [0] invalid values, [1] changed
+// hsml, [2] max squared displacement since the sort, [3] since the lists
+// were built, [4] max |coordinate|, [5] max hsml, [6] -min hsml.
+__global__ void __launch_bounds__(256) k_continue_state(int n, const int *__restrict__ id,
+                                                       const double *__restrict__ stage, State s,
+                                                       const double *__restrict__ xr,
+                                                       const double *__restrict__ yr, NbrList nl, double *part) {
+    double v[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, -INFINITY};
+    const size_t N = (size_t)n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const size_t o = (size_t)id[i];
+        const double x = stage[2 * o], y = stage[2 * o + 1];
+        const double vx = stage[2 * N + 2 * o], vy = stage[2 * N + 2 * o + 1];
+        const double m = stage[4 * N + o], rho = stage[5 * N + o], hs = stage[6 * N + o];
+        const double A = stage[7 * N + o], h = stage[8 * N + o];
+        const bool ok = isfinite(x) && isfinite(y) && isfinite(vx) && isfinite(vy) && isfinite(m) &&
+                        isfinite(A) && isfinite(rho) && isfinite(h) && rho > 0.0 && h > 0.0;
+        if (!ok) v[0] += 1.0;
+        if (!(hs == s.hs[i])) v[1] += 1.0;
+        if (ok) {
+            const double dxr = x - xr[i], dyr = y - yr[i];
+            v[2] = fmax(v[2], dxr * dxr + dyr * dyr);
+            if (nl.count[i] >= 0) {
+                const double dxl = x - nl.xl[i], dyl = y - nl.yl[i];
+                v[3] = fmax(v[3], dxl * dxl + dyl * dyl);
+            }
+            v[4] = fmax(v[4], fmax(fabs(x), fabs(y)));
+        }
+        v[5] = fmax(v[5], hs);
+        v[6] = fmax(v[6], -hs);
+        s.x[i] = x;
+        s.y[i] = y;
+        s.vx[i] = vx;
+        s.vy[i] = vy;
+        s.m[i] = m;
+        s.rho[i] = rho;
+        s.mor[i] = m / rho;
+        s.A[i] = A;
+        s.h[i] = h;
+        refresh_views(s, i);
+    }
+    __shared__ double red[7][8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < 7; ++q) {
+        for (int o = 16; o > 0; o >>= 1) {
+            const double t = __shfl_xor_sync(0xffffffffu, v[q], o);
+            v[q] = (q < 2) ? v[q] + t : fmax(v[q], t);
+        }
+        if (lane == 0) red[q][w] = v[q];
+    }
+    __syncthreads();
+    if (threadIdx.x < 7) {
+        const int q = threadIdx.x;
+        double r = red[q][0];
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) r = (q < 2) ? r + red[q][k] : fmax(r, red[q][k]);
+        part[blockIdx.x * kRedVals + q] = r;
+    }
+}
+
+// The bounds of a continued state, as the step epilogue would leave them.
+// (hsml is unchanged, so are its bounds, the bucket size and the skin)
+__global__ void k_continue_finish(Scalars *sc, Inst *inst, double dt, double t, double d2, double dl2,
+                                  double xa, int hsml_evolves) {
+    sc->dt = dt;
+    sc->t = t;
+    inst[0].t = t;
+    const unsigned long long b2 = (unsigned long long)__double_as_longlong(d2);
+    if (b2 > sc->dmax2_bits) sc->dmax2_bits = b2;
+    if (b2 > inst[0].dmax2_bits) inst[0].dmax2_bits = b2;
+    const unsigned long long bl = (unsigned long long)__double_as_longlong(dl2);
+    if (bl > sc->dlist2_bits) sc->dlist2_bits = bl;
+    const unsigned long long bx = (unsigned long long)__double_as_longlong(xa);
+    if (bx > sc->xabs_bits) sc->xabs_bits = bx;
+    // the rule of the stress pass's last block (lists_block_done)
+    const double dl = sqrt(__longlong_as_double((long long)sc->dlist2_bits));
+    if (hsml_evolves || !(dl < 0.75 * sc->skin)) sc->list_scan = 1;
+}
+
 Phys make_phys(const simp_params &p, double max_hsml) {
     Phys P{};
     P.skf = p.skf;
@@ -907,8 +991,10 @@ int step_enqueue(simp_ctx *c, int nsteps) {
     cudaStream_t s = c->stream;
     if (c->n == 0 || nsteps == 0) return SIMP_OK;   // (an empty batch)
     TRY(check_normals(c));
+    // (a grid outgrown by hsml is re-made only at the basin's scheduled
+    // sorts, so the results do not depend on how the steps are split into
+    // calls; until then the stencil radius covers the larger hsml)
     bool regridded = false;
-    TRY(maybe_regrid(c, &regridded));
     launch_reset_stats(c);
     TRY(ensure_graph(c, c->keep_diag));
     if (c->graph_profiled && !c->sort_ev[0])
@@ -979,6 +1065,67 @@ int step_complete(simp_ctx *c, double *current_time, double *dt) {
 int batch_slot_state(simp_ctx *c, int slot, double *x, double *vx, double *mass, double *rho, double *hsml,
                      double *A, double *h, double *t) {
     return get_instance_state(c, slot, x, vx, mass, rho, hsml, A, h, t);
+}
+
+// set_state of a state that continues the resident basin: the same particle
+// count and walls, the same hsml, no particle farther than one cell from
+// where it was sorted, a finite resident state.  The values are written in
+// place (k_continue_state) and the sort, cell lists, Verlet lists and step
+// graph stay.  Returns kFreshState, with the resident state overwritten or
+// not, when the state does not qualify; the caller then sets it up from
+// scratch.  Left out: Benz's kept drhodt (a fresh state zeroes it) and the
+// Wang force's wall normals (a fresh state needs them set again).
+constexpr int kFreshState = -1;   // (not a SIMP_ERR_* code)
+int continue_state(simp_ctx *c, int n, const double *x, const double *vx, const double *mass, const double *rho,
+                   const double *hsml, const double *A, const double *h, int nb, const double *xb,
+                   const double *massb, double dt, double t) {
+    const InstHost &ih = c->insts[0];
+    if (!c->have_state || !ih.active || ih.n != n || ih.nb != nb || c->drhodt || c->prm.bfa == 2)
+        return kFreshState;
+    if (!x || !vx || !mass || !rho || !hsml || !A || !h || (nb > 0 && (!xb || !massb))) return kFreshState;
+    if (nb > 0 && (std::memcmp(ih.xb.data(), xb, sizeof(double) * 2 * (size_t)nb) != 0 ||
+                   std::memcmp(ih.massb.data(), massb, sizeof(double) * (size_t)nb) != 0))
+        return kFreshState;
+    cudaStream_t s = c->stream;
+    const size_t N = (size_t)n;
+    double *stage = c->tmp;
+    SIMP_CUDA(c, cudaMemcpyAsync(stage, x, sizeof(double) * 2 * N, cudaMemcpyHostToDevice, s));
+    SIMP_CUDA(c, cudaMemcpyAsync(stage + 2 * N, vx, sizeof(double) * 2 * N, cudaMemcpyHostToDevice, s));
+    SIMP_CUDA(c, cudaMemcpyAsync(stage + 4 * N, mass, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    SIMP_CUDA(c, cudaMemcpyAsync(stage + 5 * N, rho, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    SIMP_CUDA(c, cudaMemcpyAsync(stage + 6 * N, hsml, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    SIMP_CUDA(c, cudaMemcpyAsync(stage + 7 * N, A, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    SIMP_CUDA(c, cudaMemcpyAsync(stage + 8 * N, h, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    const int rb = std::min(kRedBlocks, nblk(n, 256));
+    NbrList nl;
+    nl.nbr = c->nbr;
+    nl.count = c->nbr_count;
+    nl.xl = c->xl;
+    nl.yl = c->yl;
+    nl.stride = c->maxn;
+    k_continue_state<<<rb, 256, 0, s>>>(n, c->id, stage, c->s0, c->xr, c->yr, nl, c->red_dev);
+    c->launches += 1;
+    SIMP_CUDA(c, cudaGetLastError());
+    SIMP_CUDA(c, cudaMemcpyAsync(c->red_host, c->red_dev, sizeof(double) * kRedVals * rb, cudaMemcpyDeviceToHost, s));
+    SIMP_CUDA(c, cudaMemcpyAsync(c->sc_host, c->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, s));
+    SIMP_CUDA(c, cudaStreamSynchronize(s));
+    double v[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, -INFINITY};
+    for (int b = 0; b < rb; ++b)
+        for (int q = 0; q < 7; ++q) {
+            const double u = c->red_host[b * kRedVals + q];
+            v[q] = (q < 2) ? v[q] + u : std::max(v[q], u);
+        }
+    const Scalars &sc = *c->sc_host;
+    if (v[0] > 0.0 || v[1] > 0.0 || sc.flags != 0 || !(v[2] <= ih.I.cs * ih.I.cs)) return kFreshState;
+    // a fresh state would take max_hsml from its own largest hsml: the run
+    // continues only if that gives the physics constants in use
+    const double max_hsml = (c->prm.max_hsml > 0.0) ? c->prm.max_hsml : v[5] * 10.0;   // initialize.f90:191
+    const Phys P = make_phys(c->prm, max_hsml);
+    if (std::memcmp(&P, &c->phys, sizeof(Phys)) != 0) return kFreshState;
+    k_continue_finish<<<1, 1, 0, s>>>(c->sc, c->inst_dev, dt, t, v[2], v[3], v[4], c->prm.sle != 0 ? 1 : 0);
+    c->launches += 1;
+    SIMP_CUDA(c, cudaGetLastError());
+    return SIMP_OK;
 }
 
 }  // namespace simp
@@ -1073,6 +1220,9 @@ int32_t simp_gpu_set_state(simp_ctx *c, int32_t ntotal, const double *x, const d
                          "The number of boundary particles generated is higher than the maximum "
                          "allowed. (boundaries.f90:296-303)");
     if (ntotal < 1) return simp_fail(c, SIMP_ERR_BADARG, "set_state: bad sizes or null arrays");
+    const int cont = simp::continue_state(c, ntotal, x, vx, mass, rho, hsml, A, h, ntotalb, xb, massb, dt,
+                                          current_time);
+    if (cont != simp::kFreshState) return cont;   // continued in place, or a CUDA error
     reset_all(c);
     c->have_state = false;
     Extents e{};
