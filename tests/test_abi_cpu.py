@@ -92,6 +92,19 @@ def test_fortran_interfaces_name_exported_symbols(lib):
         assert hasattr(lib, n), n
 
 
+def test_fortran_shims_call_only_bound_entry_points():
+    """The drop-in shims (time_integration, single_step) call only entry
+    points the Fortran module binds."""
+    mod = open(os.path.join(ROOT, "fortran", "shim", "simp_gpu_mod.f90")).read()
+    bound = set(re.findall(r"(?:function|subroutine)\s+(simp_\w+)", mod))
+    for shim in ("time_integration_gpu.f90", "single_step_gpu.f90"):
+        src = open(os.path.join(ROOT, "fortran", "shim", shim)).read()
+        code = "\n".join(line.split("!", 1)[0] for line in src.splitlines())
+        used = set(re.findall(r"\b(simp_(?:gpu|params)_\w+)\s*\(", code))
+        assert used, shim
+        assert used <= bound, (shim, used - bound)
+
+
 def test_fortran_mirror_field_order():
     """The bind(C) type in the Fortran shim lists the members in C order."""
     src = open(os.path.join(ROOT, "fortran", "shim", "simp_gpu_mod.f90")).read()
