@@ -142,3 +142,41 @@ def test_invalid_state_is_refused_as_before(gpu_lib):
     with pytest.raises(SimpError):
         _set(g, b, st, rho=rho)
     g.close()
+
+
+def test_host_integrator_over_gpu_single_step(gpu_lib):
+    """The pattern of the single_step shim: the reference's predictor-
+    corrector (time_integration.f90:196-266) on the host, each right-hand
+    side from set_state + single_step.  Every set_state continues in place
+    (the half-step states included), and the trajectory follows the GPU's
+    own time_integration to FP64 rounding."""
+    b = _moving_cfg1(seed=36)
+    rho_ice = b.params.rho_ice
+    g = Simp.from_basin(b)
+    st = g.get_state()
+    dt, t = st["dt"], st["current_time"]
+    x0, v0, h0, A0 = st["x"].copy(), st["vx"].copy(), st["h"].copy(), st["A"].copy()
+
+    def rates(x, v, h, A):
+        launched, _ = _set(g, b, dict(st, x=x, vx=v, h=h, A=A, rho=rho_ice * h, dt=dt, current_time=t))
+        assert launched == 2
+        return g.single_step(t)
+
+    for _ in range(10):
+        r = rates(x0, v0, h0, A0)
+        x1, v1 = x0 + r["dxdt"] * dt / 2, v0 + r["dvxdt"] * dt / 2
+        h1, A1 = h0 + r["dhdt"] * dt / 2, np.minimum(A0 + r["dAdt"] * dt / 2, 1.0)
+        r = rates(x1, v1, h1, A1)
+        x12, v12 = x0 + r["dxdt"] * dt / 2, v0 + r["dvxdt"] * dt / 2
+        h12, A12 = h0 + r["dhdt"] * dt / 2, A0 + r["dAdt"] * dt / 2
+        x0, v0, h0, A0 = 2 * x12 - x0, 2 * v12 - v0, 2 * h12 - h0, np.minimum(2 * A12 - A0, 1.0)
+        t += dt
+    ref = Simp.from_basin(b)
+    ref.time_integration(10)
+    a = ref.get_state()
+    assert a["current_time"] == pytest.approx(t, rel=1e-14)
+    for k, c in (("x", x0), ("vx", v0), ("h", h0), ("A", A0)):
+        base = b.x if k == "x" else 0.0
+        assert rel_l2(c - base, a[k] - base) < 1e-8, (k, rel_l2(c - base, a[k] - base))
+    g.close()
+    ref.close()
