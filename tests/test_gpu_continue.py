@@ -17,6 +17,7 @@ import pytest
 
 from helpers import assert_same_pairs, rel_l2, smooth_velocity
 from simp_b200 import basins
+from simp_b200.params import PREC_MIXED
 from simp_b200.simp import Simp
 
 pytestmark = pytest.mark.gpu
@@ -44,10 +45,12 @@ def _moving_cfg1(amp=0.5, seed=31):
     return b
 
 
-@pytest.mark.parametrize("switches", ["cfg1", "reference_defaults"])
+@pytest.mark.parametrize("switches", ["cfg1", "reference_defaults", "mixed"])
 def test_handing_back_the_state_is_the_device_resident_run(gpu_lib, switches):
     b = _moving_cfg1()
     prm = b.params.copy()
+    if switches == "mixed":
+        prm.precision = PREC_MIXED
     if switches == "reference_defaults":
         # Marquis hsml (sle 2) and the VP time step (tse 2): hsml and dt
         # change every step, and the lists are rebuilt every step
