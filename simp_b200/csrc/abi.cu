@@ -698,7 +698,7 @@ int download1(simp_ctx *c, const double *a, double *h1) {
 }
 
 int get_instance_state(simp_ctx *c, int slot, double *x, double *vx, double *mass, double *rho, double *hsml,
-                       double *A, double *h, double *t) {
+                       double *A, double *h, double *t, bool with_scalars = false) {
     const InstHost &ih = c->insts[slot];
     const int nk = ih.n;
     const size_t N = (size_t)nk;
@@ -715,6 +715,8 @@ int get_instance_state(simp_ctx *c, int slot, double *x, double *vx, double *mas
             SIMP_CUDA(c, cudaMemcpyAsync(o.dst, stage + o.off, sizeof(double) * o.len, cudaMemcpyDeviceToHost, s));
     Inst I{};
     SIMP_CUDA(c, cudaMemcpyAsync(&I, c->inst_dev + slot, sizeof(Inst), cudaMemcpyDeviceToHost, s));
+    // (the scalars in the same wait, for get_state)
+    if (with_scalars) SIMP_CUDA(c, cudaMemcpyAsync(c->sc_host, c->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, s));
     SIMP_CUDA(c, cudaStreamSynchronize(s));
     if (t) *t = I.t;
     return SIMP_OK;
@@ -1350,8 +1352,7 @@ int32_t simp_gpu_get_state(simp_ctx *c, double *x, double *vx, double *mass, dou
                            double *hsml, double *A, double *h, double *dt, double *current_time) {
     if (!c) return SIMP_ERR_BADARG;
     if (!c->have_state || !c->insts[0].active) return simp_fail(c, SIMP_ERR_STATE, "get_state before set_state");
-    TRY(get_instance_state(c, 0, x, vx, mass, rho, hsml, A, h, nullptr));
-    TRY(read_scalars(c));
+    TRY(get_instance_state(c, 0, x, vx, mass, rho, hsml, A, h, nullptr, true));
     if (dt) *dt = c->sc_host->dt;
     if (current_time) *current_time = c->sc_host->t;
     return SIMP_OK;
