@@ -424,16 +424,16 @@ def run_e2e(sim, b, stream, nsteps, dist):
         dist.barrier()
     torch.cuda.synchronize()
     e0.record(stream)
+    # the host arrays' pointers, taken once (a Fortran or C host passes them as they are)
+    state_ptrs = [P(host[k]) for k in ("x", "vx", "mass", "rho", "hsml", "A", "h")]
+    wall_ptrs = [P(xb), P(massb)]
+    ptc, pdtc = ctypes.byref(tc), ctypes.byref(dtc)
     for _ in range(nsteps):
-        rc = lib.simp_gpu_set_state(sim.h, n, P(host["x"]), P(host["vx"]), P(host["mass"]), P(host["rho"]),
-                                    P(host["hsml"]), P(host["A"]), P(host["h"]), nb, P(xb), P(massb),
-                                    float(dt), float(t_now))
+        rc = lib.simp_gpu_set_state(sim.h, n, *state_ptrs, nb, *wall_ptrs, float(dt), float(t_now))
         assert rc == 0, lib.simp_gpu_last_error(sim.h)
-        rc = lib.simp_gpu_step(sim.h, 1, ctypes.byref(tc), ctypes.byref(dtc))
+        rc = lib.simp_gpu_step(sim.h, 1, ptc, pdtc)
         assert rc == 0, lib.simp_gpu_last_error(sim.h)
-        rc = lib.simp_gpu_get_state(sim.h, P(host["x"]), P(host["vx"]), P(host["mass"]), P(host["rho"]),
-                                    P(host["hsml"]), P(host["A"]), P(host["h"]), ctypes.byref(dtc),
-                                    ctypes.byref(tc))
+        rc = lib.simp_gpu_get_state(sim.h, *state_ptrs, pdtc, ptc)
         assert rc == 0, lib.simp_gpu_last_error(sim.h)
         t_now, dt = tc.value, dtc.value
     e1.record(stream)
