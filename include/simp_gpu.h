@@ -297,7 +297,7 @@ SIMP_API void *simp_gpu_stream(simp_ctx *ctx);
  * lists, with the kinematic pass as one kernel (SIMP_PASSES_GATHER_ONE) or
  * as two, pair finding then pair sums over the stored pair list
  * (SIMP_PASSES_GATHER_TWO); SIMP_PASSES_GATHER (the default) takes two
- * kernels for plain FP64 contexts of up to 400,000 particles, else one.
+ * kernels for contexts of up to 400,000 particles, else one.
  * All give the same bits.  threads: 64..256, a multiple of 32; cap: a
  * multiple of 4, within the shared memory of one block (both checked for
  * every form). */

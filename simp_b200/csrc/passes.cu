@@ -14,15 +14,15 @@ namespace {
 using namespace pass;
 
 constexpr int kBlock = 128;
-// Up to this many particles in a context the plain FP64 kinematic pass runs
-// as two kernels (k_find_pairs, k_kin_sums), above it as one (k_kinematic),
-// unless the context names one form (SIMP_PASSES_GATHER_ONE / _TWO).
-// The two-kernel pass writes and re-reads the pair list, which pays while
-// that round trip stays in L2.  Per pass, one kernel -> two (B200, basins of
-// the 500 m lattice): 147,456 particles 64.6 -> 55.1 us, 262,144 96.4 ->
+// Up to this many particles in a context the kinematic pass runs as two
+// kernels (k_find_pairs, k_kin_sums), above it as one (k_kinematic), unless
+// the context names one form (SIMP_PASSES_GATHER_ONE / _TWO).  The
+// two-kernel pass writes and re-reads the pair list, which pays while that
+// round trip stays in L2.  Per pass, one kernel -> two (B200, basins of the
+// 500 m lattice), FP64: 147,456 particles 64.6 -> 55.1 us, 262,144 96.4 ->
 // 89.2, 409,600 143.0 -> 143.3, 524,176 170.5 -> 179.8, 1,048,576 305.7 ->
-// 343.9.  The mixed form always runs one kernel: on 1,048,576 particles the
-// two-kernel pass took 267 us against 241.
+// 343.9; mixed: 147,456 66.5 -> 53.3, 262,144 100.1 -> 87.5, 409,600
+// 134.7 -> 131.9, 1,048,576 241 -> 267.
 constexpr int kSplitMaxParticles = 400000;
 // minimum resident blocks per SM, per precision form, measured against 4..8
 // (cfg2 FP64, cfg3 mixed): the FP64 kinematic pass keeps its pair math in
@@ -517,7 +517,7 @@ void launch_kinematic(simp_ctx *c, const State &s, bool diag) {
     const int g = nblk(c->n, kBlock);
     const bool mixed = c->prm.precision == SIMP_PREC_MIXED;
     const bool two = c->pass_impl == SIMP_PASSES_GATHER_TWO ||
-                     (c->pass_impl == SIMP_PASSES_GATHER && !mixed && c->n <= kSplitMaxParticles);
+                     (c->pass_impl == SIMP_PASSES_GATHER && c->n <= kSplitMaxParticles);
     if (!two) {
         switch (skf_compiled(c->prm.skf)) {
             case SIMP_SKF_CUBIC:
