@@ -29,6 +29,9 @@ module simp_gpu_mod
                           vortex_x, vortex_y, vortex_umax, vortex_radius,   &
                           dt, max_hsml, skin, zeta_max, eta_max, phi,       &
                           xi, Y, nu
+        integer(c_int32_t) :: artificial_visc, xsph_regularization,         &
+                              art_visc_alg, reserved1
+        real(c_double) :: alpha_pi, beta_pi, chi
     end type simp_params
 
     ! Mirror of struct simp_forcing (per-basin wind of a batch).

@@ -6,8 +6,8 @@
 !   back.  While the state continues the one of the previous call (same   !
 !   particles, walls and hsml, moved less than a cell) the library keeps  !
 !   its sort and neighbour lists, so a call costs the two copies and one  !
-!   right-hand side.  Link with -lsimp_gpu; compile simp_gpu_mod.f90      !
-!   first, and leave the reference's single_step.f90 out of the build.    !
+!   right-hand side.  Link with -lsimp_gpu; compile simp_gpu_mod.f90 and  !
+!   simp_host_params.f90 first, and leave the reference's single_step.f90 out of the build.    !
 !!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!
 module simp_single_step_ctx
     use, intrinsic :: iso_c_binding
@@ -21,6 +21,7 @@ subroutine single_step
     use globals
     use data_variables
     use simp_gpu_mod
+    use simp_host_params_mod
     use simp_single_step_ctx
 
     implicit none
@@ -29,9 +30,8 @@ subroutine single_step
     integer(c_int32_t) :: rc
 
     IF (.NOT. c_associated(ss_ctx)) THEN
-        ! switches and constants of globals.f90 / data_variables.f90
-        call simp_params_reference_default(prm)
-        prm%dt = dt
+        ! the host's switches and constants (globals.f90, data_variables.f90)
+        call simp_params_from_host(prm)
         rc = simp_gpu_create(prm, int(maxn, c_int32_t), int(maxnb, c_int32_t), ss_ctx)
         call simp_gpu_stop(ss_ctx, rc)
     ENDIF

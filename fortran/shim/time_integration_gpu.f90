@@ -3,7 +3,8 @@
 !   time_integration.f90:6-71) that runs the predictor-corrector on       !
 !   the GPU.  State goes up once, steps stay resident, and the module     !
 !   globals are refreshed only when output is due (save_step).            !
-!   Link with -lsimp_gpu; compile simp_gpu_mod.f90 first.                  !
+!   Link with -lsimp_gpu; compile simp_gpu_mod.f90 and                   !
+!   simp_host_params.f90 first.                                            !
 !!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!!
 subroutine time_integration
 
@@ -11,6 +12,7 @@ subroutine time_integration
     use globals
     use data_variables
     use simp_gpu_mod
+    use simp_host_params_mod
 
     implicit none
 
@@ -19,9 +21,8 @@ subroutine time_integration
     integer(c_int32_t) :: rc, nchunk
     REAL(kind=8) :: last_save, t_gpu, dt_gpu
 
-    ! switches and constants of globals.f90 / data_variables.f90
-    call simp_params_reference_default(prm)
-    prm%dt = dt
+    ! the host's switches and constants (globals.f90, data_variables.f90)
+    call simp_params_from_host(prm)
 
     rc = simp_gpu_create(prm, int(maxn, c_int32_t), int(maxnb, c_int32_t), ctx)
     call simp_gpu_stop(ctx, rc)

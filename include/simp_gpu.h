@@ -130,6 +130,21 @@ typedef struct simp_params {
        xi of bf_Wang, Young modulus Y and Poisson ratio nu of the sound speed
        c_yang used by bf_Monaghan's friction term */
     double xi, Y, nu;
+    /* regularisation (sph/regularization.f90), called by single_step when
+       xsph_regularization or artificial_visc is on (single_step.f90:99-101);
+       it then applies the artificial viscosity of art_visc_alg whichever of
+       the two switches is on (regularization.f90:29-35), as the reference
+       does.  The pair terms are evaluated per pair: a pair outside the
+       viscosity criterion contributes nothing, and the XSPH term is
+       antisymmetric (x_i gets m_j (v_i - v_j), x_j gets m_i (v_j - v_i)). */
+    int32_t artificial_visc;     /* globals.f90:180-187 (0/1)                    */
+    int32_t xsph_regularization; /* globals.f90:180-187 (0/1)                    */
+    int32_t art_visc_alg;        /* 1 Hernquist-Katz (regularization.f90:102-213),
+                                    2 Monaghan (:220-308); globals.f90:103      */
+    int32_t reserved1;
+    double alpha_pi, beta_pi;    /* artificial viscosity coefficients
+                                    (data_variables.f90:171-172)               */
+    double chi;                  /* XSPH coefficient (data_variables.f90:173)   */
 } simp_params;
 
 /* Shipped values of globals.f90 and data_variables.f90, including the

@@ -1187,6 +1187,12 @@ void simp_params_reference_default(simp_params *p) {
     p->xi = (double)0.5225f;   // default-real literals (data_variables.f90:158, 175)
     p->Y = 1.0e9;
     p->nu = (double)0.3f;
+    p->artificial_visc = 0;    // globals.f90:180-187
+    p->xsph_regularization = 0;
+    p->art_visc_alg = 1;       // globals.f90:103
+    p->alpha_pi = 1.0;         // data_variables.f90:171-173
+    p->beta_pi = 2.0;
+    p->chi = (double)0.3f;
 }
 
 int32_t simp_gpu_create(const simp_params *params, int32_t maxn, int32_t maxnb, simp_ctx **out) {

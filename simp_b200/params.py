@@ -53,11 +53,19 @@ _DBL_FIELDS = [
     "zeta_max", "eta_max", "phi",
     "xi", "Y", "nu",
 ]
+# regularisation switches and constants (after the doubles above)
+_TAIL_FIELDS = [
+    ("artificial_visc", ctypes.c_int32), ("xsph_regularization", ctypes.c_int32),
+    ("art_visc_alg", ctypes.c_int32), ("reserved1", ctypes.c_int32),
+    ("alpha_pi", ctypes.c_double), ("beta_pi", ctypes.c_double), ("chi", ctypes.c_double),
+]
+ART_VISC_HK = 1     # Hernquist and Katz (regularization.f90:102-213)
+ART_VISC_MON = 2    # Monaghan (regularization.f90:220-308)
 
 
 class SimpParams(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int32) for n in _INT_FIELDS] + [
-        (n, ctypes.c_double) for n in _DBL_FIELDS]
+        (n, ctypes.c_double) for n in _DBL_FIELDS] + _TAIL_FIELDS
 
     def copy(self) -> "SimpParams":
         out = SimpParams()
@@ -168,6 +176,12 @@ def reference_default() -> SimpParams:
     p.xi = _real4(0.5225)     # data_variables.f90:175, a default-real literal
     p.Y = 1.0e9               # :157
     p.nu = _real4(0.3)        # :158
+    p.artificial_visc = 0     # globals.f90:180-187
+    p.xsph_regularization = 0
+    p.art_visc_alg = ART_VISC_HK  # globals.f90:103
+    p.alpha_pi = 1.0          # data_variables.f90:171
+    p.beta_pi = 2.0           # :172
+    p.chi = _real4(0.3)       # :173, a default-real literal
     return p
 
 

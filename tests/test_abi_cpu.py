@@ -97,12 +97,43 @@ def test_fortran_shims_call_only_bound_entry_points():
     points the Fortran module binds."""
     mod = open(os.path.join(ROOT, "fortran", "shim", "simp_gpu_mod.f90")).read()
     bound = set(re.findall(r"(?:function|subroutine)\s+(simp_\w+)", mod))
-    for shim in ("time_integration_gpu.f90", "single_step_gpu.f90"):
+    bound.add("simp_params_from_host")   # simp_host_params.f90
+    for shim in ("time_integration_gpu.f90", "single_step_gpu.f90", "simp_host_params.f90"):
         src = open(os.path.join(ROOT, "fortran", "shim", shim)).read()
         code = "\n".join(line.split("!", 1)[0] for line in src.splitlines())
         used = set(re.findall(r"\b(simp_(?:gpu|params)_\w+)\s*\(", code))
         assert used, shim
         assert used <= bound, (shim, used - bound)
+
+
+# simp_params members the reference has no variable for: the hard-coded
+# wind and current (wind_forcing.f90:36-37, water_drag.f90:36-37) and the
+# GPU's own settings
+_NOT_FROM_HOST = {"wind_u", "wind_v", "current_u", "current_v", "vortex_x", "vortex_y", "vortex_umax",
+                  "vortex_radius", "wind_kind", "precision", "skin", "mass_from_area", "reserved0",
+                  "reserved1"}
+
+
+def test_fortran_shims_take_the_hosts_parameters():
+    """The drop-in shims build their simp_params from the host's modules:
+    every member with a counterpart in globals.f90 / data_variables.f90 is
+    assigned from the variable of the same name, and both shims use that
+    routine rather than the library's compiled-in defaults."""
+    src = open(os.path.join(ROOT, "fortran", "shim", "simp_host_params.f90")).read()
+    code = "\n".join(line.split("!", 1)[0] for line in src.splitlines())
+    assigned = {}
+    for m in re.finditer(r"prm%(\w+)\s*=\s*(.+)", code):
+        assigned[m.group(1).lower()] = m.group(2)
+    for f, _ in SimpParams._fields_:
+        if f in _NOT_FROM_HOST:
+            continue
+        assert f.lower() in assigned, f"simp_params%{f} is not taken from the host"
+        assert re.search(rf"\b{f}\b", assigned[f.lower()], re.I), (f, assigned[f.lower()])
+    for shim in ("time_integration_gpu.f90", "single_step_gpu.f90"):
+        body = open(os.path.join(ROOT, "fortran", "shim", shim)).read()
+        body = "\n".join(line.split("!", 1)[0] for line in body.splitlines())
+        assert "call simp_params_from_host(prm)" in body, shim
+        assert "simp_params_reference_default" not in body, shim
 
 
 def test_fortran_mirror_field_order():
