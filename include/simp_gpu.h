@@ -49,7 +49,9 @@ enum {
     SIMP_ERR_NONFINITE = 6, /* NaN/Inf in the state after a step               */
     SIMP_ERR_TIMEOUT = 7,   /* a bounded device-side wait gave up              */
     SIMP_ERR_NOMEM = 8,     /* device allocation failed                        */
-    SIMP_ERR_STATE = 9      /* entry point called before simp_gpu_set_state    */
+    SIMP_ERR_STATE = 9,     /* entry point called before simp_gpu_set_state    */
+    SIMP_ERR_BOUNDS = 10    /* a device index check failed (only the checked
+                               debug build, libsimp_gpu_checked.so, checks)  */
 };
 
 /* Smoothing kernel selector: the reference's skf codes (globals.f90:136-147,
@@ -83,8 +85,9 @@ typedef struct simp_params {
     int32_t nnps_algorithm;    /* 2 bucket search, 1 direct find (nnps.f90:21-30)       */
     int32_t sle;               /* 0 keep hsml, 1 Benz hsml, 2 Marquis hsml
                                   (smoothing_length.f90:24-30)                          */
-    int32_t tse;               /* 0 keep dt, 1 Monaghan (time_step.f90:40-103, without
-                                  artificial viscosity), 2 VP criterion (:132-157)     */
+    int32_t tse;               /* 0 keep dt, 1 Monaghan (time_step.f90:40-124, its CFL
+                                  criterion with the artificial-viscosity form when
+                                  artificial_visc), 2 VP criterion (:132-157)         */
     int32_t rheology;          /* 1 elliptical yield curve, 2 Mohr-Coulomb
                                   (bulk_viscosity.f90, shear_viscosity.f90)           */
     int32_t eos_alg;           /* 1 Hibler, 2 Gutfraind, 3 Kreyscher (eos.f90)         */

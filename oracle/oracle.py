@@ -53,6 +53,7 @@ def lib():
         L.orc_boundary_fdwdq.restype = ctypes.c_double
         L.orc_boundary_fdwdq.argtypes = [ctypes.c_void_p, ctypes.c_double]
         L.orc_set_wall_normals.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+        L.orc_set_regularization_form.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_interaction_stats.argtypes = [ctypes.c_void_p, _ip, _ip, ctypes.POINTER(ctypes.c_longlong), _ip]
         L.orc_set_threads.argtypes = [ctypes.c_int]
         L.orc_max_threads.restype = ctypes.c_int
@@ -114,6 +115,11 @@ class Oracle:
         if prm.bfa == 2 and b.nb > 0 and getattr(b, "bn", None) is not None:
             o.set_wall_normals(b.bn)
         return o
+
+    def set_regularization_form(self, literal: bool):
+        """Regularisation pair loops: per pair (False, the library's form) or
+        the reference's serial loops literally (True)."""
+        self._chk(lib().orc_set_regularization_form(self.h, 1 if literal else 0))
 
     def set_wall_normals(self, b_normal):
         bn = np.ascontiguousarray(b_normal, np.float64).reshape(-1, 2)

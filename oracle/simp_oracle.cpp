@@ -62,6 +62,12 @@ struct Orc {
     std::vector<int> count_np;
     std::string err;
     bool bad = false;   // the state blew up (no bucket grid could be built)
+    // regularisation pair loops: 0 per pair (a pair outside the viscosity
+    // criterion contributes nothing, XSPH antisymmetric: the library's
+    // form); 1 the reference's serial loops literally (pi_ij keeps the last
+    // pair's value, regularization.f90:193-196, 285-291; XSPH adds the same
+    // signed term to both particles, :82-89)
+    int reg_literal = 0;
 };
 
 // ---------------------------------------------------------------------------
@@ -666,6 +672,86 @@ void external_forces(Orc &o) {
     }
 }
 
+// The sound speed the reference keeps in c(:): c_yang of the current density
+// when sound_speed refreshes it (artificial viscosity, Monaghan time step or
+// boundary friction, sound_speed.f90:21-27), else never set (zero).
+bool sound_speed_on(const simp_params &P) {
+    return P.artificial_visc || P.tse == 1 || P.boundary_friction;
+}
+
+// regularization.f90:5-310, called by single_step.f90:99-101 after the drag
+// terms: XSPH (:45-95) when xsph_regularization, then the artificial
+// viscosity of art_visc_alg (:29-35), Hernquist-Katz (:102-213) or Monaghan
+// (:220-308), whichever of the two switches brought it here.  Both loops run
+// serially over the pair list with the last right-hand side's w and dwdx.
+void regularization(Orc &o) {
+    const simp_params &P = o.P;
+    const int n = o.ntotal;
+    const bool lit = o.reg_literal != 0;
+    if (P.xsph_regularization) {
+        std::vector<double> xs(2 * (size_t)n, 0.0);
+        for (int k = 0; k < o.nip; ++k) {
+            const int i = o.p_i[k] - 1, j = o.p_j[k] - 1;
+            const double dvx[2] = {o.vx[2 * i] - o.vx[2 * j], o.vx[2 * i + 1] - o.vx[2 * j + 1]};
+            const double rbar = 0.5 * (o.rho[i] + o.rho[j]);
+            for (int d = 0; d < 2; ++d) {
+                xs[2 * i + d] = xs[2 * i + d] + o.mass[j] * dvx[d] * o.w[k] / rbar;
+                const double tj = o.mass[i] * dvx[d] * o.w[k] / rbar;
+                xs[2 * j + d] = lit ? xs[2 * j + d] + tj : xs[2 * j + d] - tj;
+            }
+        }
+        for (size_t q = 0; q < 2 * (size_t)n; ++q) o.dxdt[q] = o.dxdt[q] - P.chi * xs[q];   // :93
+    }
+    if (P.art_visc_alg == 1) {
+        std::vector<double> div(n, 0.0), lv(n);
+        for (int k = 0; k < o.nip; ++k) {                                 // :148-167
+            const int i = o.p_i[k] - 1, j = o.p_j[k] - 1;
+            const double dvx[2] = {o.vx[2 * i] - o.vx[2 * j], o.vx[2 * i + 1] - o.vx[2 * j + 1]};
+            const double w1 = dvx[0] * o.dwdx[2 * k], w4 = dvx[1] * o.dwdx[2 * k + 1];
+            div[i] = div[i] - o.mass[j] * (w1 + w4) / o.rho[i];
+            div[j] = div[j] - o.mass[i] * (w1 + w4) / o.rho[j];
+        }
+        for (int i = 0; i < n; ++i) {                                     // :170-176
+            if (div[i] >= 0.0) div[i] = 0.0;
+            lv[i] = (P.alpha_pi * o.hsml[i] * o.c[i] * std::fabs(div[i]) +
+                     P.beta_pi * p2(std::fabs(div[i]) * o.hsml[i])) * o.rho[i];
+        }
+        double pi_ij = 0.0;
+        for (int k = 0; k < o.nip; ++k) {                                 // :179-211
+            const int i = o.p_i[k] - 1, j = o.p_j[k] - 1;
+            const double dx[2] = {o.x[2 * i] - o.x[2 * j], o.x[2 * i + 1] - o.x[2 * j + 1]};
+            const double dvx[2] = {o.vx[2 * i] - o.vx[2 * j], o.vx[2 * i + 1] - o.vx[2 * j + 1]};
+            const double crit = dvx[0] * dx[0] + dvx[1] * dx[1];
+            if (crit <= 0.0) pi_ij = lv[i] / p2(o.rho[i]) + lv[j] / p2(o.rho[j]);
+            else if (!lit) pi_ij = 0.0;
+            for (int d = 0; d < 2; ++d) {
+                o.dvxdt[2 * i + d] = o.dvxdt[2 * i + d] - o.mass[j] * pi_ij * o.dwdx[2 * k + d];
+                o.dvxdt[2 * j + d] = o.dvxdt[2 * j + d] + o.mass[i] * pi_ij * o.dwdx[2 * k + d];
+            }
+        }
+    } else if (P.art_visc_alg == 2) {
+        double pi_ij = 0.0;
+        for (int k = 0; k < o.nip; ++k) {                                 // :268-306
+            const int i = o.p_i[k] - 1, j = o.p_j[k] - 1;
+            const double dx[2] = {o.x[2 * i] - o.x[2 * j], o.x[2 * i + 1] - o.x[2 * j + 1]};
+            const double dvx[2] = {o.vx[2 * i] - o.vx[2 * j], o.vx[2 * i + 1] - o.vx[2 * j + 1]};
+            const double v_r = dvx[0] * dx[0] + dvx[1] * dx[1];
+            const double s_cor = real4(0.01f) * o.hsml_ij[k];
+            if (v_r <= 0.0) {
+                const double iota = o.hsml_ij[k] * v_r / (p2(o.r_ij[k]) + p2(s_cor));
+                pi_ij = (P.beta_pi * p2(iota) - P.alpha_pi * iota * (o.c[i] + o.c[j]) / 2) /
+                        ((o.rho[i] + o.rho[j]) / 2);
+            } else if (!lit) {
+                pi_ij = 0.0;
+            }
+            for (int d = 0; d < 2; ++d) {
+                o.dvxdt[2 * i + d] = o.dvxdt[2 * i + d] - o.mass[j] * pi_ij * o.dwdx[2 * k + d];
+                o.dvxdt[2 * j + d] = o.dvxdt[2 * j + d] + o.mass[i] * pi_ij * o.dwdx[2 * k + d];
+            }
+        }
+    }
+}
+
 // single_step.f90:5-109.
 void single_step(Orc &o) {
     const int n = o.ntotal;
@@ -713,6 +799,7 @@ void single_step(Orc &o) {
     internal_stress(o);                                             // :87
     if (o.P.boundary_pressure || o.P.boundary_friction) boundary_kernel(o);  // :90-92
     external_forces(o);                                             // :95-96
+    if (o.P.xsph_regularization || o.P.artificial_visc) regularization(o);   // :99-101
     for (int i = 0; i < n; ++i) {                                   // :104-106
         o.dhdt[i] = -o.h[i] * div[i] / o.rho[i];
         o.dAdt[i] = -o.A[i] * div[i] / o.rho[i];
@@ -776,7 +863,7 @@ void density(Orc &o) {
 // sound_speed.f90:20-27 with c_yang :54-55: only when something reads c.
 void sound_speed(Orc &o) {
     const simp_params &P = o.P;
-    if (!P.boundary_friction && P.tse != 1) return;   // (artificial_visc is off)
+    if (!sound_speed_on(P)) return;
     for (int i = 0; i < o.ntotal; ++i)
         o.c[i] = std::pow(P.Y * (1 - P.nu) / (o.rho[i] * (1 + P.nu) * (1 - 2 * P.nu)), 0.5);
 }
@@ -821,16 +908,33 @@ void smoothing_length(Orc &o) {
     }
 }
 
-// time_step.f90:40-103 (Monaghan_time_step, artificial_visc off): the
-// force criterion from the last right-hand side's accelerations and the
-// CFL criterion from the sound speed.
+// time_step.f90:40-124 (Monaghan_time_step): the force criterion from the
+// last right-hand side's accelerations and the CFL criterion from the sound
+// speed; with artificial viscosity the CFL criterion also takes the velocity
+// divergence over the last right-hand side's pairs and kernel gradients with
+// the current velocities, masses and densities (:89-115).
 void monaghan_time_step(Orc &o) {
     const int n = o.ntotal;
+    const simp_params &P = o.P;
     const double fF = 0.25;
+    std::vector<double> div(n, 0.0);
+    if (P.artificial_visc) {
+        for (int k = 0; k < o.nip; ++k) {
+            const int i = o.p_i[k] - 1, j = o.p_j[k] - 1;
+            const double dvx[2] = {o.vx[2 * i] - o.vx[2 * j], o.vx[2 * i + 1] - o.vx[2 * j + 1]};
+            const double w1 = dvx[0] * o.dwdx[2 * k], w4 = dvx[1] * o.dwdx[2 * k + 1];
+            div[i] = div[i] - o.mass[j] * (w1 + w4) / o.rho[i];
+            div[j] = div[j] - o.mass[i] * (w1 + w4) / o.rho[j];
+        }
+    }
     double mf = 0.0, mc = 0.0;
     for (int i = 0; i < n; ++i) {
         const double acc = std::pow(p2(o.dvxdt[2 * i]) + p2(o.dvxdt[2 * i + 1]), 0.5);
-        const double a = o.hsml[i] / acc, c = o.hsml[i] / o.c[i];
+        const double a = o.hsml[i] / acc;
+        const double c = P.artificial_visc
+            ? real4(0.3f) * o.hsml[i] / (o.c[i] + o.hsml[i] * std::fabs(div[i]) +
+                                         real4(1.2f) * (P.alpha_pi * o.c[i] + P.beta_pi * o.hsml[i] * std::fabs(div[i])))
+            : o.hsml[i] / o.c[i];
         mf = (i == 0) ? a : std::min(mf, a);
         mc = (i == 0) ? c : std::min(mc, c);
     }
@@ -1034,6 +1138,13 @@ int orc_set_state(void *hh, int n, const double *x, const double *vx, const doub
     o->max_hsml = (o->P.max_hsml > 0.0) ? o->P.max_hsml : mh * 10.0;  // initialize.f90:191
     o->nip = o->bnip = 0;
     sound_speed(*o);                                                   // initialize.f90:200
+    return 0;
+}
+
+// Form of the regularisation pair loops: 0 per pair (the library's), 1 the
+// reference's serial loops literally.
+int orc_set_regularization_form(void *hh, int literal) {
+    ((Orc *)hh)->reg_literal = literal ? 1 : 0;
     return 0;
 }
 

@@ -278,6 +278,16 @@ Phys make_phys(const simp_params &p, double max_hsml) {
     P.xi = p.xi;
     P.Y = p.Y;
     P.nu = p.nu;
+    // regularization is called when either switch is on, and then applies
+    // the artificial viscosity of art_visc_alg (regularization.f90:23-35)
+    const bool reg = p.xsph_regularization || p.artificial_visc;
+    P.xsph = p.xsph_regularization ? 1 : 0;
+    P.art_visc = (reg && (p.art_visc_alg == 1 || p.art_visc_alg == 2)) ? p.art_visc_alg : 0;
+    P.artificial_visc = p.artificial_visc ? 1 : 0;
+    P.csound = (p.artificial_visc || p.tse == 1 || p.boundary_friction) ? 1 : 0;   // sound_speed.f90:21
+    P.alpha_pi = p.alpha_pi;
+    P.beta_pi = p.beta_pi;
+    P.chi = p.chi;
     return P;
 }
 
@@ -320,7 +330,7 @@ void free_all(simp_ctx *c) {
                     c->pair_j, c->pair_count, c->nbr_tmp, c->s0.hsf,
                     c->inst_dev, c->row_map, c->chunk_cnt, c->chunk_off, c->chunks, c->s0.xy, c->s0.vxy,
                     c->s0.pf, c->s0.mm, c->s0.hmm, c->s1.xy, c->s1.vxy, c->s1.pf, c->s1.mm, c->s1.hmm,
-                    c->tau_a, c->tau_b, c->tau_q, c->pair_dw, c->drhodt, c->red_dev};
+                    c->tau_a, c->tau_b, c->tau_q, c->pair_dw, c->drhodt, c->red_dev, c->reg};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->sc_host) cudaFreeHost(c->sc_host);
@@ -730,14 +740,18 @@ void enqueue_step(simp_ctx *c, bool diag, bool prof) {
     };
     // continuity density (den_alg 2) and Benz hsml (sle 1) add a density-rate
     // pass after an update (timed with the stress pass before it)
+    // (and so does the Monaghan time step with artificial viscosity, whose
+    // divergence takes the updated velocities)
     const bool den2 = c->prm.den_alg == 2, benz = c->prm.sle == 1;
+    const bool tsdiv = c->prm.tse == 1 && c->prm.artificial_visc;
     mark(0);
     if (c->prm.int_algorithm == 1) {
         // euler_scheme (time_integration.f90:86-148): one right-hand side
         launch_kinematic(c, c->s0, diag);
+        launch_regularize(c, c->s0);
         mark(1);
         launch_stress(c, c->s0, c->s0, EPI_EULER);
-        if (den2 || benz) launch_density_rate(c, c->s0, c->s1, den2 ? 2 : 0, true);
+        if (den2 || benz || tsdiv) launch_density_rate(c, c->s0, c->s1, den2 ? 2 : 0, true);
         mark(2);
         launch_copy_s1_to_s0(c);
         mark(3);
@@ -747,14 +761,17 @@ void enqueue_step(simp_ctx *c, bool diag, bool prof) {
         // same first half step, a different final update
         const bool leap = c->prm.int_algorithm == 3;
         launch_kinematic(c, c->s0, false);
+        launch_regularize(c, c->s0);
         mark(1);
         launch_stress(c, c->s0, c->s0, EPI_PREDICT);
         if (den2) launch_density_rate(c, c->s0, c->s1, 1, false);
         mark(2);
         launch_kinematic(c, c->s1, diag);
+        launch_regularize(c, c->s1);
         mark(3);
         launch_stress(c, c->s1, c->s0, leap ? EPI_LEAP : EPI_CORRECT);
-        if (leap ? (den2 || benz) : benz) launch_density_rate(c, c->s1, c->s0, (leap && den2) ? 2 : 0, true);
+        if (leap ? (den2 || benz || tsdiv) : (benz || tsdiv))
+            launch_density_rate(c, c->s1, c->s0, (leap && den2) ? 2 : 0, true);
         mark(4);
     }
     launch_step_finish(c);
@@ -828,6 +845,9 @@ int maybe_regrid(simp_ctx *c, bool *done) {
 }
 
 int check_after(simp_ctx *c) {
+    if (const unsigned f = take_bounds_flags())
+        return simp_fail(c, SIMP_ERR_BOUNDS, "device index check failed (sites " + std::to_string(f) +
+                                                 ": 1 neighbour, 2 cell, 4 sort slot, 8 tile slot)");
     const Scalars &s = *c->sc_host;
     if ((s.flags & FLAG_NONFINITE) && c->max_inst == 1)   // batches flag the basin instead
         return simp_fail(c, SIMP_ERR_NONFINITE, "non-finite particle state after a step");
@@ -898,6 +918,7 @@ int create(const simp_params *params, int32_t maxn, int32_t maxnb, int32_t max_i
     }
     TRY(dalloc(c, &c->diag, 9 * M));
     TRY(dalloc(c, &c->rates, 4 * M));
+    if (c->prm.xsph_regularization || c->prm.artificial_visc) TRY(dalloc(c, &c->reg, 4 * M));
     TRY(dalloc(c, &c->cell, M));
     TRY(dalloc(c, &c->id, M));
     TRY(dalloc(c, &c->pinst, M));
@@ -956,6 +977,23 @@ simp_forcing forcing_of(const simp_params &p) {
 
 namespace simp {
 
+// Flag words of the debug build's index checks (check.cuh), one reader per
+// translation unit built with them.
+static std::vector<unsigned (*)()> &bounds_readers() {
+    static std::vector<unsigned (*)()> v;
+    return v;
+}
+int register_bounds_reader(unsigned (*take)()) {
+    bounds_readers().push_back(take);
+    return 1;
+}
+unsigned take_bounds_flags() {
+    unsigned f = 0u;
+    for (auto take : bounds_readers()) f |= take();
+    return f;
+}
+
+
 // bf_Wang reads b_normal (boundary_force.f90:146-147), which the reference
 // sets with the walls (boundaries.f90:232-287): a basin with walls needs
 // them before its first right-hand side.
@@ -981,6 +1019,7 @@ double bytes_per_particle(const simp_params &p) {
     b += mixed ? kDwRows * 8.0 : 0.0;                         // kept kernel gradients
     b += 9 * 8.0 + 4 * 8.0;                                   // diagnostics, rates
     if (p.sle == 1 && p.den_alg != 2) b += 8.0;               // Benz's kept drhodt
+    if (p.xsph_regularization || p.artificial_visc) b += 4 * 8.0;   // regularisation terms
     b += 4 * 4.0 + 15 * 8.0 + 5 * 4.0 + 4.0;                  // sort keys, scratch
     b += 16.0 / kMinTileThreads + 48.0;                       // chunks, cell lists (worst case)
     return b;
@@ -1217,6 +1256,7 @@ int32_t simp_gpu_set_state(simp_ctx *c, int32_t ntotal, const double *x, const d
                            const double *A, const double *h, int32_t ntotalb, const double *xb,
                            const double *massb, double dt, double current_time) {
     if (!c) return SIMP_ERR_BADARG;
+    SIMP_RANGE("simp_gpu_set_state");
     if (!c->stream) return simp_fail(c, SIMP_ERR_STATE, "context was not created successfully");
     if (c->max_inst != 1) return simp_fail(c, SIMP_ERR_BADARG, "set_state is for single-basin contexts; use simp_gpu_batch_add");
     if (ntotal > c->maxn)
@@ -1358,6 +1398,7 @@ int32_t simp_gpu_get_state(simp_ctx *c, double *x, double *vx, double *mass, dou
                            double *hsml, double *A, double *h, double *dt, double *current_time) {
     if (!c) return SIMP_ERR_BADARG;
     if (!c->have_state || !c->insts[0].active) return simp_fail(c, SIMP_ERR_STATE, "get_state before set_state");
+    SIMP_RANGE("simp_gpu_get_state");
     TRY(get_instance_state(c, 0, x, vx, mass, rho, hsml, A, h, nullptr, true));
     if (dt) *dt = c->sc_host->dt;
     if (current_time) *current_time = c->sc_host->t;
@@ -1404,7 +1445,11 @@ int32_t simp_gpu_nnps(simp_ctx *c, int32_t *nip, int32_t *p_i, int32_t *p_j, dou
                       double *br_ij, int32_t bcap) {
     if (!c) return SIMP_ERR_BADARG;
     if (!c->have_state || c->max_inst != 1) return simp_fail(c, SIMP_ERR_STATE, "nnps needs a single basin with state");
-    return export_pairs(c, nip, p_i, p_j, r_ij, hsml_ij, cap, bnip, bp_i, bp_j, br_ij, bcap);
+    SIMP_RANGE("simp_gpu_nnps");
+    TRY(export_pairs(c, nip, p_i, p_j, r_ij, hsml_ij, cap, bnip, bp_i, bp_j, br_ij, bcap));
+    if (const unsigned f = take_bounds_flags())
+        return simp_fail(c, SIMP_ERR_BOUNDS, "device index check failed (sites " + std::to_string(f) + ")");
+    return SIMP_OK;
 }
 
 int32_t simp_gpu_interaction_stats(simp_ctx *c, int32_t *maxip, int32_t *minip, int64_t *sumip,
@@ -1423,17 +1468,21 @@ int32_t simp_gpu_single_step(simp_ctx *c, double current_time, double *dxdt, dou
                              double *dhdt, double *dAdt) {
     if (!c) return SIMP_ERR_BADARG;
     if (!c->have_state || c->max_inst != 1) return simp_fail(c, SIMP_ERR_STATE, "single_step needs a single basin with state");
+    SIMP_RANGE("simp_gpu_single_step");
     TRY(check_normals(c));
     cudaStream_t s = c->stream;
     k_set_time0<<<1, 1, 0, s>>>(c->sc, c->inst_dev, current_time);
     c->launches += 1;
     launch_reset_stats(c);
     launch_kinematic(c, c->s0, true);
+    launch_regularize(c, c->s0);
     launch_stress(c, c->s0, c->s0, EPI_RATES);
     SIMP_CUDA(c, cudaGetLastError());
     c->lists_valid = true;
     const size_t M = (size_t)c->maxn;
-    if (dxdt) TRY(download2(c, c->s0.vx, c->s0.vy, dxdt));
+    // dx/dt: the velocities, or with XSPH what the rates epilogue wrote
+    if (dxdt && c->reg && c->prm.xsph_regularization) TRY(download2(c, c->reg + 2 * M, c->reg + 3 * M, dxdt));
+    else if (dxdt) TRY(download2(c, c->s0.vx, c->s0.vy, dxdt));
     if (dvxdt) TRY(download2(c, c->rates, c->rates + M, dvxdt));
     if (dhdt) TRY(download1(c, c->rates + 2 * M, dhdt));
     if (dAdt) TRY(download1(c, c->rates + 3 * M, dAdt));
@@ -1444,10 +1493,13 @@ int32_t simp_gpu_single_step(simp_ctx *c, double current_time, double *dxdt, dou
 int32_t simp_gpu_sum_density(simp_ctx *c, double *rho_out) {
     if (!c || !rho_out) return SIMP_ERR_BADARG;
     if (!c->have_state || c->max_inst != 1) return simp_fail(c, SIMP_ERR_STATE, "sum_density needs a single basin with state");
+    SIMP_RANGE("simp_gpu_sum_density");
     double *stage = c->tmp;
     TRY(sum_density(c, stage));
     SIMP_CUDA(c, cudaMemcpyAsync(rho_out, stage, sizeof(double) * c->n, cudaMemcpyDeviceToHost, c->stream));
     SIMP_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (const unsigned f = take_bounds_flags())
+        return simp_fail(c, SIMP_ERR_BOUNDS, "device index check failed (sites " + std::to_string(f) + ")");
     return SIMP_OK;
 }
 
@@ -1456,6 +1508,7 @@ int32_t simp_gpu_sum_density(simp_ctx *c, double *rho_out) {
 // between the device-side stencil radius keeps the cell list exact.
 int32_t simp_gpu_step(simp_ctx *c, int32_t nsteps, double *current_time, double *dt) {
     if (!c || nsteps < 0) return SIMP_ERR_BADARG;
+    SIMP_RANGE("simp_gpu_step");
     TRY(simp::step_enqueue(c, nsteps));
     return simp::step_complete(c, current_time, dt);
 }
@@ -1500,10 +1553,12 @@ static int time_rhs(simp_ctx *c, int reps, double *ms) {
     SIMP_CUDA(c, cudaEventCreate(&e0));
     SIMP_CUDA(c, cudaEventCreate(&e1));
     launch_kinematic(c, c->s0, false);          // warm-up
+    launch_regularize(c, c->s0);
     launch_stress(c, c->s0, c->s0, EPI_RATES);
     cudaEventRecord(e0, c->stream);
     for (int r = 0; r < reps; ++r) {
         launch_kinematic(c, c->s0, false);
+        launch_regularize(c, c->s0);
         launch_stress(c, c->s0, c->s0, EPI_RATES);
     }
     cudaEventRecord(e1, c->stream);

@@ -166,7 +166,9 @@ __global__ void k_scatter(int n, const int *__restrict__ key, const int *__restr
     if (i >= n) return;
     const int k = key[i];
     const int slot = atomicSub(&cnt[k], 1) - 1;
-    perm[start[k] + slot] = i;
+    const int pos = start[k] + slot;
+    if (!SIMP_IN_RANGE(pos, 0, n, SITE_SORT)) return;
+    perm[pos] = i;
 }
 
 // Sort each cell's entries by original particle index (insertion sort; a
@@ -324,6 +326,7 @@ void launch_scan_i32(const int *in, int *out, int n, void *tmp, cudaStream_t s) 
 // Verlet lists follow the particles unless `new_lists` (or no list was built
 // yet), in which case the next kinematic pass rebuilds them all.
 int rebuild(simp_ctx *c, const DueMask &due, int from, bool new_lists) {
+    SIMP_RANGE("re-sort");
     const int n = c->n;
     cudaStream_t s = c->stream;
     const int B = 256;

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/simp_gpu.h"
+#include "check.cuh"
 
 namespace simp {
 
@@ -53,6 +54,7 @@ struct NbrList {
     int *count;
     double *xl, *yl;
     int stride;
+    int n = 0;   // particles in the context (the debug build's index checks)
 };
 
 // The kernel gradients of a right-hand side's pairs, kept by the kinematic
@@ -68,6 +70,7 @@ struct PairList {
     int *pj;
     int *count;
     int stride;
+    int n = 0;   // particles in the context (the debug build's index checks)
 };
 
 // Uniform cell grid of one basin.  cell = clamp(floor((x - x0) * inv_cs));
@@ -167,6 +170,12 @@ struct Phys {
     double zeta_max, eta_max, mu;   // Mohr-Coulomb caps and tan(phi)
     int bfa, boundary_friction;     // boundary force algorithm and its friction branch
     double kappa_t, xi, Y, nu;      // friction parameters; Young modulus and Poisson ratio
+    // regularisation (regularization.f90): XSPH, the artificial viscosity
+    // (0 none, 1 Hernquist-Katz, 2 Monaghan; applied whenever either switch
+    // is on, as the reference's regularization does), its coefficients
+    int xsph, art_visc, artificial_visc;
+    int csound;                     // 1: c_yang is refreshed (sound_speed.f90:21-27), 0: c stays 0
+    double alpha_pi, beta_pi, chi;
 };
 
 // Interaction-count bookkeeping for nnps.f90:613-670.
@@ -471,18 +480,30 @@ __device__ __forceinline__ double boundary_fdwdq(const Phys &P, double br, doubl
 __device__ __forceinline__ double sound_speed(const Phys &P, double rho) {
     return sqrt(P.Y * (1.0 - P.nu) / (rho * (1.0 + P.nu) * (1.0 - 2.0 * P.nu)));
 }
+// The value the reference's c(:) holds: c_yang when sound_speed refreshes it
+// (artificial viscosity, Monaghan time step or boundary friction), else the
+// zero it was never moved from.
+__device__ __forceinline__ double sound_speed_held(const Phys &P, double rho) {
+    return P.csound ? sound_speed(P, rho) : 0.0;
+}
 
 // Time-step candidate of one particle (time_step.f90:132-157 VP_time_step;
-// :40-103 Monaghan_time_step without artificial viscosity, whose
-// dt = min(0.25 sqrt(min hsml / |a|), min hsml / c) is the min over the
-// particles of min(0.25 sqrt(hsml / |a|), hsml / c), sqrt being monotone).
+// :40-124 Monaghan_time_step, whose dt = min(0.25 sqrt(min hsml / |a|),
+// min CFL) is the min over the particles of min(0.25 sqrt(hsml / |a|), CFL),
+// sqrt being monotone).  CFL: hsml / c, or with artificial viscosity
+// 0.3 hsml / (c + hsml |div| + 1.2 (alpha_pi c + beta_pi hsml |div|))
+// (:111-115; 0.3 and 1.2 are default-real literals).
 // hs: the new hsml, a2: |dv/dt|^2 of the last right-hand side, rho: the new
-// density (c_yang is refreshed from it before time_step).
-__device__ __forceinline__ double dt_candidate(const Phys &P, double hs, double a2, double rho) {
+// density (c_yang is refreshed from it before time_step), adiv: |div v|
+// with the new velocities (artificial viscosity only).
+__device__ __forceinline__ double dt_candidate(const Phys &P, double hs, double a2, double rho, double adiv) {
     if (P.tse == 2) return P.rho_ice * (hs * hs) * P.delta_min / (P.P_star * (1.0 + P.k_t));
     const double acc = sqrt(a2);
     const double f = 0.25 * sqrt(hs / acc);
-    const double cfl = hs / sound_speed(P, rho);
+    const double c = sound_speed(P, rho);
+    const double cfl = P.artificial_visc
+        ? (double)0.3f * hs / (c + hs * adiv + (double)1.2f * (P.alpha_pi * c + P.beta_pi * hs * adiv))
+        : hs / c;
     return f < cfl ? f : cfl;
 }
 

@@ -81,6 +81,10 @@ struct simp_ctx {
     double *diag = nullptr;        // 9 * maxn
     // rates of the last single_step (cell order): ax, ay, dhdt, dAdt
     double *rates = nullptr;       // 4 * maxn
+    // regularisation terms of the current right-hand side (4 * maxn, only
+    // with XSPH or artificial viscosity): viscous acceleration x, y and the
+    // XSPH sum x, y (dx/dt after single_step)
+    double *reg = nullptr;
     // wall particles, sorted by cell key
     double *bx = nullptr, *by = nullptr, *bm = nullptr;
     double *bnx = nullptr, *bny = nullptr;   // wall normals (bfa = 2 only)
@@ -165,6 +169,9 @@ void launch_stress(simp_ctx *c, const State &nb, const State &own, EpiMode mode)
 // the step's final hsml, its bounds and the VP dt
 void launch_density_rate(simp_ctx *c, const State &g, const State &v, int rho_upd, bool tail);
 void launch_step_finish(simp_ctx *c);
+// XSPH and artificial viscosity of the right-hand side at s, over the pairs
+// the kinematic pass just found (a no-op when both are off)
+void launch_regularize(simp_ctx *c, const State &s);
 void launch_copy_s1_to_s0(simp_ctx *c);
 void launch_reset_stats(simp_ctx *c);
 

@@ -39,6 +39,7 @@ __device__ __forceinline__ bool bin_rule_ok(const BinRule &b, double xj, double 
 template <class F>
 __device__ __forceinline__ void for_stencil_rows(const Grid &g, int ci, int R, F &&f) {
     const int local = ci - g.base;
+    if (!SIMP_IN_RANGE(local, 0, (long long)g.ncx * g.ncy, SITE_CELL)) return;
     const int cx = local % g.ncx, cy = local / g.ncx;
     const int r0 = max(cy - R, 0), r1 = min(cy + R, g.ncy - 1);
     const int c0 = max(cx - R, 0), c1 = min(cx + R, g.ncx - 1);

@@ -186,6 +186,7 @@ __device__ __forceinline__ void for_each_current_pair(const State &s, const NbrL
     if (cnt >= 0 && cnt <= kMaxNbr && valid) {
         for (int k = 0; k < cnt; ++k) {
             const int j = __ldg(&nl.nbr[(size_t)k * nl.stride + i]);
+            if (!SIMP_IN_RANGE(j, 0, nl.n, SITE_NEIGHBOUR)) continue;
             if (is_pair(s, p, j)) on_pair(j);
         }
     } else {
@@ -215,8 +216,10 @@ __device__ __forceinline__ void for_each_current_pair_batched(const State &s, co
             int jj[kBatch];
             float4 ff[kBatch];
 #pragma unroll
-            for (int u = 0; u < kBatch; ++u)
+            for (int u = 0; u < kBatch; ++u) {
                 jj[u] = (k0 + u < cnt) ? __ldg(&nl.nbr[(size_t)(k0 + u) * nl.stride + i]) : -1;
+                if (jj[u] >= 0 && !SIMP_IN_RANGE(jj[u], 0, nl.n, SITE_NEIGHBOUR)) jj[u] = -1;
+            }
 #pragma unroll
             for (int u = 0; u < kBatch; ++u)
                 ff[u] = (jj[u] >= 0 && p.use_f32) ? __ldg(&s.pf[jj[u]]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -455,6 +458,10 @@ struct StressArgs {
     NbrList nl;
     PairList pl;
     double *rates;
+    // regularisation terms of this right-hand side (k_regularize), 4 maxn:
+    // the artificial-viscosity acceleration (x, y) and the XSPH sum (x, y),
+    // which a rates epilogue replaces by dx/dt; null when both are off
+    double *reg;
     const double *xr, *yr;
     double *hs_next;
     int n, maxn, mode;
@@ -665,6 +672,21 @@ __device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool l
         ax += k * ru * fabs(ru);
         ay += k * rv * fabs(rv);
     }
+    // regularisation, single_step.f90:99-101 (after the drag): the
+    // artificial viscosity into dv/dt, the XSPH sum into dx/dt
+    // (regularization.f90:93, then single_step.f90:106: dxdt = -chi xsph + v)
+    double dxdt = vxi, dydt = vyi;
+    if (a.reg) {
+        const size_t M = (size_t)a.maxn;
+        if (P.art_visc == 1 || P.art_visc == 2) {
+            ax += a.reg[i];
+            ay += a.reg[M + i];
+        }
+        if (P.xsph) {
+            dxdt = -(P.chi * a.reg[2 * M + i]) + vxi;
+            dydt = -(P.chi * a.reg[3 * M + i]) + vyi;
+        }
+    }
     // prognostic rates, single_step.f90:104-106
     const double dv = a.div[i];
     const double dhdt = -hh * dv / rho;
@@ -677,6 +699,10 @@ __device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool l
             a.rates[M + i] = ay;
             a.rates[2 * M + i] = dhdt;
             a.rates[3 * M + i] = dAdt;
+            if (a.reg && P.xsph) {   // dx/dt in place of the XSPH sum
+                a.reg[2 * M + i] = dxdt;
+                a.reg[3 * M + i] = dydt;
+            }
         }
         return;
     }
@@ -686,32 +712,32 @@ __device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool l
     double xn, yn, vxn, vyn, hn, An;
     if (a.mode == EPI_PREDICT) {
         // time_integration.f90:207-215 (and the leap-frog's first half, :333-341)
-        xn = x0 + vxi * dt / 2.0;
-        yn = y0 + vyi * dt / 2.0;
+        xn = x0 + dxdt * dt / 2.0;
+        yn = y0 + dydt * dt / 2.0;
         vxn = vx0 + ax * dt / 2.0;
         vyn = vy0 + ay * dt / 2.0;
         hn = h0 + dhdt * dt / 2.0;
         An = A0 + dAdt * dt / 2.0;
     } else if (a.mode == EPI_EULER) {
         // euler_scheme, time_integration.f90:117-125
-        xn = x0 + vxi * dt;
-        yn = y0 + vyi * dt;
+        xn = x0 + dxdt * dt;
+        yn = y0 + dydt * dt;
         vxn = vx0 + ax * dt;
         vyn = vy0 + ay * dt;
         hn = h0 + dhdt * dt;
         An = A0 + dAdt * dt;
     } else if (a.mode == EPI_LEAP) {
         // leapfrog_scheme, time_integration.f90:361-369 (vx0: the step-start
-        // velocity, vxi: the half-step one)
+        // velocity, dxdt: the half-step right-hand side's dx/dt)
         vxn = vx0 + ax * dt;
         vyn = vy0 + ay * dt;
         hn = h0 + dhdt * dt;
-        xn = x0 + (vx0 + vxi) * dt / 2.0;
-        yn = y0 + (vy0 + vyi) * dt / 2.0;
+        xn = x0 + (vx0 + dxdt) * dt / 2.0;
+        yn = y0 + (vy0 + dydt) * dt / 2.0;
         An = A0 + dAdt * dt;
     } else {
         // time_integration.f90:236-259
-        const double x12 = x0 + vxi * dt / 2.0, y12 = y0 + vyi * dt / 2.0;
+        const double x12 = x0 + dxdt * dt / 2.0, y12 = y0 + dydt * dt / 2.0;
         const double vx12 = vx0 + ax * dt / 2.0, vy12 = vy0 + ay * dt / 2.0;
         const double h12 = h0 + dhdt * dt / 2.0, A12 = A0 + dAdt * dt / 2.0;
         xn = 2.0 * x12 - x0;
@@ -725,11 +751,13 @@ __device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool l
     // the step's last update: hsml, VP time step (after the corrector, the
     // Euler step or the leap-frog's second half).  `tail_later`: a
     // density-rate pass (k_density_rate) follows and does them, because the
-    // final density (con_density) or Benz's hsml needs the updated
-    // velocities of the neighbours.
+    // final density (con_density), Benz's hsml or the Monaghan time step
+    // with artificial viscosity needs the updated velocities of the
+    // neighbours.
     const bool final_update = a.mode == EPI_CORRECT || a.mode == EPI_EULER || a.mode == EPI_LEAP;
     const bool den2 = P.den_alg == 2;
-    const bool tail_later = final_update && ((den2 && a.mode != EPI_CORRECT) || P.sle == 1);
+    const bool tail_later = final_update && ((den2 && a.mode != EPI_CORRECT) || P.sle == 1 ||
+                                             (P.tse == 1 && P.artificial_visc));
     double rhon;
     if (!den2) {
         rhon = hn * P.rho_ice;                                // density.f90:192
@@ -810,7 +838,7 @@ __device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool l
     }
     if (corr && P.tse != 0) {                                   // time_step.f90:20-26
         active |= 32u;
-        if (live) v[5] = dbits(dt_candidate(P, hsn, ax * ax + ay * ay, rhon));
+        if (live) v[5] = dbits(dt_candidate(P, hsn, ax * ax + ay * ay, rhon, 0.0));
     }
     if (tail_later && P.tse == 1 && live) a.rates[i] = ax * ax + ay * ay;   // for k_density_rate
     block_bounds(a.sc, active, v);

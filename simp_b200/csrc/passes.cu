@@ -84,6 +84,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<T>::kin) k_kinematic(KinArgs
 #pragma unroll 4
         for (int k = 0; k < cnt; ++k) {
             const int j = s_list[k * kBlock + t];
+            if (!SIMP_IN_RANGE(j, 0, a.n, SITE_NEIGHBOUR)) continue;
             if (done + k < kMaxPairs) a.pl.pj[(size_t)(done + k) * a.pl.stride + i] = j;
             const double2 q = __ldg(&s.xy[j]), v = __ldg(&s.vxy[j]);
             const KinNb<T> nb = Nb<T>::kin(s, j);
@@ -209,6 +210,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<T>::kin) k_kin_sums(KinArgs 
     const T hiT = Nb<T>::h(s, i), inv_hiT = (T)inv_hi;
     typename Vec2<T>::type *dwr = reinterpret_cast<typename Vec2<T>::type *>(a.dw);
     auto pair = [&](int k, int j) {
+        if (!SIMP_IN_RANGE(j, 0, a.n, SITE_NEIGHBOUR)) return;
         const double2 q = __ldg(&s.xy[j]), v = __ldg(&s.vxy[j]);
         const KinNb<T> nb = Nb<T>::kin(s, j);
         const PairGeom<T> pg = pair_geom<T, false, SKF>(P, (T)(xi - q.x), (T)(yi - q.y), hiT, inv_hiT, nb.h);
@@ -245,6 +247,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<T>::stress) k_stress(StressA
     StressSums<T> ss;
     const T hiT = Nb<T>::h(s, i), inv_hiT = (T)inv_hi;
     auto accumulate = [&](int j) {
+        if (!SIMP_IN_RANGE(j, 0, a.n, SITE_NEIGHBOUR)) return;
         const double2 q = __ldg(&s.xy[j]);
         const StressNb<T> nb = Nb<T>::stress(s, a.rec, j);
         const PairGeom<T> pg = pair_geom<T, false, SKF>(P, (T)(xi - q.x), (T)(yi - q.y), hiT, inv_hiT, nb.h);
@@ -258,7 +261,9 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<T>::stress) k_stress(StressA
         for (int k = 0; k < cnt; ++k) {
             const size_t r = (size_t)k * a.pl.stride + i;
             const typename Vec2<T>::type g = __ldg(&dwr[r]);
-            const StressNb<T> nb = Nb<T>::stress_rec(a.rec, __ldg(&a.pl.pj[r]));
+            const int j = __ldg(&a.pl.pj[r]);
+            if (!SIMP_IN_RANGE(j, 0, a.n, SITE_NEIGHBOUR)) continue;
+            const StressNb<T> nb = Nb<T>::stress_rec(a.rec, j);
             ss.add(g.x, g.y, nb.m, nb.t11, nb.t12, nb.t22);
         }
     } else if (cnt <= kMaxPairs) {
@@ -277,6 +282,104 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<T>::stress) k_stress(StressA
     }
     stress_finish<SKF>(a, i, live, ki, I, dead, xi, yi, hi, ci, ss.sx.get(), ss.sy.get(), ss.tx.get(), ss.ty.get(),
                        cnt, true);
+}
+
+// Regularisation of a right-hand side (regularization.f90, called by
+// single_step.f90:99-101), per particle i over the pairs the kinematic pass
+// just found, in FP64 in both precision forms:
+//   XSPH (:45-95)  xs_i = sum_j m_j (v_i - v_j) W_ij / ((rho_i + rho_j) / 2)
+//   artificial viscosity, av_i = -sum_j m_j pi_ij grad_i W_ij with
+//     Hernquist-Katz (:102-213): pi_ij = lv_i / rho_i^2 + lv_j / rho_j^2,
+//       lv = (alpha_pi hsml c |d| + beta_pi (|d| hsml)^2) rho, d the
+//       velocity divergence (the kinematic pass's sum over rho) where it is
+//       negative, else 0;
+//     Monaghan (:220-308): pi_ij = (beta_pi iota^2 - alpha_pi iota
+//       (c_i + c_j) / 2) / ((rho_i + rho_j) / 2), iota = hsml_ij v_r /
+//       (r_ij^2 + (0.01 hsml_ij)^2), v_r = (v_i - v_j) . (x_i - x_j);
+//     for pairs with (v_i - v_j) . (x_i - x_j) <= 0, else pi_ij = 0.
+// The reference runs both loops serially over its pair list, where pi_ij
+// keeps the previous pair's value for a pair outside the criterion and XSPH
+// adds the same-signed term to both particles; the gather here evaluates
+// every pair on its own (zero outside the criterion, XSPH antisymmetric).
+struct RegArgs {
+    State s;
+    const double *div;   // the kinematic pass's -sum_j m_j (v_i - v_j) . grad W
+    PairList pl;
+    NbrList nl;
+    const int *cell_start, *cell, *pinst;
+    const Inst *inst;
+    Scalars *sc;
+    Phys P;
+    double *reg;
+    int n, maxn;
+};
+
+// lv / rho^2 of the Hernquist-Katz viscosity of particle k
+__device__ __forceinline__ double hk_lv_r2(const Phys &P, const State &s, const double *div, int k) {
+    const double rho = s.rho[k], hs = s.hs[k];
+    double d = div[k] / rho;
+    if (d >= 0.0) d = 0.0;
+    const double c = sound_speed_held(P, rho);
+    const double ad = fabs(d);
+    const double lv = (P.alpha_pi * hs * c * ad + P.beta_pi * ((ad * hs) * (ad * hs))) * rho;
+    return lv / (rho * rho);
+}
+
+__global__ void __launch_bounds__(kBlock) k_regularize(RegArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const State &s = a.s;
+    const Phys &P = a.P;
+    const size_t M = (size_t)a.maxn;
+    const Inst &I = a.inst[a.pinst[i]];
+    const double2 xy = s.xy[i], v = s.vxy[i];
+    const double xi = xy.x, yi = xy.y, vxi = v.x, vyi = v.y;
+    const double hi = s.hs[i], inv_hi = 1.0 / hi, rhoi = s.rho[i];
+    const double ci = sound_speed_held(P, rhoi);
+    const double pii = (P.art_visc == 1) ? hk_lv_r2(P, s, a.div, i) : 0.0;
+    Sum<double> avx, avy, xsx, xsy;
+    auto pair = [&](int j) {
+        if (!SIMP_IN_RANGE(j, 0, a.n, SITE_NEIGHBOUR)) return;
+        const double2 q = s.xy[j], w = s.vxy[j];
+        const double dx = xi - q.x, dy = yi - q.y;
+        const double dvx = vxi - w.x, dvy = vyi - w.y;
+        const double hj = s.hs[j], rhoj = s.rho[j], mj = s.m[j];
+        const PairGeom<double> pg = pair_geom<double, true>(P, dx, dy, hi, inv_hi, hj);
+        if (P.xsph) {
+            const double rbar = 0.5 * (rhoi + rhoj);
+            xsx.madd(mj * dvx * pg.w / rbar, 1.0);
+            xsy.madd(mj * dvy * pg.w / rbar, 1.0);
+        }
+        const double vr = dvx * dx + dvy * dy;
+        if ((P.art_visc == 1 || P.art_visc == 2) && vr <= 0.0) {
+            double pij;
+            if (P.art_visc == 1) {
+                pij = pii + hk_lv_r2(P, s, a.div, j);
+            } else {
+                const double hij = __dmul_rn(__dadd_rn(hi, hj), 0.5);
+                const double r = ref_distance(dx, dy);
+                const double scor = (double)0.01f * hij;
+                const double iota = hij * vr / (r * r + scor * scor);
+                const double cj = sound_speed_held(P, rhoj);
+                pij = (P.beta_pi * (iota * iota) - P.alpha_pi * iota * (ci + cj) / 2.0) / ((rhoi + rhoj) / 2.0);
+            }
+            avx.madd(-(mj * pij), pg.gfac * pg.dx);
+            avy.madd(-(mj * pij), pg.gfac * pg.dy);
+        }
+    };
+    const bool dead = (I.flags & FLAG_NONFINITE) != 0;
+    const int cnt = a.pl.count[i];
+    if (dead) {
+    } else if (cnt <= kMaxPairs) {
+        for (int k = 0; k < cnt; ++k) pair(a.pl.pj[(size_t)k * a.pl.stride + i]);
+    } else {
+        const PairCtx pc = pair_ctx(s, a.sc, I, a.cell_start, i);
+        for_each_current_pair(s, a.nl, a.sc, i, a.cell[i], pc, pair);
+    }
+    a.reg[i] = avx.get();
+    a.reg[M + i] = avy.get();
+    a.reg[2 * M + i] = xsx.get();
+    a.reg[3 * M + i] = xsy.get();
 }
 
 // Density rate drho/dt_i = sum_j m_j (v_i - v_j) . grad_i W_ij over the
@@ -306,6 +409,7 @@ struct DensArgs {
     Scalars *sc;
     Phys P;
     int n, rho_upd, tail;
+    int dt_div;          // the Monaghan time step's divergence (artificial viscosity)
 };
 
 __global__ void __launch_bounds__(kBlock) k_density_rate(DensArgs a) {
@@ -319,13 +423,17 @@ __global__ void __launch_bounds__(kBlock) k_density_rate(DensArgs a) {
     const double xi = g.x[i], yi = g.y[i], hi = g.hs[i];
     const double inv_hi = 1.0 / hi;
     const double vxi = a.v.vx[i], vyi = a.v.vy[i];
-    Sum<double> r;
+    Sum<double> r, rt;
     auto add = [&](int j) {
+        if (!SIMP_IN_RANGE(j, 0, a.n, SITE_NEIGHBOUR)) return;
         const double2 q = g.xy[j];
         const PairGeom<double> pg = pair_geom<double, false>(P, xi - q.x, yi - q.y, hi, inv_hi, g.hs[j]);
         const double2 v = a.v.vxy[j];
         const double dvx = vxi - v.x, dvy = vyi - v.y;
-        r.madd(a.mj[j], fma(dvx, pg.gfac * pg.dx, dvy * (pg.gfac * pg.dy)));
+        const double t = fma(dvx, pg.gfac * pg.dx, dvy * (pg.gfac * pg.dy));
+        r.madd(a.mj[j], t);
+        // time_step.f90:93-109: the current masses (after mass_evolution)
+        if (a.dt_div) rt.madd(a.v.m[j], t);
     };
     const int cnt = a.pl.count[i];
     if (dead) {
@@ -383,7 +491,9 @@ __global__ void __launch_bounds__(kBlock) k_density_rate(DensArgs a) {
     }
     if (P.tse != 0) {                                          // time_step.f90:20-26
         active |= 32u;
-        if (live) v[5] = dbits(dt_candidate(P, hsn, P.tse == 1 ? a.a2[i] : 0.0, rhon));
+        // |div v| = |sum_j m_j (v_i - v_j) . grad W| / rho_i (time_step.f90:108-111)
+        const double adiv = a.dt_div ? fabs(rt.get() / rhon) : 0.0;
+        if (live) v[5] = dbits(dt_candidate(P, hsn, P.tse == 1 ? a.a2[i] : 0.0, rhon, adiv));
     }
     block_bounds(a.sc, active, v);
 }
@@ -469,6 +579,7 @@ NbrList nbr_list(simp_ctx *c) {
     nl.xl = c->xl;
     nl.yl = c->yl;
     nl.stride = c->maxn;
+    nl.n = c->n;
     return nl;
 }
 
@@ -485,12 +596,14 @@ PairList pair_list(simp_ctx *c) {
     pl.pj = c->pair_j;
     pl.count = c->pair_count;
     pl.stride = c->maxn;
+    pl.n = c->n;
     return pl;
 }
 
 }  // namespace
 
 void launch_kinematic(simp_ctx *c, const State &s, bool diag) {
+    SIMP_RANGE("kinematic pass");
     KinArgs a{};
     a.s = s;
     a.cell_start = c->cell_start;
@@ -553,6 +666,7 @@ void launch_kinematic(simp_ctx *c, const State &s, bool diag) {
 }
 
 void launch_stress(simp_ctx *c, const State &rhs, const State &base, EpiMode mode) {
+    SIMP_RANGE("stress pass");
     StressArgs a{};
     a.rhs = rhs;
     a.base = base;
@@ -579,6 +693,7 @@ void launch_stress(simp_ctx *c, const State &rhs, const State &base, EpiMode mod
     a.nl = nbr_list(c);
     a.pl = pair_list(c);
     a.rates = c->rates;
+    a.reg = c->reg;
     a.xr = c->xr;
     a.yr = c->yr;
     a.hs_next = c->tmp;   // hsml of the next step (committed by launch_step_finish)
@@ -607,7 +722,29 @@ void launch_stress(simp_ctx *c, const State &rhs, const State &base, EpiMode mod
     c->launches += 1;
 }
 
+void launch_regularize(simp_ctx *c, const State &s) {
+    if (!c->reg) return;
+    SIMP_RANGE("regularisation pass");
+    RegArgs a{};
+    a.s = s;
+    a.div = c->div;
+    a.pl = pair_list(c);
+    a.nl = nbr_list(c);
+    a.cell_start = c->cell_start;
+    a.cell = c->cell;
+    a.pinst = c->pinst;
+    a.inst = c->inst_dev;
+    a.sc = c->sc;
+    a.P = c->phys;
+    a.reg = c->reg;
+    a.n = c->n;
+    a.maxn = c->maxn;
+    k_regularize<<<nblk(c->n, kBlock), kBlock, 0, c->stream>>>(a);
+    c->launches += 1;
+}
+
 void launch_density_rate(simp_ctx *c, const State &g, const State &v, int rho_upd, bool tail) {
+    SIMP_RANGE("density-rate pass");
     DensArgs a{};
     a.g = g;
     a.v = v;
@@ -626,6 +763,7 @@ void launch_density_rate(simp_ctx *c, const State &g, const State &v, int rho_up
     a.n = c->n;
     a.rho_upd = rho_upd;
     a.tail = tail ? 1 : 0;
+    a.dt_div = (tail && c->prm.tse == 1 && c->prm.artificial_visc) ? 1 : 0;
     k_density_rate<<<nblk(c->n, kBlock), kBlock, 0, c->stream>>>(a);
     c->launches += 1;
 }

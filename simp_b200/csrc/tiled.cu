@@ -249,6 +249,7 @@ __global__ void __launch_bounds__(kMaxTileThreads) k_kin_tiled(KinArgs a) {
                 const unsigned short e = tl.list[k * blockDim.x + t];
                 const int sl = e & 0x7fff;
                 if (sl == own) continue;
+                if (!SIMP_IN_RANGE(sl, 0, a.cap, SITE_TILE)) continue;
                 const double xj = tl.x[sl], yj = tl.y[sl], hj = tl.hs[sl];
                 if (e & kExact) {
                     double r;

@@ -27,6 +27,7 @@ SIMP_ERR_NONFINITE = 6
 SIMP_ERR_TIMEOUT = 7
 SIMP_ERR_NOMEM = 8
 SIMP_ERR_STATE = 9
+SIMP_ERR_BOUNDS = 10
 
 DIAG_NAMES = ("eps11", "eps12", "eps22", "zeta", "eta", "p", "sig11", "sig12", "sig22")
 
@@ -48,8 +49,9 @@ def _f64(a, shape=None):
 class Simp:
     """One resident basin: ntotal particles, ntotalb wall particles."""
 
-    def __init__(self, params: SimpParams, maxn: int, maxnb: int):
-        self.lib = _lib.load()
+    def __init__(self, params: SimpParams, maxn: int, maxnb: int, lib=None):
+        # lib: another build of the library (the checked debug build), else the default one
+        self.lib = lib if lib is not None else _lib.load()
         self.params = params.copy()
         h = ctypes.c_void_p()
         rc = self.lib.simp_gpu_create(ctypes.byref(self.params), int(maxn), int(maxnb), ctypes.byref(h))
@@ -85,9 +87,9 @@ class Simp:
             raise SimpError(rc, self.lib.simp_gpu_last_error(self.h).decode())
 
     @classmethod
-    def from_basin(cls, b, params: SimpParams | None = None, maxn: int | None = None):
+    def from_basin(cls, b, params: SimpParams | None = None, maxn: int | None = None, lib=None):
         prm = b.params if params is None else params
-        s = cls(prm, maxn or b.n, max(b.nb, 1))
+        s = cls(prm, maxn or b.n, max(b.nb, 1), lib=lib)
         s.set_state(b.x, b.vx, b.mass, b.rho, b.hsml, b.A, b.h, b.xb, b.massb, prm.dt, 0.0)
         if prm.bfa == 2 and b.nb > 0 and getattr(b, "bn", None) is not None:
             s.set_wall_normals(b.bn)
