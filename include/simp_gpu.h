@@ -50,8 +50,9 @@ enum {
     SIMP_ERR_TIMEOUT = 7,   /* a bounded device-side wait gave up              */
     SIMP_ERR_NOMEM = 8,     /* device allocation failed                        */
     SIMP_ERR_STATE = 9,     /* entry point called before simp_gpu_set_state    */
-    SIMP_ERR_BOUNDS = 10    /* a device index check failed (only the checked
+    SIMP_ERR_BOUNDS = 10,   /* a device index check failed (only the checked
                                debug build, libsimp_gpu_checked.so, checks)  */
+    SIMP_ERR_CANCELLED = 11 /* a served request was cancelled (simp_serve.h)  */
 };
 
 /* Smoothing kernel selector: the reference's skf codes (globals.f90:136-147,

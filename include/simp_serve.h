@@ -46,6 +46,7 @@ typedef struct simp_request_stats {
 
 typedef struct simp_server_stats {
     int64_t submitted, completed, failed;
+    int64_t cancelled;              /* left by simp_server_cancel               */
     int64_t particle_steps;         /* of completed requests                    */
     int64_t batch_steps;            /* steps of the served batch                */
     int64_t peak_resident_particles;
@@ -77,8 +78,19 @@ SIMP_API int32_t simp_server_submit(simp_server *srv, const simp_forcing *forcin
                                     double *x_out, double *vx_out, double *h_out, double *A_out,
                                     int64_t *request_id);
 
-/* Runs the stream until every submitted request has completed or failed. */
+/* Runs the stream until every submitted request has completed, failed or
+ * been cancelled. */
 SIMP_API int32_t simp_server_run(simp_server *srv);
+
+/* Cancels a request at the first scheduling decision at or after at_s
+ * seconds into the run (at_s < 0: the next decision).  A request still
+ * pending is never admitted; a resident one leaves the batch, and its FP64
+ * replica, between two steps, with its *_out arrays left untouched; one
+ * already completed is not affected.  Its status becomes
+ * SIMP_ERR_CANCELLED.  The other requests' results do not change (each is
+ * the same as stepped alone).  Safe to call from another thread while
+ * simp_server_run runs. */
+SIMP_API int32_t simp_server_cancel(simp_server *srv, int64_t request_id, double at_s);
 
 SIMP_API int32_t simp_server_request(const simp_server *srv, int64_t request_id,
                                      simp_request_stats *out);

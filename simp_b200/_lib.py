@@ -66,6 +66,7 @@ SIGNATURES = {
                                   _i32, _dp, _dp, ctypes.c_int64, ctypes.c_double, _dp, _dp, _dp, _dp,
                                   ctypes.POINTER(ctypes.c_int64)]),
     "simp_server_run": (_i32, [_vp]),
+    "simp_server_cancel": (_i32, [_vp, ctypes.c_int64, ctypes.c_double]),
     "simp_server_request": (_i32, [_vp, ctypes.c_int64, ctypes.POINTER(RequestStats)]),
     "simp_server_stats_get": (_i32, [_vp, ctypes.POINTER(ServerStats)]),
     "simp_server_last_error": (ctypes.c_char_p, [_vp]),

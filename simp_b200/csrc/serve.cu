@@ -6,6 +6,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -29,7 +30,7 @@ struct Request {
     int64_t nsteps = 0;
     double arrival = 0.0;
     // progress
-    enum { PENDING, RESIDENT, DONE, FAILED } state = PENDING;
+    enum { PENDING, RESIDENT, DONE, FAILED, CANCELLED } state = PENDING;
     int slot = -1, spot_slot = -1;
     int64_t remaining = 0;
     simp_request_stats st{};
@@ -51,6 +52,10 @@ struct simp_server {
     std::vector<int> resident;      // request ids on the device
     simp_server_stats stats{};
     std::string err;
+    // cancellations asked for (request id, run time), possibly from another
+    // thread while run() steps; applied at the scheduling decisions
+    std::mutex cancel_mu;
+    std::vector<std::pair<int64_t, double>> cancels;
 };
 
 namespace {
@@ -82,6 +87,10 @@ int ctx_error(simp_server *s, simp_ctx *c, int rc) {
 int admit(simp_server *s, double now) {
     while (s->next < s->order.size()) {
         Request &r = s->reqs[s->order[s->next]];
+        if (r.state == Request::CANCELLED) {   // cancelled before it was admitted
+            s->next += 1;
+            continue;
+        }
         if (r.arrival > now) break;
         if ((int)s->resident.size() >= s->cfg.max_instances) break;
         if (s->res_main + r.n > s->maxn_main || s->resb_main + r.nb > s->maxnb_main) {
@@ -159,6 +168,51 @@ int retire(simp_server *s, int id) {
         s->stats.particle_steps += (int64_t)r.n * steps;
     } else {
         s->stats.failed += 1;
+    }
+    return SIMP_OK;
+}
+
+// Cancellations that are due at `now`: a pending request is marked (admit
+// skips it), a resident one leaves both batches between steps.
+int apply_cancels(simp_server *s, double now) {
+    std::vector<int64_t> due;
+    {
+        std::lock_guard<std::mutex> lk(s->cancel_mu);
+        std::vector<std::pair<int64_t, double>> later;
+        for (const auto &c : s->cancels) {
+            if (c.second <= now) due.push_back(c.first);
+            else later.push_back(c);
+        }
+        s->cancels.swap(later);
+    }
+    for (int64_t id : due) {
+        Request &r = s->reqs[(size_t)id];
+        if (r.state == Request::PENDING) {
+            r.state = Request::CANCELLED;
+        } else if (r.state == Request::RESIDENT) {
+            if (r.spot_slot >= 0) {
+                const int rc = simp_gpu_batch_remove(s->spot, r.spot_slot);
+                if (rc != SIMP_OK) return ctx_error(s, s->spot, rc);
+                s->spot_count -= 1;
+                s->res_spot -= r.n;
+                s->resb_spot -= r.nb;
+                r.spot_slot = -1;
+            }
+            int64_t steps = 0;
+            simp_gpu_batch_info(s->main, r.slot, nullptr, &steps, nullptr);
+            const int rc = simp_gpu_batch_remove(s->main, r.slot);
+            if (rc != SIMP_OK) return ctx_error(s, s->main, rc);
+            s->res_main -= r.n;
+            s->resb_main -= r.nb;
+            r.st.steps = steps;
+            r.state = Request::CANCELLED;
+            s->resident.erase(std::find(s->resident.begin(), s->resident.end(), (int)id));
+        } else {
+            continue;   // completed or failed already
+        }
+        r.st.status = SIMP_ERR_CANCELLED;
+        r.st.completed_s = now;
+        s->stats.cancelled += 1;
     }
     return SIMP_OK;
 }
@@ -255,8 +309,10 @@ int32_t simp_server_run(simp_server *s) {
     auto now = [&]() { return std::chrono::duration<double>(clock_t_::now() - t0).count(); };
     for (;;) {
         const double t = now();
+        int rc = apply_cancels(s, t);
+        if (rc != SIMP_OK) return rc;
         const size_t before = s->resident.size();
-        int rc = admit(s, t);
+        rc = admit(s, t);
         if (rc != SIMP_OK) return rc;
         s->stats.admit_s += now() - t;
         for (size_t k = before; k < s->resident.size(); ++k) s->reqs[s->resident[k]].st.admitted_s = now();
@@ -304,6 +360,14 @@ int32_t simp_server_run(simp_server *s) {
         s->resident.swap(keep);
         s->stats.retire_s += now() - tr;
     }
+    return SIMP_OK;
+}
+
+int32_t simp_server_cancel(simp_server *s, int64_t id, double at_s) {
+    if (!s || id < 0) return SIMP_ERR_BADARG;
+    std::lock_guard<std::mutex> lk(s->cancel_mu);
+    if (id >= (int64_t)s->reqs.size()) return fail(s, SIMP_ERR_BADARG, "cancel: unknown request");
+    s->cancels.emplace_back(id, at_s < 0.0 ? -1.0 : at_s);
     return SIMP_OK;
 }
 

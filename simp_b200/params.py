@@ -111,6 +111,7 @@ class RequestStats(ctypes.Structure):
 class ServerStats(ctypes.Structure):
     """``simp_server_stats`` (include/simp_serve.h)."""
     _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
+                ("cancelled", ctypes.c_int64),
                 ("particle_steps", ctypes.c_int64), ("batch_steps", ctypes.c_int64),
                 ("peak_resident_particles", ctypes.c_int64), ("peak_resident_requests", ctypes.c_int32),
                 ("reserved0", ctypes.c_int32), ("makespan_s", ctypes.c_double),

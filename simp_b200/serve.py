@@ -108,6 +108,12 @@ class Server:
     def run(self):
         self._chk(self.lib.simp_server_run(self.h))
 
+    def cancel(self, rid: int, at_s: float = -1.0):
+        """Cancels request rid at the first scheduling decision at or after
+        at_s seconds into the run (at_s < 0: the next one); callable from
+        another thread while run() is in progress."""
+        self._chk(self.lib.simp_server_cancel(self.h, int(rid), float(at_s)))
+
     def request(self, rid: int) -> dict:
         st = RequestStats()
         self._chk(self.lib.simp_server_request(self.h, int(rid), ctypes.byref(st)))

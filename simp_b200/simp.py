@@ -28,6 +28,7 @@ SIMP_ERR_TIMEOUT = 7
 SIMP_ERR_NOMEM = 8
 SIMP_ERR_STATE = 9
 SIMP_ERR_BOUNDS = 10
+SIMP_ERR_CANCELLED = 11
 
 DIAG_NAMES = ("eps11", "eps12", "eps22", "zeta", "eta", "p", "sig11", "sig12", "sig22")
 

@@ -105,3 +105,62 @@ def test_serial_fp64_baseline_runs(gpu_lib):
     assert r["particle_steps"] == sum(q.basin.n * q.nsteps for q in reqs)
     assert r["value"] > 0 and r["p50_s"] <= r["p99_s"]
     assert reqs[0].basin.params.precision == PREC_MIXED
+
+
+def test_cancel_resident_and_pending(gpu_lib):
+    """Host-injected cancellation: a resident request that cannot finish is
+    cancelled mid-run and leaves the batch between steps; a request that has
+    not arrived is cancelled before admission.  Both report
+    SIMP_ERR_CANCELLED with their outputs untouched; every other request
+    completes with the same bits as stepped alone."""
+    from simp_b200.simp import SIMP_ERR_CANCELLED
+    reqs = _stream(count=6, seed=36, steps=(20, 60))
+    reqs[1].nsteps = 10 ** 7          # cannot finish before its cancellation
+    reqs[4].arrival_s = 30.0          # would arrive long after the others are done
+    with serve.Server(reqs[0].basin.params, 2 * GB, max_instances=16, max_request_particles=20000,
+                      quantum_steps=8, spot_every=1) as srv:
+        ids = [srv.submit(r) for r in reqs]
+        srv.cancel(ids[1], at_s=0.05)
+        srv.cancel(ids[4], at_s=0.0)
+        srv.run()
+        st = srv.stats()
+        assert st["cancelled"] == 2 and st["completed"] == 4 and st["failed"] == 0
+        q1, q4 = srv.request(ids[1]), srv.request(ids[4])
+        assert q1["status"] == SIMP_ERR_CANCELLED and 0 < q1["steps"] < reqs[1].nsteps
+        assert q1["admitted_s"] <= 0.05 <= q1["completed_s"]
+        assert q4["status"] == SIMP_ERR_CANCELLED and q4["steps"] == 0 and q4["admitted_s"] < 0
+        for rid in (ids[1], ids[4]):
+            assert all(not np.any(v) for v in srv.outputs[rid].values())
+        assert st["makespan_s"] < 20.0    # the cancelled request was not waited for
+        for k, (rid, r) in enumerate(zip(ids, reqs)):
+            if k in (1, 4):
+                continue
+            q = srv.request(rid)
+            assert q["status"] == 0 and q["steps"] == r.nsteps
+            ref = _alone(r)
+            for f in ("x", "vx", "h", "A"):
+                assert np.array_equal(srv.outputs[rid][f], ref[f]), (rid, f)
+
+
+def test_cancel_from_another_thread(gpu_lib):
+    """simp_server_cancel while simp_server_run steps on the calling thread."""
+    import threading
+    import time
+    from simp_b200.simp import SIMP_ERR_CANCELLED
+    reqs = _stream(count=3, seed=37, steps=(10, 20))
+    reqs[0].nsteps = 10 ** 7
+    with serve.Server(reqs[0].basin.params, 2 * GB, max_instances=8, max_request_particles=20000,
+                      quantum_steps=4) as srv:
+        ids = [srv.submit(r) for r in reqs]
+
+        def later():
+            time.sleep(0.2)
+            srv.cancel(ids[0])
+
+        th = threading.Thread(target=later)
+        th.start()
+        srv.run()
+        th.join()
+        q = srv.request(ids[0])
+        assert q["status"] == SIMP_ERR_CANCELLED and 0 < q["steps"] < reqs[0].nsteps
+        assert srv.stats()["completed"] == 2
