@@ -13,7 +13,10 @@ namespace {
 
 using namespace pass;
 
-constexpr int kBlock = 128;
+#ifndef SIMP_PASS_BLOCK
+#define SIMP_PASS_BLOCK 128
+#endif
+constexpr int kBlock = SIMP_PASS_BLOCK;   // threads per block of the gather passes
 // Up to this many particles in a context the kinematic pass runs as two
 // kernels (k_find_pairs, k_kin_sums), above it as one (k_kinematic), unless
 // the context names one form (SIMP_PASSES_GATHER_ONE / _TWO).  The
