@@ -45,8 +45,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--forms", default="mixed,batched,served",
                     help="comma list of the other forms to measure on rank 0 ('' for none)")
-    ap.add_argument("--served-requests", type=int, default=48)
-    ap.add_argument("--served-steps-scale", type=float, default=0.25)
+    ap.add_argument("--served-requests", type=int, default=64)
+    ap.add_argument("--served-steps-scale", type=float, default=1.0,
+                    help="factor on the requests' step counts U(100, 2000) (1: as the served workload states)")
     return ap.parse_args()
 
 
@@ -335,9 +336,16 @@ def run_forms(args, which):
             res[name] = {"value": b.n * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps}
         g32.set_state(b.x, b.vx, b.mass, b.rho, b.hsml, b.A, b.h, b.xb, b.massb, b.params.dt, 0.0)
         g64.set_state(b.x, b.vx, b.mass, b.rho, b.hsml, b.A, b.h, b.xb, b.massb, b.params.dt, 0.0)
-        g32.time_integration(50)
-        g64.time_integration(50)
-        s32, s64 = g32.get_state(), g64.get_state()
+        # the workload's own length: 2,000 steps of both forms on the same
+        # seed, errors recorded along the way
+        traj = {}
+        done = 0
+        for mark in (50, 500, 2000):
+            g32.time_integration(mark - done)
+            g64.time_integration(mark - done)
+            done = mark
+            s32, s64 = g32.get_state(), g64.get_state()
+            traj[str(mark)] = {k: rel(s32[k], s64[k]) for k in ("vx", "h", "A")}
         g32.close()
         g64.close()
         out["mixed_single_instance"] = {
@@ -346,7 +354,11 @@ def run_forms(args, which):
             "fp64_same_basin": res["fp64"], "steps": args.steps,
             "l2": "not flushed: one call of K steps; per-step working set > 126 MB L2",
             "err_vs_fp64": {"rhs_rel_l2": err_rhs,
-                            "traj50_rel_l2": {k: rel(s32[k], s64[k]) for k in ("vx", "h")}}}
+                            "traj_rel_l2_by_step": traj,
+                            "bound": "1e-4 relative L2 (velocity, thickness) against FP64 on the same seed",
+                            "dt_s": b.params.dt, "vp_dt_bound_s": basins.vp_dt_bound(b.dx),
+                            "note": "dt under the reference's viscous-plastic bound (time_step.f90:155); above "
+                                    "it any rounding difference, a reordered FP64 sum included, grows every step"}}
     if "batched" in which:
         # 64 uneven basins (log-uniform 4,096..262,144 particles), mixed
         bs = basins.cfg4(64, steps=500)
@@ -359,10 +371,22 @@ def run_forms(args, which):
             l0 = bt.kernel_launches()
             ms = _device_steps(bt.step, st, args.steps)
             launches = bt.kernel_launches() - l0
+            # the kernels' own time of the same number of steps (in-graph
+            # events): what separates it from the step time is the launch
+            # gaps, the most a single persistent launch per sub-step could save
+            bt.lib.simp_gpu_profile(bt.h, 1)
+            bt.step(args.steps)
+            kms = (ctypes.c_double * 6)()
+            nst = ctypes.c_int64()
+            bt.lib.simp_gpu_kernel_times(bt.h, kms, 6, ctypes.byref(nst))
+            bt.lib.simp_gpu_profile(bt.h, 0)
+            kernel_ms = sum(kms) / max(1, nst.value)
         out["batched_ensemble"] = {
             "workload": f"64 basins, {ntot} particles (log-uniform 4,096..262,144), dx=1 km, mixed, dt=1e-4 s",
             "metric": METRIC, "value": ntot * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
             "steps": args.steps, "launches_per_step": launches / args.steps,
+            "kernel_ms_per_step": kernel_ms,
+            "launch_gap_frac": max(0.0, 1.0 - kernel_ms / (ms / args.steps)),
             "l2": "not flushed: one call of K steps; working set > 126 MB L2"}
     if "served" in which:
         # offered load well above either arm's capacity (arrivals within a
@@ -383,8 +407,10 @@ def run_forms(args, which):
         served_value = sst["particle_steps"] / sst["makespan_s"]
         out["served_stream"] = {
             "workload": (f"{len(reqs)} requests, Poisson 100/s, particles log-uniform 1,024..1,048,576, "
-                         f"steps U(100, 2000) x {args.served_steps_scale}, dx=1 km, dt=1e-4 s, mixed, "
-                         "HBM budget 150 GB, FP64 replica of every 8th request"),
+                         "steps U(100, 2000)" + (f" x {args.served_steps_scale}" if args.served_steps_scale != 1.0 else "") +
+                         ", dx=1 km, dt=1e-4 s, mixed, HBM budget 150 GB, FP64 replica of every 8th request"),
+            "budget_capacity_particles": sst["capacity_particles"],
+            "peak_resident_frac_of_capacity": sst["peak_resident_particles"] / max(1.0, sst["capacity_particles"]),
             "metric": METRIC, "value": served_value, "p50_s": float(np.percentile(lat, 50)),
             "p99_s": float(np.percentile(lat, 99)), "makespan_s": sst["makespan_s"],
             "particle_steps": sst["particle_steps"], "peak_resident_requests": sst["peak_resident_requests"],
