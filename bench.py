@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--forms", default="mixed,batched,served",
                     help="comma list of the other forms to measure on rank 0 ('' for none)")
     ap.add_argument("--served-requests", type=int, default=64)
+    ap.add_argument("--served-rate", type=float, default=100.0, help="Poisson arrival rate of the served stream (1/s)")
     ap.add_argument("--served-steps-scale", type=float, default=1.0,
                     help="factor on the requests' step counts U(100, 2000) (1: as the served workload states)")
     return ap.parse_args()
@@ -391,10 +392,10 @@ def run_forms(args, which):
     if "served" in which:
         # offered load well above either arm's capacity (arrivals within a
         # fraction of a second), so the makespan measures capacity
-        reqs = serve.sample_stream(args.served_requests, seed=5, rate_hz=100.0,
+        reqs = serve.sample_stream(args.served_requests, seed=5, rate_hz=args.served_rate,
                                    steps_scale=args.served_steps_scale)
         big = max(r.basin.n for r in reqs)
-        with serve.Server(reqs[0].basin.params, 150e9, max_instances=256, max_request_particles=big,
+        with serve.Server(reqs[0].basin.params, 150e9, max_instances=1024, max_request_particles=big,
                           quantum_steps=32, spot_every=8) as srv:
             ids = [srv.submit(r) for r in reqs]
             srv.run()
@@ -406,7 +407,7 @@ def run_forms(args, which):
         ser = serve.serial_fp64(reqs)
         served_value = sst["particle_steps"] / sst["makespan_s"]
         out["served_stream"] = {
-            "workload": (f"{len(reqs)} requests, Poisson 100/s, particles log-uniform 1,024..1,048,576, "
+            "workload": (f"{len(reqs)} requests, Poisson {args.served_rate:g}/s, particles log-uniform 1,024..1,048,576, "
                          "steps U(100, 2000)" + (f" x {args.served_steps_scale}" if args.served_steps_scale != 1.0 else "") +
                          ", dx=1 km, dt=1e-4 s, mixed, HBM budget 150 GB, FP64 replica of every 8th request"),
             "budget_capacity_particles": sst["capacity_particles"],

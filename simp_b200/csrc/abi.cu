@@ -61,6 +61,8 @@ __global__ void k_mark_removed(int n, int slot, int *pinst) {
     if (i < n && pinst[i] == slot) pinst[i] = -1;
 }
 
+__global__ void k_flag_inst(Inst *inst, int slot, int flag) { atomicOr(&inst[slot].flags, flag); }
+
 // One instance's state to its own particle order: stage = [x,y interleaved |
 // vx,vy interleaved | mass | rho | hsml | A | h], 9 n_k doubles.
 __global__ void k_pack_state(int n, int slot, int id_base, int nk, const int *__restrict__ pinst,
@@ -590,6 +592,8 @@ int stage_instance(simp_ctx *c, int n, const double *x, const double *vx, const 
 }
 
 // Appends the staged basin after the current particles and sorts it in.
+int flush_batch(simp_ctx *c, bool compact);
+
 int add_instance(simp_ctx *c, int slot, const simp_forcing &f, const Extents &e, int nb, const double *xb,
                  const double *massb, double t0) {
     const int n = e.n;
@@ -640,11 +644,15 @@ int add_instance(simp_ctx *c, int slot, const simp_forcing &f, const Extents &e,
     c->launches += 2;
     SIMP_CUDA(c, cudaGetLastError());
     c->n += n;
+    c->nb += nb;
     // the new basin's keys come last: only its own range is sorted, and the
-    // resident basins keep their places and their Verlet lists
-    TRY(layout(c));
-    TRY(rebuild(c, mask_of(slot), off, false));
-    SIMP_CUDA(c, cudaStreamSynchronize(s));
+    // resident basins keep their places and their Verlet lists.  A batch lays
+    // out and sorts the basins admitted since its last flush together, at
+    // the next flush (the next step, or a read of a basin).
+    c->pending_from = std::min(c->pending_from, off);
+    if (c->pending_due.empty()) c->pending_due.assign(kMaxSlots / 64, 0ull);
+    c->pending_due[(size_t)slot >> 6] |= 1ull << (slot & 63);
+    if (c->max_inst == 1) return flush_batch(c, false);
     return SIMP_OK;
 }
 
@@ -656,19 +664,60 @@ int inst_offset(const simp_ctx *c, int slot) {
     return off;
 }
 
+// A retired basin leaves the batch at once (it is neither searched nor
+// stepped, and its slot reads as free), but its particles keep their places
+// until a compaction drops all retired basins together: when they make up a
+// quarter of the batch, or an admission needs their room or slot.  Every
+// compaction moves the basins after the first retired one down, as one
+// removal at a time would, so the survivors' results do not change.
 int remove_instance(simp_ctx *c, int slot) {
     InstHost &h = c->insts[slot];
-    if (!h.active) return simp_fail(c, SIMP_ERR_BADARG, "slot is free");
-    const int from = inst_offset(c, slot);   // the basins after it shift down
-    cudaStream_t s = c->stream;
-    k_mark_removed<<<nblk(c->n, kB), kB, 0, s>>>(c->n, slot, c->pinst);
+    if (!h.active || h.retired) return simp_fail(c, SIMP_ERR_BADARG, "slot is free");
+    h.retired = true;
+    h.I.flags |= FLAG_RETIRED;
+    c->zombie_n += h.n;
+    k_flag_inst<<<1, 1, 0, c->stream>>>(c->inst_dev, slot, FLAG_RETIRED);
     c->launches += 1;
-    h = InstHost{};
-    TRY(layout(c));
-    TRY(rebuild(c, DueMask{}, from, false));
-    SIMP_CUDA(c, cudaStreamSynchronize(s));
+    SIMP_CUDA(c, cudaGetLastError());
+    if (c->max_inst == 1) return flush_batch(c, true);
     return SIMP_OK;
 }
+
+// The deferred work of a batch: with `compact`, every retired basin's
+// particles are dropped; the basins admitted since the last flush are laid
+// out and sorted.  One layout and one sort from the first position that
+// changes.
+int flush_batch(simp_ctx *c, bool compact) {
+    int from = c->pending_from;
+    DueMask due{};
+    for (size_t w = 0; w < c->pending_due.size() && w < (size_t)(kMaxSlots / 64); ++w) due.w[w] = c->pending_due[w];
+    bool any = from != 0x7fffffff;
+    if (compact && c->zombie_n > 0) {
+        for (int q = 0; q < c->max_inst; ++q) {
+            const InstHost &h = c->insts[q];
+            if (!h.active || !h.retired) continue;
+            from = std::min(from, inst_offset(c, q));   // (offsets before any is dropped)
+            k_mark_removed<<<nblk(c->n, kB), kB, 0, c->stream>>>(c->n, q, c->pinst);
+            c->launches += 1;
+            due.w[q >> 6] &= ~(1ull << (q & 63));
+        }
+        for (InstHost &h : c->insts)
+            if (h.active && h.retired) h = InstHost{};
+        c->zombie_n = 0;
+        any = true;
+    }
+    if (!any) return SIMP_OK;
+    TRY(layout(c));
+    TRY(rebuild(c, due, from, false));
+    SIMP_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->pending_from = 0x7fffffff;
+    c->pending_due.clear();
+    return SIMP_OK;
+}
+
+// Before a step: the pending admissions, and a compaction once retired
+// basins hold a quarter of the batch's particles.
+int flush_for_step(simp_ctx *c) { return flush_batch(c, c->zombie_n > 0 && 4 * c->zombie_n >= c->n); }
 
 int reset_all(simp_ctx *c) {
     for (InstHost &h : c->insts) h = InstHost{};
@@ -1030,6 +1079,7 @@ double bytes_per_particle(const simp_params &p) {
 int step_enqueue(simp_ctx *c, int nsteps) {
     if (!c->have_state) return simp_fail(c, SIMP_ERR_STATE, "step before set_state");
     cudaStream_t s = c->stream;
+    TRY(flush_for_step(c));
     if (c->n == 0 || nsteps == 0) return SIMP_OK;   // (an empty batch)
     TRY(check_normals(c));
     // (a grid outgrown by hsml is re-made only at the basin's scheduled
@@ -1045,7 +1095,7 @@ int step_enqueue(simp_ctx *c, int nsteps) {
         bool any = false;
         for (int q = 0; q < c->max_inst; ++q) {
             InstHost &h = c->insts[q];
-            if (h.active && h.steps_since_sort >= kSortEvery) {
+            if (h.active && !h.retired && h.steps_since_sort >= kSortEvery) {
                 due.w[q >> 6] |= 1ull << (q & 63);
                 h.steps_since_sort = 0;
                 any = true;
@@ -1069,7 +1119,7 @@ int step_enqueue(simp_ctx *c, int nsteps) {
         c->launches += c->graph_kernels;
         c->lists_valid = true;
         for (InstHost &h : c->insts)
-            if (h.active) {
+            if (h.active && !h.retired) {
                 ++h.steps_since_sort;
                 ++h.steps_done;
             }
@@ -1105,6 +1155,8 @@ int step_complete(simp_ctx *c, double *current_time, double *dt) {
 
 int batch_slot_state(simp_ctx *c, int slot, double *x, double *vx, double *mass, double *rho, double *hsml,
                      double *A, double *h, double *t) {
+    if (!c->insts[slot].active || c->insts[slot].retired) return simp_fail(c, SIMP_ERR_BADARG, "slot is free");
+    TRY(flush_batch(c, false));
     return get_instance_state(c, slot, x, vx, mass, rho, hsml, A, h, t);
 }
 
@@ -1306,9 +1358,20 @@ int32_t simp_gpu_batch_add(simp_ctx *c, const simp_forcing *forcing, int32_t nto
                            const double *massb, int32_t *slot) {
     if (!c || !forcing || !slot) return SIMP_ERR_BADARG;
     if (!c->stream) return simp_fail(c, SIMP_ERR_STATE, "context was not created successfully");
-    int q = -1;
-    for (int k = 0; k < c->max_inst; ++k)
-        if (!c->insts[k].active) { q = k; break; }
+    auto free_slot = [&]() {
+        for (int k = 0; k < c->max_inst; ++k)
+            if (!c->insts[k].active) return k;
+        return -1;
+    };
+    int q = free_slot();
+    // retired basins still hold their slots and room until a compaction,
+    // which an admission runs when it needs them, or once they make up a
+    // quarter of the batch
+    if ((q < 0 || c->n + (long long)ntotal > c->maxn || c->nb + (long long)ntotalb > c->maxnb ||
+         4 * c->zombie_n >= c->n) && c->zombie_n > 0) {
+        TRY(flush_batch(c, true));
+        q = free_slot();
+    }
     if (q < 0) return simp_fail(c, SIMP_ERR_MAXN, "no free slot in the batch");
     Extents e{};
     TRY(stage_instance(c, ntotal, x, vx, mass, rho, hsml, A, h, ntotalb, xb, massb, &e));
@@ -1374,18 +1437,21 @@ int32_t simp_gpu_batch_remove(simp_ctx *c, int32_t slot) {
 int32_t simp_gpu_batch_get_state(simp_ctx *c, int32_t slot, double *x, double *vx, double *mass, double *rho,
                                  double *hsml, double *A, double *h, double *current_time) {
     if (!c || slot < 0 || slot >= c->max_inst) return SIMP_ERR_BADARG;
-    if (!c->insts[slot].active) return simp_fail(c, SIMP_ERR_BADARG, "slot is free");
+    if (!c->insts[slot].active || c->insts[slot].retired) return simp_fail(c, SIMP_ERR_BADARG, "slot is free");
+    TRY(flush_batch(c, false));
     return get_instance_state(c, slot, x, vx, mass, rho, hsml, A, h, current_time);
 }
 
 int32_t simp_gpu_batch_info(simp_ctx *c, int32_t slot, int32_t *ntotal, int64_t *steps, int32_t *flags) {
     if (!c || slot < 0 || slot >= c->max_inst) return SIMP_ERR_BADARG;
     const InstHost &h = c->insts[slot];
-    if (ntotal) *ntotal = h.active ? h.n : 0;
+    const bool live = h.active && !h.retired;
+    if (ntotal) *ntotal = live ? h.n : 0;
     if (steps) *steps = h.steps_done;
     if (flags) {
         *flags = 0;
-        if (h.active) {
+        if (live) {
+            TRY(flush_batch(c, false));
             Inst I{};
             TRY(read_inst(c, slot, &I));
             *flags = I.flags;
@@ -1575,6 +1641,7 @@ static int time_rhs(simp_ctx *c, int reps, double *ms) {
 int32_t simp_gpu_autotune(simp_ctx *c, int32_t reps, double *ms_best) {
     if (!c || reps < 1) return SIMP_ERR_BADARG;
     if (!c->have_state || c->n == 0) return simp_fail(c, SIMP_ERR_STATE, "autotune needs particles");
+    TRY(flush_batch(c, true));
     struct Cand { int impl, threads, cap; };
     const Cand cands[] = {
         {SIMP_PASSES_TILED, 128, 512},  {SIMP_PASSES_TILED, 128, 768},  {SIMP_PASSES_TILED, 128, 1024},

@@ -149,7 +149,7 @@ __global__ void k_refresh_sortpos(int n, const int *__restrict__ pinst, DueMask 
     if (i >= n) return;
     const int q = pinst[i];
     if (q < 0 || !((due.w[q >> 6] >> (q & 63)) & 1ull)) return;
-    if (inst[q].flags & FLAG_NONFINITE) return;
+    if (inst_dead(inst[q].flags)) return;
     xr[i] = x[i];
     yr[i] = y[i];
 }

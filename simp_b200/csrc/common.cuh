@@ -141,7 +141,14 @@ struct Scalars {
     int pad2;
 };
 
-enum : int { FLAG_NONFINITE = 1 };
+enum : int { FLAG_NONFINITE = 1, FLAG_RETIRED = 2 };
+
+// A basin that is neither searched nor stepped: its state turned non-finite
+// (it is carried until the caller retires it), or it was retired and its
+// storage waits for the next compaction of the batch.
+__host__ __device__ __forceinline__ bool inst_dead(int flags) {
+    return (flags & (FLAG_NONFINITE | FLAG_RETIRED)) != 0;
+}
 
 // Ordered-bits helpers for non-negative doubles (bit order = value order).
 __device__ __forceinline__ unsigned long long dbits(double v) {

@@ -12,6 +12,7 @@
 // Host bookkeeping of one instance slot.
 struct InstHost {
     bool active = false;
+    bool retired = false;          // removed, storage kept until the next compaction
     simp::Inst I{};                // host copy of the device table entry
     int n = 0, nb = 0;             // particles and wall particles
     int id_base = 0;               // global particle id = id_base + local index
@@ -52,6 +53,13 @@ struct simp_ctx {
     int ninst = 0;                 // table entries in use (highest active slot + 1)
     int id_stride = 0;             // 0 for a single basin, 1 << 21 for batches
     long long next_order = 0;      // admission counter
+    // batches defer the layout and the sort of admissions and the removal of
+    // retired basins to the next flush (abi.cu: flush_batch): the first
+    // position written since, the admitted slots still to sort, and the
+    // particles of retired basins still in place
+    int pending_from = 0x7fffffff;
+    std::vector<unsigned long long> pending_due;
+    long long zombie_n = 0;
     int total_cells = 0;           // cell keys over all instances
 
     // particle state sets (device, cell order)

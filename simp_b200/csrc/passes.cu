@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<T>::kin) k_kinematic(KinArgs
     const Inst &I = a.inst[a.pinst[i]];
     // a basin whose state turned non-finite is not searched any more (its
     // stencil would span its whole grid); it is only carried until retired
-    const bool dead = (I.flags & FLAG_NONFINITE) != 0;
+    const bool dead = inst_dead(I.flags);
     const PairCtx pc = pair_ctx(s, a.sc, I, a.cell_start, i);
     const double xi = pc.xi, yi = pc.yi, hi = pc.hi;
     const double vxi = s.vx[i], vyi = s.vy[i];
@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(kBlock, SIMP_FIND_MIN_BLOCKS) k_find_pairs(Kin
     const Inst &I = a.inst[a.pinst[i]];
     // a basin whose state turned non-finite is not searched any more (its
     // stencil would span its whole grid); it is only carried until retired
-    const bool dead = (I.flags & FLAG_NONFINITE) != 0;
+    const bool dead = inst_dead(I.flags);
     const PairCtx pc = pair_ctx(s, a.sc, I, a.cell_start, i);
     int npairs = 0;
     auto on_pair = [&](int j) {
@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<T>::stress) k_stress(StressA
     const int ci = a.cell[i];
     const int ki = a.pinst[i];
     const Inst &I = a.inst[ki];
-    const bool dead = (I.flags & FLAG_NONFINITE) != 0;   // see k_kinematic
+    const bool dead = inst_dead(I.flags);   // see k_kinematic
     StressSums<T> ss;
     const T hiT = Nb<T>::h(s, i), inv_hiT = (T)inv_hi;
     auto accumulate = [&](int j) {
@@ -283,8 +283,10 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<T>::stress) k_stress(StressA
             ++cnt;
         });
     }
-    stress_finish<SKF>(a, i, live, ki, I, dead, xi, yi, hi, ci, ss.sx.get(), ss.sy.get(), ss.tx.get(), ss.ty.get(),
-                       cnt, true);
+    // (a retired basin's particles are not written any more: their state
+    // stays as it was until the batch's next compaction drops them)
+    stress_finish<SKF>(a, i, live && !(I.flags & FLAG_RETIRED), ki, I, dead, xi, yi, hi, ci, ss.sx.get(), ss.sy.get(),
+                       ss.tx.get(), ss.ty.get(), cnt, true);
 }
 
 // Regularisation of a right-hand side (regularization.f90, called by
@@ -370,7 +372,7 @@ __global__ void __launch_bounds__(kBlock) k_regularize(RegArgs a) {
             avy.madd(-(mj * pij), pg.gfac * pg.dy);
         }
     };
-    const bool dead = (I.flags & FLAG_NONFINITE) != 0;
+    const bool dead = inst_dead(I.flags);
     const int cnt = a.pl.count[i];
     if (dead) {
     } else if (cnt <= kMaxPairs) {
@@ -417,12 +419,12 @@ struct DensArgs {
 
 __global__ void __launch_bounds__(kBlock) k_density_rate(DensArgs a) {
     const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = i0 < a.n;
-    const int i = live ? i0 : a.n - 1;   // dead lanes mirror the last particle for the reductions
+    const int i = i0 < a.n ? i0 : a.n - 1;   // dead lanes mirror the last particle for the reductions
     const State &g = a.g;
     const Phys &P = a.P;
     const Inst &I = a.inst[a.pinst[i]];
-    const bool dead = (I.flags & FLAG_NONFINITE) != 0;
+    const bool live = i0 < a.n && !(I.flags & FLAG_RETIRED);   // (a retired basin is not written)
+    const bool dead = inst_dead(I.flags);
     const double xi = g.x[i], yi = g.y[i], hi = g.hs[i];
     const double inv_hi = 1.0 / hi;
     const double vxi = a.v.vx[i], vyi = a.v.vy[i];

@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(kMaxTileThreads) k_kin_tiled(KinArgs a) {
     __syncthreads();
     const State &s = a.s;
     const Phys &P = a.P;
-    const bool dead = (I.flags & FLAG_NONFINITE) != 0;
+    const bool dead = inst_dead(I.flags);
     const KinTile<T> tl = kin_tile<T>(smem, a.cap);
     if (fits) {
         for_halo(h, [&](int j, int k) {
@@ -420,7 +420,7 @@ __global__ void __launch_bounds__(kMaxTileThreads) k_stress_tiled(StressArgs a) 
     const double xi = s.x[i], yi = s.y[i], hi = s.hs[i];
     const double inv_hi = 1.0 / hi;
     const int ci = a.cell[i];
-    const bool dead = (I.flags & FLAG_NONFINITE) != 0;
+    const bool dead = inst_dead(I.flags);
     StressSums<T> ss;
     const T hiT = Nb<T>::h(s, i), inv_hiT = (T)inv_hi;
     auto terms = [&](double xj, double yj, T hj, T mj, T t11, T t12, T t22) {
@@ -469,8 +469,9 @@ __global__ void __launch_bounds__(kMaxTileThreads) k_stress_tiled(StressArgs a) 
             ++cnt;
         });
     }
-    stress_finish<SKF>(a, i, live, ch.q, I, dead, xi, yi, hi, ci, ss.sx.get(), ss.sy.get(), ss.tx.get(), ss.ty.get(),
-                  cnt, true);
+    // (a retired basin's particles are not written any more)
+    stress_finish<SKF>(a, i, live && !(I.flags & FLAG_RETIRED), ch.q, I, dead, xi, yi, hi, ci, ss.sx.get(),
+                       ss.sy.get(), ss.tx.get(), ss.ty.get(), cnt, true);
 }
 
 int chunk_bound(const simp_ctx *c) {

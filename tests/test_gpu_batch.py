@@ -152,3 +152,36 @@ def test_batch_rejects_adaptive_dt(gpu_lib):
     with pytest.raises(SimpError) as ex:
         Batch(prm, 1000, 100, 4)
     assert ex.value.code == SIMP_ERR_BADARG
+
+
+def test_retired_basins_compacted_later(gpu_lib):
+    """A basin that leaves a batch is retired at once (its slot reads as
+    free, it is neither searched nor stepped) and dropped from memory by a
+    later compaction, which runs once retired basins hold a quarter of the
+    batch or an admission needs their slot.  The basins that stay give the
+    same bits as alone throughout."""
+    A = _inst(5, 1600)
+    small = [_inst(10 + k, 100) for k in range(3)]
+    prm = A.params
+    with _batch(prm, slots=4) as alone:
+        sa = alone.add(A)
+        alone.step(30)
+        ref = alone.get_state(sa)
+    with _batch(prm, slots=4) as mix:
+        sa = mix.add(A)
+        ss = [mix.add(b) for b in small]       # every slot taken
+        mix.step(10)
+        mix.remove(ss[0])                      # 100 of 1,900 particles: kept in place for now
+        assert mix.info(ss[0])["ntotal"] == 0
+        with pytest.raises(SimpError) as e:
+            mix.get_state(ss[0])
+        assert e.value.code == SIMP_ERR_BADARG
+        mix.step(10)
+        mix.remove(ss[1])
+        s_new = mix.add(_inst(20, 144))        # no free slot: the retired ones are compacted first
+        assert s_new in (ss[0], ss[1])
+        mix.step(10)
+        got = mix.get_state(sa)
+        assert mix.info(sa)["steps"] == 30
+        assert mix.info(ss[2])["steps"] == 30
+    _assert_bitwise(got, ref, "alone vs batch with retirements and a compaction")
