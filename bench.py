@@ -45,8 +45,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--forms", default="mixed,batched,served",
                     help="comma list of the other forms to measure on rank 0 ('' for none)")
-    ap.add_argument("--served-requests", type=int, default=64)
-    ap.add_argument("--served-rate", type=float, default=100.0, help="Poisson arrival rate of the served stream (1/s)")
+    # enough requests, arriving fast enough, that the 150 GB budget binds
+    # (about 97M resident particles of this size distribution)
+    ap.add_argument("--served-requests", type=int, default=700)
+    ap.add_argument("--served-rate", type=float, default=1000.0, help="Poisson arrival rate of the served stream (1/s)")
     ap.add_argument("--served-steps-scale", type=float, default=1.0,
                     help="factor on the requests' step counts U(100, 2000) (1: as the served workload states)")
     return ap.parse_args()
@@ -257,7 +259,10 @@ def run_ours(args):
                          f"({el:.1f} s), C++ FP64 restatement of the reference, OpenMP threads={threads}"}
     sim.close()
     forms = None
-    if rank == 0 and args.forms:
+    # (the other forms are one-GPU measurements of rank 0; under torchrun the
+    # other ranks would wait for them at the closing barrier, so they run
+    # only at N = 1)
+    if rank == 0 and world == 1 and args.forms:
         forms = run_forms(args, [f for f in args.forms.split(",") if f])
     if rank == 0:
         line = {

@@ -173,9 +173,8 @@ def test_retired_basins_compacted_later(gpu_lib):
         mix.step(10)
         mix.remove(ss[0])                      # 100 of 1,900 particles: kept in place for now
         assert mix.info(ss[0])["ntotal"] == 0
-        with pytest.raises(SimpError) as e:
-            mix.get_state(ss[0])
-        assert e.value.code == SIMP_ERR_BADARG
+        rc = mix.lib.simp_gpu_batch_get_state(mix.h, ss[0], None, None, None, None, None, None, None, None)
+        assert rc == SIMP_ERR_BADARG
         mix.step(10)
         mix.remove(ss[1])
         s_new = mix.add(_inst(20, 144))        # no free slot: the retired ones are compacted first
