@@ -487,3 +487,27 @@ def test_con_density_mixed_precision(gpu_lib):
     for k in ("rho", "vx", "h"):
         assert rel_l2(s32[k], s64[k]) < 1e-6, (k, rel_l2(s32[k], s64[k]))
     assert not np.array_equal(s64["rho"], b.rho)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3])
+@pytest.mark.parametrize("walls", ["", "+x"])
+def test_tiny_basins(gpu_lib, oracle_mod, n, walls):
+    """Ragged smallest inputs: one, two or three particles (no pair, one
+    pair, a chain), with and without a wall line: pairs, one right-hand side
+    and five steps against the oracle."""
+    b = basins.make_basin(3, 2000.0, 60 + n, walls=walls)
+    keep = np.arange(n)
+    for k in ("mass", "rho", "hsml", "A", "h"):
+        setattr(b, k, getattr(b, k)[keep].copy())
+    b.x = b.x[keep].copy()
+    b.vx = np.tile([0.2, -0.1], (n, 1)) * (1.0 + np.arange(n))[:, None]
+    g, o = _pair(b, oracle_mod)
+    assert_same_pairs(g.nnps(), o.nnps())
+    rg, ro = g.single_step(600.0), o.single_step(600.0)
+    for k in ("dxdt", "dvxdt", "dhdt", "dAdt"):
+        assert rel_l2(rg[k], ro[k]) < TOL_RHS, (k, rel_l2(rg[k], ro[k]))
+    g.time_integration(5)
+    o.step(5)
+    sg, so = g.get_state(), o.get_state()
+    for k in ("x", "vx", "h", "A"):
+        assert rel_l2(sg[k], so[k]) < 1e-9, (k, rel_l2(sg[k], so[k]))
