@@ -184,3 +184,25 @@ def test_retired_basins_compacted_later(gpu_lib):
         assert mix.info(sa)["steps"] == 30
         assert mix.info(ss[2])["steps"] == 30
     _assert_bitwise(got, ref, "alone vs batch with retirements and a compaction")
+
+
+def test_full_ensemble_against_oracle(gpu_lib, oracle_mod):
+    """The batched workload at its full size (64 basins, 4,096..262,144
+    particles each, 5.2M in all, mixed precision, its own dt): after 5 steps
+    the three smallest basins and a median one against the FP64 oracle run
+    alone, within the mixed form's bar (measured ~1e-9 in velocity)."""
+    bs = basins.cfg4(64, steps=500)
+    order = np.argsort([x.n for x in bs])
+    with Batch(bs[0].params, sum(x.n for x in bs), sum(x.nb for x in bs), 64) as bt:
+        slots = [bt.add(x) for x in bs]
+        bt.step(5)
+        for k in list(order[:3]) + [order[32]]:
+            got = bt.get_state(slots[k])
+            prm = bs[k].params.copy()
+            prm.precision = PREC_FP64
+            o = oracle_mod.Oracle.from_basin(bs[k], prm)
+            o.step(5)
+            so = o.get_state()
+            for f in ("vx", "h", "A"):
+                e = rel_l2(got[f], so[f])
+                assert e < 1e-4, (bs[k].name, f, e)
