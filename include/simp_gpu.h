@@ -290,14 +290,18 @@ SIMP_API int32_t simp_gpu_batch_info(simp_ctx *ctx, int32_t slot, int32_t *ntota
  *   x       device, 2*n interleaved positions   hsml, mass, rho: device, n
  *   rho_out device, n (original order)          skf: SIMP_SKF_*
  *   stream  cudaStream_t to run on (NULL: the legacy default stream)
+ * The buffers must be device memory of the current device or managed
+ * memory; host arrays are refused with SIMP_ERR_BADARG.
  * It calls no cudaMalloc, cudaFree or allocating library routine: its cell
- * list lives in one fixed array inside the library (about 5 MB, held on
+ * list lives in one fixed array inside the library (about 7 MB, held on
  * every GPU that loads the library until the process exits).  n must be at
  * most SIMP_NOALLOC_MAX_PARTICLES, else SIMP_ERR_BADARG.  The first call on
- * each device looks up that array's device address, so make it before any
- * stream capture.  All calls share the array: calls that overlap on the GPU
- * race and must be serialised by the caller.  Asynchronous: returns after
- * enqueueing on stream. */
+ * each device (and the first after another CUDA context became current on
+ * it) looks up that array's device address, so make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race
+ * and must be serialised by the caller.  An error left by earlier work on
+ * the calling thread is reported as SIMP_ERR_CUDA before anything is
+ * launched.  Asynchronous: returns after enqueueing on stream. */
 #define SIMP_NOALLOC_MAX_PARTICLES 65536
 SIMP_API int32_t simp_gpu_sum_density_noalloc(const double *x, const double *hsml,
                                               const double *mass, const double *rho,
