@@ -95,8 +95,11 @@ typedef struct simp_params {
     int32_t pa_sph;            /* 1 (s_i/rho_i^2 + s_j/rho_j^2) stress_1,
                                   2 (s_i + s_j)/rho_j stress_2 (internal_stress.f90)  */
     int32_t skf;               /* SIMP_SKF_*                                            */
-    int32_t den_alg;           /* 3 diagnostic, 2 continuity (con_density) in the step;
-                                  1 summation: simp_gpu_sum_density (density.f90:20-30)  */
+    int32_t den_alg;           /* density.f90:20-30 in the step: 3 diagnostic,
+                                  2 continuity (con_density), 1 summation (sum_density
+                                  with the reference's kept kernel_zero array;
+                                  simp_gpu_sum_density is the sum alone, with W(0)
+                                  at each particle's own hsml)                         */
     int32_t bfa;               /* boundary force (boundary_force.f90:20-27): 1 Monaghan,
                                   2 Wang (needs simp_gpu_set_wall_normals), 3 Marquis  */
     int32_t viscosity;         /* globals.f90:180-187 logical switches (0/1)            */

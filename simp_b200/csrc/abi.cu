@@ -41,9 +41,10 @@ __global__ void k_deinterleave(int n, const double *__restrict__ in, double *__r
     b[i] = in[2 * i + 1];
 }
 
-// New particles [off, off + n): ids, instance, sort positions, m / rho.
+// New particles [off, off + n): ids, instance, sort positions, m / rho, and
+// the summation density's kept kernel_zero (initialize.f90:60).
 __global__ void k_init_new(int n, int off, int id_base, int slot, int *id, int *pinst, State s, double *xr,
-                           double *yr, int *nbr_count) {
+                           double *yr, int *nbr_count, double *k0) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const int i = off + k;
@@ -54,6 +55,7 @@ __global__ void k_init_new(int n, int off, int id_base, int slot, int *id, int *
     yr[i] = s.y[i];
     s.mor[i] = s.m[i] / s.rho[i];
     refresh_views(s, i);
+    if (k0) k0[i] = 0.0;
 }
 
 __global__ void k_mark_removed(int n, int slot, int *pinst) {
@@ -248,6 +250,7 @@ Phys make_phys(const simp_params &p, double max_hsml) {
     P.boundary_pressure = p.boundary_pressure;
     P.sle = p.sle;
     P.den_alg = p.den_alg;
+    P.nnps = p.nnps_algorithm;
     P.mass_from_area = p.mass_from_area;
     P.tse = p.tse;
     P.hsml_multiplicity = p.hsml_multiplicity;
@@ -303,8 +306,7 @@ int check_params(simp_ctx *c, const simp_params &p, bool batch) {
     if (p.eos_alg < 1 || p.eos_alg > 3) return bad("eos_alg (1, 2 or 3)");
     if (p.pa_sph != 1 && p.pa_sph != 2) return bad("pa_sph (1 or 2)");
     if (!skf_known(p.skf)) return bad("skf (1 to 9)");
-    if (p.den_alg != 2 && p.den_alg != 3)
-        return bad("den_alg (2 or 3 in the step; the summation density is simp_gpu_sum_density)");
+    if (p.den_alg < 1 || p.den_alg > 3) return bad("den_alg (1 summation, 2 continuity, 3 h rho_ice)");
     if (p.bfa < 1 || p.bfa > 3) return bad("bfa (1 Monaghan, 2 Wang, 3 Marquis)");
     if (p.bfa == 2 && batch) return bad("bfa = 2 (wall normals) in a batch");
     if (p.precision != SIMP_PREC_FP64 && p.precision != SIMP_PREC_MIXED) return bad("precision (0 FP64, 1 mixed)");
@@ -332,7 +334,7 @@ void free_all(simp_ctx *c) {
                     c->pair_j, c->pair_count, c->nbr_tmp, c->s0.hsf,
                     c->inst_dev, c->row_map, c->chunk_cnt, c->chunk_off, c->chunks, c->s0.xy, c->s0.vxy,
                     c->s0.pf, c->s0.mm, c->s0.hmm, c->s1.xy, c->s1.vxy, c->s1.pf, c->s1.mm, c->s1.hmm,
-                    c->tau_a, c->tau_b, c->tau_q, c->pair_dw, c->drhodt, c->red_dev, c->reg};
+                    c->tau_a, c->tau_b, c->tau_q, c->pair_dw, c->drhodt, c->k0, c->red_dev, c->reg};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->sc_host) cudaFreeHost(c->sc_host);
@@ -639,7 +641,7 @@ int add_instance(simp_ctx *c, int slot, const simp_forcing &f, const Extents &e,
     cudaStream_t s = c->stream;
     const int off = c->n;
     k_init_new<<<nblk(n, kB), kB, 0, s>>>(n, off, ih.id_base, slot, c->id, c->pinst, c->s0, c->xr, c->yr,
-                                          c->nbr_count);
+                                          c->nbr_count, c->k0);
     k_grow_xabs<<<1, 1, 0, s>>>(c->sc, pxa);
     c->launches += 2;
     SIMP_CUDA(c, cudaGetLastError());
@@ -793,14 +795,21 @@ void enqueue_step(simp_ctx *c, bool diag, bool prof) {
     // divergence takes the updated velocities)
     const bool den2 = c->prm.den_alg == 2, benz = c->prm.sle == 1;
     const bool tsdiv = c->prm.tse == 1 && c->prm.artificial_visc;
+    // summation density (den_alg 1, density.f90:41-100) replaces the
+    // update's density by a pass over the right-hand side's pairs with the
+    // masses and densities of the reference's call; its last call of the
+    // step also does the tail above
+    const bool den1 = c->prm.den_alg == 1;
+    State &s0 = c->s0, &s1 = c->s1;
     mark(0);
     if (c->prm.int_algorithm == 1) {
         // euler_scheme (time_integration.f90:86-148): one right-hand side
-        launch_kinematic(c, c->s0, diag);
-        launch_regularize(c, c->s0);
+        launch_kinematic(c, s0, diag);
+        launch_regularize(c, s0);
         mark(1);
-        launch_stress(c, c->s0, c->s0, EPI_EULER);
-        if (den2 || benz || tsdiv) launch_density_rate(c, c->s0, c->s1, den2 ? 2 : 0, true);
+        launch_stress(c, s0, s0, EPI_EULER);
+        if (den1) launch_sum_density(c, s0, s1, s0.m, s0.rho, s1.rho, true);         // :128
+        else if (den2 || benz || tsdiv) launch_density_rate(c, s0, s1, den2 ? 2 : 0, true);
         mark(2);
         launch_copy_s1_to_s0(c);
         mark(3);
@@ -809,18 +818,30 @@ void enqueue_step(simp_ctx *c, bool diag, bool prof) {
         // predictor_corrector (:155-282) or leapfrog_scheme (:289-391): the
         // same first half step, a different final update
         const bool leap = c->prm.int_algorithm == 3;
-        launch_kinematic(c, c->s0, false);
-        launch_regularize(c, c->s0);
+        launch_kinematic(c, s0, false);
+        launch_regularize(c, s0);
         mark(1);
-        launch_stress(c, c->s0, c->s0, EPI_PREDICT);
-        if (den2) launch_density_rate(c, c->s0, c->s1, 1, false);
+        launch_stress(c, s0, s0, EPI_PREDICT);
+        if (den1) launch_sum_density(c, s0, s1, s0.m, s0.rho, s1.rho, false);        // :217, :344
+        else if (den2) launch_density_rate(c, s0, s1, 1, false);
         mark(2);
-        launch_kinematic(c, c->s1, diag);
-        launch_regularize(c, c->s1);
+        launch_kinematic(c, s1, diag);
+        launch_regularize(c, s1);
         mark(3);
-        launch_stress(c, c->s1, c->s0, leap ? EPI_LEAP : EPI_CORRECT);
-        if (leap ? (den2 || benz || tsdiv) : (benz || tsdiv))
-            launch_density_rate(c, c->s1, c->s0, (leap && den2) ? 2 : 0, true);
+        launch_stress(c, s1, s0, leap ? EPI_LEAP : EPI_CORRECT);
+        if (den1 && leap) {
+            launch_sum_density(c, s1, s0, s1.m, s1.rho, s0.rho, true);                // :372
+        } else if (den1) {
+            // two calls (:242 and :262) over the corrector's pairs, the
+            // second reading the first's densities: the second writes
+            // scratch (the half-step density, no longer read) and is
+            // copied in after
+            launch_sum_density(c, s1, s0, s1.m, s1.rho, s0.rho, false);
+            launch_sum_density(c, s1, s0, s1.m, s0.rho, s1.rho, true);
+            launch_commit_rho(c, s1.rho, s0);
+        } else if (leap ? (den2 || benz || tsdiv) : (benz || tsdiv)) {
+            launch_density_rate(c, s1, s0, (leap && den2) ? 2 : 0, true);
+        }
         mark(4);
     }
     launch_step_finish(c);
@@ -972,8 +993,9 @@ int create(const simp_params *params, int32_t maxn, int32_t maxnb, int32_t max_i
     TRY(dalloc(c, &c->id, M));
     TRY(dalloc(c, &c->pinst, M));
     TRY(dalloc(c, &c->perm, M));
-    TRY(dalloc(c, &c->tmp, 15 * MX));
+    TRY(dalloc(c, &c->tmp, 16 * MX));
     if (c->prm.sle == 1 && c->prm.den_alg != 2) TRY(dalloc(c, &c->drhodt, M));
+    if (c->prm.den_alg == 1) TRY(dalloc(c, &c->k0, M));
     TRY(dalloc(c, &c->itmp, 5 * MX));
     TRY(dalloc(c, &c->bx, MB));
     TRY(dalloc(c, &c->by, MB));
@@ -1069,7 +1091,8 @@ double bytes_per_particle(const simp_params &p) {
     b += 9 * 8.0 + 4 * 8.0;                                   // diagnostics, rates
     if (p.sle == 1 && p.den_alg != 2) b += 8.0;               // Benz's kept drhodt
     if (p.xsph_regularization || p.artificial_visc) b += 4 * 8.0;   // regularisation terms
-    b += 4 * 4.0 + 15 * 8.0 + 5 * 4.0 + 4.0;                  // sort keys, scratch
+    if (p.den_alg == 1) b += 8.0;                             // kept kernel_zero
+    b += 4 * 4.0 + 16 * 8.0 + 5 * 4.0 + 4.0;                  // sort keys, scratch
     b += 16.0 / kMinTileThreads + 48.0;                       // chunks, cell lists (worst case)
     return b;
 }
@@ -1218,6 +1241,8 @@ int continue_state(simp_ctx *c, int n, const double *x, const double *vx, const 
     k_continue_finish<<<1, 1, 0, s>>>(c->sc, c->inst_dev, dt, t, v[2], v[3], v[4], c->prm.sle != 0 ? 1 : 0);
     c->launches += 1;
     SIMP_CUDA(c, cudaGetLastError());
+    // (a set state starts the kept kernel_zero again, initialize.f90:60)
+    if (c->k0) SIMP_CUDA(c, cudaMemsetAsync(c->k0, 0, sizeof(double) * (size_t)c->maxn, s));
     return SIMP_OK;
 }
 
@@ -1347,6 +1372,7 @@ int32_t simp_gpu_set_state(simp_ctx *c, int32_t ntotal, const double *x, const d
     SIMP_CUDA(c, cudaMemcpyAsync(c->sc, c->sc_host, sizeof(Scalars), cudaMemcpyHostToDevice, c->stream));
     SIMP_CUDA(c, cudaMemsetAsync(c->inst_dev, 0, sizeof(Inst), c->stream));
     if (c->drhodt) SIMP_CUDA(c, cudaMemsetAsync(c->drhodt, 0, sizeof(double) * (size_t)c->maxn, c->stream));
+    if (c->k0) SIMP_CUDA(c, cudaMemsetAsync(c->k0, 0, sizeof(double) * (size_t)c->maxn, c->stream));
     TRY(add_instance(c, 0, forcing_of(c->prm), e, ntotalb, xb, massb, current_time));
     c->have_state = true;
     return SIMP_OK;
@@ -1543,6 +1569,9 @@ int32_t simp_gpu_single_step(simp_ctx *c, double current_time, double *dxdt, dou
     launch_kinematic(c, c->s0, true);
     launch_regularize(c, c->s0);
     launch_stress(c, c->s0, c->s0, EPI_RATES);
+    // the right-hand side's pair loop also sets the summation density's kept
+    // kernel_zero (kernel.f90:503): the density itself goes to scratch
+    if (c->k0) launch_sum_density(c, c->s0, c->s0, c->s0.m, c->s0.rho, c->tmp, false);
     SIMP_CUDA(c, cudaGetLastError());
     c->lists_valid = true;
     const size_t M = (size_t)c->maxn;

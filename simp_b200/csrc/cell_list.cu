@@ -187,7 +187,7 @@ __global__ void k_cell_sort(int ncells, const int *__restrict__ start, int *__re
     }
 }
 
-constexpr int kGathered = 13;   // (the last one only with Benz's kept drhodt)
+constexpr int kGathered = 14;   // (the last two only with Benz's kept drhodt and the kept kernel_zero)
 struct Gather {
     const double *src[kGathered];
     double *dst[kGathered];
@@ -352,7 +352,7 @@ int rebuild(simp_ctx *c, const DueMask &due, int from, bool new_lists) {
         if (c->total_cells > 0)
             k_cell_sort<<<nblk(c->total_cells, 128), 128, 0, s>>>(c->total_cells, c->cell_start, c->perm, c->id);
         double *srcs[kGathered] = {c->s0.x, c->s0.y, c->s0.vx, c->s0.vy, c->s0.m, c->s0.rho,
-                                   c->s0.mor, c->s0.h, c->s0.A, c->s0.hs, c->xr, c->yr, c->drhodt};
+                                   c->s0.mor, c->s0.h, c->s0.A, c->s0.hs, c->xr, c->yr, c->drhodt, c->k0};
         Gather gd;
         for (int a = 0; a < kGathered; ++a) {
             gd.src[a] = srcs[a];
@@ -365,7 +365,7 @@ int rebuild(simp_ctx *c, const DueMask &due, int from, bool new_lists) {
             c->launches += 1;
             if (keep_lists) {
                 NbrList nl{c->nbr, c->nbr_count, c->xl, c->yl, c->maxn};
-                double *xl_new = c->tmp + 13 * MX, *yl_new = c->tmp + 14 * MX;
+                double *xl_new = c->tmp + 14 * MX, *yl_new = c->tmp + 15 * MX;
                 k_remap_lists<<<nblk(kept, 128), 128, 0, s>>>(kept, from, due, c->pinst, c->perm, inv, n, nl,
                                                               c->nbr_tmp, cnt_new, xl_new, yl_new);
                 k_put_back_lists<<<nblk(kept, B), B, 0, s>>>(kept, from, due, c->pinst, nl, c->nbr_tmp, cnt_new,

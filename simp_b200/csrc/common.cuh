@@ -168,6 +168,7 @@ struct Phys {
     int sle, den_alg, mass_from_area, tse, hsml_multiplicity;
     int rheology, pa_sph, int_algorithm;
     int max_ind_int;
+    int nnps;       // 1 direct search, 2 bucket search (the pair orientation)
     double P_star, c_eos, e, delta_min, k_t;
     double rho_ice, rho_air, rho_water, c_wind, c_water;
     double b_length, kappa_n, alpha;

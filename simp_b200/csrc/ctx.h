@@ -66,6 +66,7 @@ struct simp_ctx {
     simp::State s0{}, s1{};
     double *mass1 = nullptr;       // half-step mass when the mass update is on
     double *drhodt = nullptr;      // Benz hsml without con_density: the reference's drhodt, kept across steps
+    double *k0 = nullptr;          // summation density in the step: the reference's kernel_zero, kept likewise
     double *red_dev = nullptr;     // per-block extents of a basin being admitted
     double *red_host = nullptr;    // (pinned copy)
     double *xr = nullptr, *yr = nullptr;  // sort positions (updated when the instance is re-sorted)
@@ -117,7 +118,7 @@ struct simp_ctx {
     // rebuild scratch
     int *cnt = nullptr;            // per-cell counters (cell_cap)
     int *perm = nullptr;           // maxn
-    double *tmp = nullptr;         // 15 * max(maxn, maxnb) doubles reorder scratch
+    double *tmp = nullptr;         // 16 * max(maxn, maxnb) doubles reorder scratch
     int *itmp = nullptr;           // 5 * max(maxn, maxnb) ints
     void *scan_tmp = nullptr;
     size_t scan_tmp_bytes = 0;
@@ -176,6 +177,12 @@ void launch_stress(simp_ctx *c, const State &nb, const State &own, EpiMode mode)
 // (con_density, Benz_hsml): rho_upd 0 none, 1 half step, 2 full step; tail:
 // the step's final hsml, its bounds and the VP dt
 void launch_density_rate(simp_ctx *c, const State &g, const State &v, int rho_upd, bool tail);
+// summation density (den_alg 1) over the last right-hand side's pairs at
+// state g: masses m_sum and densities rho_in of the reference's call, result
+// into rho_out (v.rho, or scratch for launch_commit_rho); tail as above
+void launch_sum_density(simp_ctx *c, const State &g, const State &v, const double *m_sum, const double *rho_in,
+                        double *rho_out, bool tail);
+void launch_commit_rho(simp_ctx *c, const double *src, const State &o);
 void launch_step_finish(simp_ctx *c);
 // XSPH and artificial viscosity of the right-hand side at s, over the pairs
 // the kinematic pass just found (a no-op when both are off)

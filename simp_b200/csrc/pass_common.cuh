@@ -755,11 +755,13 @@ __device__ __forceinline__ void stress_finish(const StressArgs &a, int i, bool l
     // with artificial viscosity needs the updated velocities of the
     // neighbours.
     const bool final_update = a.mode == EPI_CORRECT || a.mode == EPI_EULER || a.mode == EPI_LEAP;
-    const bool den2 = P.den_alg == 2;
-    const bool tail_later = final_update && ((den2 && a.mode != EPI_CORRECT) || P.sle == 1 ||
+    const bool den2 = P.den_alg == 2, den1 = P.den_alg == 1;
+    const bool tail_later = final_update && ((den2 && a.mode != EPI_CORRECT) || den1 || P.sle == 1 ||
                                              (P.tse == 1 && P.artificial_visc));
     double rhon;
-    if (!den2) {
+    if (den1) {
+        rhon = s.rho[i];   // the density of the call, until the summation pass replaces it
+    } else if (!den2) {
         rhon = hn * P.rho_ice;                                // density.f90:192
     } else if (a.mode == EPI_CORRECT) {
         // time_integration.f90:242-266: drho/dt of the corrector's density

@@ -415,6 +415,27 @@ struct DensArgs {
     Phys P;
     int n, rho_upd, tail;
     int dt_div;          // the Monaghan time step's divergence (artificial viscosity)
+    // summation density (den_alg = 1, density.f90:41-100): rho_out =
+    // (k0 m_i + sum_j m_j W_ij) / (k0 m_i / rho_i + sum_j m_j W_ij / rho_j)
+    // over the right-hand side's pairs and kernel values, with the masses
+    // m_sum and densities rho_in at the reference's density call; rho_out
+    // is o.rho (then m/rho and the packed copies follow) or a scratch array
+    // that k_commit_rho copies in
+    int sum_mode;
+    const double *m_sum, *rho_in;
+    double *rho_out;
+    // its self term kernel_zero(i) m_i: the reference keeps kernel_zero per
+    // particle and sets it in each right-hand side's pair loop for the p_i
+    // of every pair, W(0) at the pair's hsml (kernel.f90:503, set to 0 by
+    // initialize.f90:60), so a particle that is p_i of no pair keeps an
+    // earlier value.  Which particle of a pair is p_i follows the search:
+    // direct_find (nnps.f90:41-148) the lower index; the bucket search
+    // (nnps.f90:259-411) the lower index within one bucket, else the
+    // particle whose bucket has the other's to its right, above, above
+    // right or above left.  Of several pairs the serial pair order's last
+    // gives the value (it matters only where hsml varies)
+    double *k0;
+    const int *id;
 };
 
 __global__ void __launch_bounds__(kBlock) k_density_rate(DensArgs a) {
@@ -428,11 +449,42 @@ __global__ void __launch_bounds__(kBlock) k_density_rate(DensArgs a) {
     const double xi = g.x[i], yi = g.y[i], hi = g.hs[i];
     const double inv_hi = 1.0 / hi;
     const double vxi = a.v.vx[i], vyi = a.v.vy[i];
-    Sum<double> r, rt;
+    Sum<double> r, rt, num, den;
+    // p_i rule of the summation density's kernel_zero (DensArgs)
+    const int idi = a.sum_mode ? a.id[i] : 0;
+    const long long bxi = (a.sum_mode && P.nnps == 2) ? ref_bin(xi, I.bs) : 0;
+    const long long byi = (a.sum_mode && P.nnps == 2) ? ref_bin(yi, I.bs) : 0;
+    long long last = -1;   // (position in the serial pair order, category then index)
+    double h_last = 0.0;
     auto add = [&](int j) {
         if (!SIMP_IN_RANGE(j, 0, a.n, SITE_NEIGHBOUR)) return;
         const double2 q = g.xy[j];
-        const PairGeom<double> pg = pair_geom<double, false>(P, xi - q.x, yi - q.y, hi, inv_hi, g.hs[j]);
+        PairGeom<double> pg;
+        if (a.sum_mode) {
+            pg = pair_geom<double, true>(P, xi - q.x, yi - q.y, hi, inv_hi, g.hs[j]);
+            const double mw = a.m_sum[j] * pg.w;
+            num.madd(mw, 1.0);
+            den.madd(mw / a.rho_in[j], 1.0);
+            const int idj = a.id[j];
+            int cat = -1;
+            if (P.nnps != 2) {
+                cat = idj > idi ? 0 : -1;
+            } else {
+                const long long dx = ref_bin(q.x, I.bs) - bxi, dy = ref_bin(q.y, I.bs) - byi;
+                if (dx == 0 && dy == 0) cat = idj > idi ? 0 : -1;
+                else if (dy == 0 && dx == 1) cat = 1;     // right
+                else if (dy == 1 && dx == 0) cat = 2;     // up
+                else if (dy == 1 && dx == 1) cat = 3;     // up-right
+                else if (dy == 1 && dx == -1) cat = 4;    // up-left
+            }
+            const long long key = cat < 0 ? -1 : ((long long)cat << 32) | (long long)(unsigned)idj;
+            if (key > last) {
+                last = key;
+                h_last = g.hs[j];
+            }
+        } else {
+            pg = pair_geom<double, false>(P, xi - q.x, yi - q.y, hi, inv_hi, g.hs[j]);
+        }
         const double2 v = a.v.vxy[j];
         const double dvx = vxi - v.x, dvy = vyi - v.y;
         const double t = fma(dvx, pg.gfac * pg.dx, dvy * (pg.gfac * pg.dy));
@@ -457,7 +509,20 @@ __global__ void __launch_bounds__(kBlock) k_density_rate(DensArgs a) {
     const double dt = a.sc->dt;
     const State &o = a.v;
     double rhon = o.rho[i];
-    if (a.rho_upd && live) {
+    if (a.sum_mode) {
+        double k0 = a.k0[i];
+        if (last >= 0) k0 = kernel_zero(P, (hi + h_last) / 2.0);   // nnps.f90:278
+        const double k0m = k0 * a.m_sum[i];
+        rhon = (k0m + num.get()) / (k0m / a.rho_in[i] + den.get());
+        if (live) {
+            a.k0[i] = k0;
+            a.rho_out[i] = rhon;
+            if (a.rho_out == o.rho) {
+                o.mor[i] = o.m[i] / rhon;
+                refresh_views(o, i);
+            }
+        }
+    } else if (a.rho_upd && live) {
         rhon = (a.rho_upd == 1) ? a.rho1[i] + drhodt * dt / 2.0 : a.rho1[i] + drhodt * dt;
         o.rho[i] = rhon;
         o.mor[i] = o.m[i] / rhon;
@@ -501,6 +566,18 @@ __global__ void __launch_bounds__(kBlock) k_density_rate(DensArgs a) {
         if (live) v[5] = dbits(dt_candidate(P, hsn, P.tse == 1 ? a.a2[i] : 0.0, rhon, adiv));
     }
     block_bounds(a.sc, active, v);
+}
+
+// The summation density written to scratch by the second of two passes
+// into the state (the first pass read the state's density).
+__global__ void k_commit_rho(int n, const double *__restrict__ src, State o, const int *__restrict__ pinst,
+                             const Inst *__restrict__ inst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || (inst[pinst[i]].flags & FLAG_RETIRED)) return;
+    const double r = src[i];
+    o.rho[i] = r;
+    o.mor[i] = o.m[i] / r;
+    refresh_views(o, i);
 }
 
 // New hsml of the next step (sle = 1, 2) and its FP32 copy.
@@ -770,6 +847,43 @@ void launch_density_rate(simp_ctx *c, const State &g, const State &v, int rho_up
     a.tail = tail ? 1 : 0;
     a.dt_div = (tail && c->prm.tse == 1 && c->prm.artificial_visc) ? 1 : 0;
     k_density_rate<<<nblk(c->n, kBlock), kBlock, 0, c->stream>>>(a);
+    c->launches += 1;
+}
+
+void launch_sum_density(simp_ctx *c, const State &g, const State &v, const double *m_sum, const double *rho_in,
+                        double *rho_out, bool tail) {
+    SIMP_RANGE("summation-density pass");
+    DensArgs a{};
+    a.g = g;
+    a.v = v;
+    a.rho1 = c->s0.rho;
+    a.acc = c->drhodt;
+    a.mj = c->drhodt ? v.m : g.m;
+    a.a2 = c->rates;
+    a.hs_next = c->tmp;
+    a.pl = pair_list(c);
+    a.cell_start = c->cell_start;
+    a.cell = c->cell;
+    a.pinst = c->pinst;
+    a.inst = c->inst_dev;
+    a.sc = c->sc;
+    a.P = c->phys;
+    a.n = c->n;
+    a.rho_upd = 0;
+    a.tail = tail ? 1 : 0;
+    a.dt_div = (tail && c->prm.tse == 1 && c->prm.artificial_visc) ? 1 : 0;
+    a.sum_mode = 1;
+    a.m_sum = m_sum;
+    a.rho_in = rho_in;
+    a.rho_out = rho_out;
+    a.k0 = c->k0;
+    a.id = c->id;
+    k_density_rate<<<nblk(c->n, kBlock), kBlock, 0, c->stream>>>(a);
+    c->launches += 1;
+}
+
+void launch_commit_rho(simp_ctx *c, const double *src, const State &o) {
+    k_commit_rho<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->n, src, o, c->pinst, c->inst_dev);
     c->launches += 1;
 }
 
