@@ -250,6 +250,12 @@ def run_ours(args):
     # end to end through the C ABI with host buffers: upload the state from
     # pinned host memory, one step, download the state
     e2e = run_e2e(sim, b, stream, min(args.e2e_steps, args.steps), dist)
+    lk = e2e["link"]
+    # the floor: the step's copies at the link's plain rates around the
+    # device-timed step
+    floor_ms = lk["h2d_ms"] + lk["d2h_ms"] + dev_ms_max / args.steps
+    lk["floor_value"] = world * b.n / (floor_ms / 1e3)
+    lk["e2e_frac_of_floor"] = e2e["value"] / lk["floor_value"]
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -489,7 +495,35 @@ def run_e2e(sim, b, stream, nsteps, dist):
     d2h = n * (2 * 16 + 5 * 8) + 16
     return {"value": world * n * nsteps / (ms / 1e3), "unit": METRIC, "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "steps": nsteps,
-            "path": "simp_gpu_set_state (pinned host) + simp_gpu_step(1) + simp_gpu_get_state (pinned host)"}
+            "path": "simp_gpu_set_state (pinned host) + simp_gpu_step(1) + simp_gpu_get_state (pinned host)",
+            "link": link_copy_rates(stream, n * (2 * 16 + 5 * 8))}
+
+
+def link_copy_rates(stream, nbytes, reps=20):
+    """Plain pinned-host <-> device copies of one step's state bytes, as one
+    buffer each way: the host link's rate, the floor under the end-to-end
+    step (copies in, the step, copies out)."""
+    import torch
+    hb = torch.empty(nbytes // 8, dtype=torch.float64, pin_memory=True)
+    db = torch.empty(nbytes // 8, dtype=torch.float64, device="cuda")
+    out = {"bytes": nbytes}
+    with torch.cuda.stream(stream):
+        for name, f in (("h2d", lambda: db.copy_(hb, non_blocking=True)),
+                        ("d2h", lambda: hb.copy_(db, non_blocking=True))):
+            for _ in range(3):
+                f()
+            stream.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                f()
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            out[name + "_ms"] = ms
+            out[name + "_gbs"] = nbytes / ms / 1e6
+    return out
 
 
 def main():
