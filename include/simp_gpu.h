@@ -179,7 +179,8 @@ SIMP_API int32_t simp_gpu_set_state(simp_ctx *ctx, int32_t ntotal, const double 
                            double current_time);
 
 /* Download the state in the caller's original particle order.  Any pointer
- * may be NULL to skip that field. */
+ * may be NULL to skip that field.  After simp_gpu_step without outputs it
+ * also returns those steps' status (the state is written either way). */
 SIMP_API int32_t simp_gpu_get_state(simp_ctx *ctx, double *x, double *vx, double *mass,
                            double *rho, double *hsml, double *A, double *h,
                            double *dt, double *current_time);
@@ -221,7 +222,12 @@ SIMP_API int32_t simp_gpu_sum_density(simp_ctx *ctx, double *rho_out);
  * predictor_corrector :263-390), state resident on the device.  On return
  * *current_time and *dt hold the integrator's values; current_time advances
  * by the dt computed at the end of each step, as the reference does
- * (time_integration.f90:179). */
+ * (time_integration.f90:179).  With current_time and dt both NULL (single-
+ * basin contexts) the call returns once the steps are enqueued, without
+ * waiting for them: the next simp_gpu_get_state returns their status, and
+ * the next simp_gpu_step, simp_gpu_single_step or simp_gpu_nnps waits for
+ * them and returns it before doing anything else; simp_gpu_set_state drops
+ * it (the new state replaces theirs). */
 SIMP_API int32_t simp_gpu_step(simp_ctx *ctx, int32_t nsteps, double *current_time,
                       double *dt);
 

@@ -1048,6 +1048,13 @@ simp_forcing forcing_of(const simp_params &p) {
 
 namespace simp {
 
+int complete_pending(simp_ctx *c) {
+    if (!c->pending_check) return SIMP_OK;
+    c->pending_check = false;
+    TRY(read_scalars(c));
+    return check_after(c);
+}
+
 // Flag words of the debug build's index checks (check.cuh), one reader per
 // translation unit built with them.
 static std::vector<unsigned (*)()> &bounds_readers() {
@@ -1101,6 +1108,7 @@ double bytes_per_particle(const simp_params &p) {
 // waiting for them (profiling mode waits step by step).
 int step_enqueue(simp_ctx *c, int nsteps) {
     if (!c->have_state) return simp_fail(c, SIMP_ERR_STATE, "step before set_state");
+    TRY(complete_pending(c));   // (this step resets the statistics those steps left)
     cudaStream_t s = c->stream;
     TRY(flush_for_step(c));
     if (c->n == 0 || nsteps == 0) return SIMP_OK;   // (an empty batch)
@@ -1169,8 +1177,7 @@ int step_complete(simp_ctx *c, double *current_time, double *dt) {
         if (dt) *dt = c->prm.dt;
         return SIMP_OK;
     }
-    SIMP_CUDA(c, cudaStreamSynchronize(c->stream));
-    TRY(read_scalars(c));
+    TRY(read_scalars(c));   // (one wait: the scalars queue behind the steps)
     if (current_time) *current_time = c->sc_host->t;
     if (dt) *dt = c->sc_host->dt;
     return check_after(c);
@@ -1345,6 +1352,7 @@ int32_t simp_gpu_set_state(simp_ctx *c, int32_t ntotal, const double *x, const d
                          "The number of boundary particles generated is higher than the maximum "
                          "allowed. (boundaries.f90:296-303)");
     if (ntotal < 1) return simp_fail(c, SIMP_ERR_BADARG, "set_state: bad sizes or null arrays");
+    c->pending_check = false;   // (a new state replaces what steps without outputs left)
     const int cont = simp::continue_state(c, ntotal, x, vx, mass, rho, hsml, A, h, ntotalb, xb, massb, dt,
                                           current_time);
     if (cont != simp::kFreshState) return cont;   // continued in place, or a CUDA error
@@ -1494,6 +1502,10 @@ int32_t simp_gpu_get_state(simp_ctx *c, double *x, double *vx, double *mass, dou
     TRY(get_instance_state(c, 0, x, vx, mass, rho, hsml, A, h, nullptr, true));
     if (dt) *dt = c->sc_host->dt;
     if (current_time) *current_time = c->sc_host->t;
+    if (c->pending_check) {   // the status of steps enqueued without outputs
+        c->pending_check = false;
+        return check_after(c);
+    }
     return SIMP_OK;
 }
 
@@ -1561,6 +1573,7 @@ int32_t simp_gpu_single_step(simp_ctx *c, double current_time, double *dxdt, dou
     if (!c) return SIMP_ERR_BADARG;
     if (!c->have_state || c->max_inst != 1) return simp_fail(c, SIMP_ERR_STATE, "single_step needs a single basin with state");
     SIMP_RANGE("simp_gpu_single_step");
+    TRY(complete_pending(c));
     TRY(check_normals(c));
     cudaStream_t s = c->stream;
     k_set_time0<<<1, 1, 0, s>>>(c->sc, c->inst_dev, current_time);
@@ -1605,6 +1618,12 @@ int32_t simp_gpu_step(simp_ctx *c, int32_t nsteps, double *current_time, double 
     if (!c || nsteps < 0) return SIMP_ERR_BADARG;
     SIMP_RANGE("simp_gpu_step");
     TRY(simp::step_enqueue(c, nsteps));
+    if (!current_time && !dt && c->max_inst == 1 && c->n > 0 && nsteps > 0) {
+        // no outputs: return once enqueued; the next get_state or step
+        // reads the status in its own wait
+        c->pending_check = true;
+        return SIMP_OK;
+    }
     return simp::step_complete(c, current_time, dt);
 }
 

@@ -83,6 +83,7 @@ struct simp_ctx {
     int *nbr_count = nullptr;      // maxn
     int *nbr_tmp = nullptr;        // kMaxNbr * maxn: lists being renamed by a sort
     bool lists_valid = false;      // every particle's list was built by a kinematic pass
+    bool pending_check = false;    // steps simp_gpu_step enqueued without outputs, status not read yet
     int *pair_j = nullptr;         // kMaxPairs * maxn exact pairs of the current RHS
     int *pair_count = nullptr;     // maxn
     void *pair_dw = nullptr;       // kernel gradient per pair: kDwRows x maxn float2 (mixed form only)
@@ -202,6 +203,8 @@ double bytes_per_particle(const simp_params &p);
 // abi.cu: the step driver split for callers that overlap contexts
 int step_enqueue(simp_ctx *c, int nsteps);
 int step_complete(simp_ctx *c, double *current_time, double *dt);
+// the status of steps enqueued without outputs (waits for them); SIMP_OK when none
+int complete_pending(simp_ctx *c);
 int batch_slot_state(simp_ctx *c, int slot, double *x, double *vx, double *mass, double *rho, double *hsml,
                      double *A, double *h, double *t);
 

@@ -205,6 +205,7 @@ __global__ void __launch_bounds__(kBlock) k_sum_density(DenArgs a) {
 int export_pairs(simp_ctx *c, int32_t *nip, int32_t *p_i, int32_t *p_j, double *r_ij,
                  double *hsml_ij, int32_t cap, int32_t *bnip, int32_t *bp_i, int32_t *bp_j,
                  double *br_ij, int32_t bcap) {
+    if (const int rc = complete_pending(c)) return rc;   // (the search resets the statistics)
     cudaStream_t st = c->stream;
     const int n = c->n;
     ExpArgs a{};

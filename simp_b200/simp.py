@@ -209,6 +209,12 @@ class Simp:
     def predictor_corrector(self):
         return self.time_integration(1)
 
+    def step_enqueue(self, nsteps: int):
+        """nsteps iterations without waiting for them (simp_gpu_step without
+        outputs): the next get_state returns their status with the state, the
+        next time_integration, single_step or nnps waits for them first."""
+        self._chk(self.lib.simp_gpu_step(self.h, int(nsteps), None, None))
+
 
 class Batch:
     """A batch of resident basins stepped together (one launch per kernel per
