@@ -41,6 +41,17 @@ __global__ void k_deinterleave(int n, const double *__restrict__ in, double *__r
     b[i] = in[2 * i + 1];
 }
 
+// Fields of a single basin into the caller's order; a null source is skipped.
+__global__ void k_pack_fields(int n, int id_base, const int *__restrict__ id, const double *__restrict__ a,
+                              const double *__restrict__ b, double *__restrict__ out_a, double *__restrict__ out_b) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int o = id[k] - id_base;
+    if (!SIMP_IN_RANGE(o, 0, n, SITE_SORT)) return;
+    if (a) out_a[o] = a[k];
+    if (b) out_b[o] = b[k];
+}
+
 // New particles [off, off + n): ids, instance, sort positions, m / rho, and
 // the summation density's kept kernel_zero (initialize.f90:60).
 __global__ void k_init_new(int n, int off, int id_base, int slot, int *id, int *pinst, State s, double *xr,
@@ -334,7 +345,8 @@ void free_all(simp_ctx *c) {
                     c->pair_j, c->pair_count, c->nbr_tmp, c->s0.hsf,
                     c->inst_dev, c->row_map, c->chunk_cnt, c->chunk_off, c->chunks, c->s0.xy, c->s0.vxy,
                     c->s0.pf, c->s0.mm, c->s0.hmm, c->s1.xy, c->s1.vxy, c->s1.pf, c->s1.mm, c->s1.hmm,
-                    c->tau_a, c->tau_b, c->tau_q, c->pair_dw, c->drhodt, c->k0, c->red_dev, c->reg};
+                    c->tau_a, c->tau_b, c->tau_q, c->pair_dw, c->drhodt, c->k0, c->red_dev, c->reg,
+                    c->early_stage};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->sc_host) cudaFreeHost(c->sc_host);
@@ -344,6 +356,8 @@ void free_all(simp_ctx *c) {
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : c->sort_ev)
         if (e) cudaEventDestroy(e);
+    if (c->ev_graph) cudaEventDestroy(c->ev_graph);
+    if (c->side) cudaStreamDestroy(c->side);
     if (c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -988,6 +1002,11 @@ int create(const simp_params *params, int32_t maxn, int32_t maxnb, int32_t max_i
     }
     TRY(dalloc(c, &c->diag, 9 * M));
     TRY(dalloc(c, &c->rates, 4 * M));
+    if (c->max_inst == 1) {
+        SIMP_CUDA(c, cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+        SIMP_CUDA(c, cudaEventCreateWithFlags(&c->ev_graph, cudaEventDisableTiming));
+        TRY(dalloc(c, &c->early_stage, 2 * M));
+    }
     if (c->prm.xsph_regularization || c->prm.artificial_visc) TRY(dalloc(c, &c->reg, 4 * M));
     TRY(dalloc(c, &c->cell, M));
     TRY(dalloc(c, &c->id, M));
@@ -1085,7 +1104,7 @@ int check_normals(simp_ctx *c) {
 
 // Device bytes per unit of maxn of a context with these parameters (the
 // allocations of create() below, with room for its cell lists).
-double bytes_per_particle(const simp_params &p) {
+double bytes_per_particle(const simp_params &p, bool single_basin) {
     const bool mixed = p.precision == SIMP_PREC_MIXED;
     double b = 26 * 8.0;                                      // FP64 state sets and per-RHS fields
     if (p.mass_from_area && p.sle != 2) b += 8.0;             // half-step mass
@@ -1101,6 +1120,7 @@ double bytes_per_particle(const simp_params &p) {
     if (p.den_alg == 1) b += 8.0;                             // kept kernel_zero
     b += 4 * 4.0 + 16 * 8.0 + 5 * 4.0 + 4.0;                  // sort keys, scratch
     b += 16.0 / kMinTileThreads + 48.0;                       // chunks, cell lists (worst case)
+    if (single_basin) b += 2 * 8.0;                           // read-back stage of the fixed fields
     return b;
 }
 
@@ -1145,6 +1165,7 @@ int step_enqueue(simp_ctx *c, int nsteps) {
                 c->prof_ms[simp_ctx::kProfKernels] += ms;
             }
         }
+        if (c->ev_graph) SIMP_CUDA(c, cudaEventRecord(c->ev_graph, s));
         cudaError_t e = cudaGraphLaunch(c->step_graph, s);
         if (e != cudaSuccess) return simp_cuda_check(c, e, "cudaGraphLaunch");
         c->launches += c->graph_kernels;
@@ -1499,7 +1520,31 @@ int32_t simp_gpu_get_state(simp_ctx *c, double *x, double *vx, double *mass, dou
     if (!c) return SIMP_ERR_BADARG;
     if (!c->have_state || !c->insts[0].active) return simp_fail(c, SIMP_ERR_STATE, "get_state before set_state");
     SIMP_RANGE("simp_gpu_get_state");
-    TRY(get_instance_state(c, 0, x, vx, mass, rho, hsml, A, h, nullptr, true));
+    // after steps enqueued without outputs: the fields no step writes are
+    // read back while the steps run (the side stream starts at the last
+    // step's graph, after any re-sort), the others after them
+    const bool mass_fixed = !c->mass1, hsml_fixed = c->prm.sle == 0;
+    double *early_m = (c->pending_check && c->side && mass && mass_fixed) ? mass : nullptr;
+    double *early_h = (c->pending_check && c->side && hsml && hsml_fixed) ? hsml : nullptr;
+    if (early_m || early_h) {
+        const int n = c->n;
+        const size_t N = (size_t)n;
+        SIMP_CUDA(c, cudaStreamWaitEvent(c->side, c->ev_graph, 0));
+        k_pack_fields<<<nblk(n, kB), kB, 0, c->side>>>(n, c->insts[0].id_base, c->id, early_m ? c->s0.m : nullptr,
+                                                        early_h ? c->s0.hs : nullptr, c->early_stage,
+                                                        c->early_stage + N);
+        c->launches += 1;
+        SIMP_CUDA(c, cudaGetLastError());
+        if (early_m)
+            SIMP_CUDA(c, cudaMemcpyAsync(early_m, c->early_stage, sizeof(double) * N, cudaMemcpyDeviceToHost, c->side));
+        if (early_h)
+            SIMP_CUDA(c, cudaMemcpyAsync(early_h, c->early_stage + N, sizeof(double) * N, cudaMemcpyDeviceToHost,
+                                         c->side));
+    }
+    const int rc = get_instance_state(c, 0, x, vx, early_m ? nullptr : mass, rho, early_h ? nullptr : hsml, A, h,
+                                      nullptr, true);
+    if (early_m || early_h) SIMP_CUDA(c, cudaStreamSynchronize(c->side));
+    TRY(rc);
     if (dt) *dt = c->sc_host->dt;
     if (current_time) *current_time = c->sc_host->t;
     if (c->pending_check) {   // the status of steps enqueued without outputs

@@ -46,6 +46,12 @@ struct simp_ctx {
     std::string err;
     cudaStream_t stream = nullptr;
     int device = 0;
+    // single-basin contexts: get_state after steps enqueued without outputs
+    // reads the fields no step writes (mass without mass evolution, hsml
+    // when fixed) on a side stream while those steps run
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_graph = nullptr;   // recorded before each step graph launch
+    double *early_stage = nullptr;    // 2 maxn: those fields in the caller's order
 
     // instances
     std::vector<InstHost> insts;   // max_inst slots
@@ -198,7 +204,7 @@ int tiled_configure(simp_ctx *c);
 size_t tiled_smem_bytes(int precision, int pass, int cap, int threads);
 
 // abi.cu: device bytes per particle of capacity
-double bytes_per_particle(const simp_params &p);
+double bytes_per_particle(const simp_params &p, bool single_basin = false);
 
 // abi.cu: the step driver split for callers that overlap contexts
 int step_enqueue(simp_ctx *c, int nsteps);

@@ -240,7 +240,7 @@ int32_t simp_server_create(const simp_params *params, const simp_server_config *
         const double spot_n = 2.0 * cfg->max_request_particles;
         s->maxn_spot = (int)spot_n;
         s->maxnb_spot = std::max(1, s->maxn_spot / kWallsPerParticleDiv);
-        budget -= spot_n * (simp::bytes_per_particle(p64) + kBytesPerWall / kWallsPerParticleDiv);
+        budget -= spot_n * (simp::bytes_per_particle(p64, true) + kBytesPerWall / kWallsPerParticleDiv);
     }
     const double cap = std::floor(budget / per);
     if (cap < cfg->max_request_particles)

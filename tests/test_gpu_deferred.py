@@ -22,9 +22,16 @@ def _basin():
     return b
 
 
-def test_enqueued_steps_same_bits_as_waited(gpu_lib):
+@pytest.mark.parametrize("switches", [{}, {"mass_from_area": 1}, {"sle": 2}, {"sle": 1, "int_algorithm": 1}])
+def test_enqueued_steps_same_bits_as_waited(gpu_lib, switches):
+    """With fixed hsml and mass, get_state reads those two fields while the
+    step runs, from after its re-sort (every 16 steps); with either evolving
+    it reads them after the step."""
     b = _basin()
-    a, e = Simp.from_basin(b), Simp.from_basin(b)
+    prm = b.params.copy()
+    for k, v in switches.items():
+        setattr(prm, k, v)
+    a, e = Simp.from_basin(b, prm), Simp.from_basin(b, prm)
     for _ in range(20):                      # (a re-sort comes at step 16)
         t, dt = a.time_integration(1)
         e.step_enqueue(1)
