@@ -482,16 +482,24 @@ def run_e2e(sim, b, stream, nsteps, dist):
     state_ptrs = [P(host[k]) for k in ("x", "vx", "mass", "rho", "hsml", "A", "h")]
     wall_ptrs = [P(xb), P(massb)]
     ptc, pdtc = ctypes.byref(tc), ctypes.byref(dtc)
+    calls = {"set_state": [], "step": [], "get_state": []}
+    clock = time.perf_counter
     for _ in range(nsteps):
+        c0 = clock()
         rc = lib.simp_gpu_set_state(sim.h, n, *state_ptrs, nb, *wall_ptrs, float(dt), float(t_now))
         assert rc == 0, lib.simp_gpu_last_error(sim.h)
+        c1 = clock()
         # (no outputs: the step is enqueued and get_state, which returns
         # time and dt, reads its status in the same wait)
         rc = lib.simp_gpu_step(sim.h, 1, None, None)
         assert rc == 0, lib.simp_gpu_last_error(sim.h)
+        c2 = clock()
         rc = lib.simp_gpu_get_state(sim.h, *state_ptrs, pdtc, ptc)
         assert rc == 0, lib.simp_gpu_last_error(sim.h)
+        c3 = clock()
         t_now, dt = tc.value, dtc.value
+        for k, v in zip(calls, (c1 - c0, c2 - c1, c3 - c2)):
+            calls[k].append(v)
     e1.record(stream)
     torch.cuda.synchronize()
     ms = job_time_ms(dist, e0.elapsed_time(e1))
@@ -501,6 +509,8 @@ def run_e2e(sim, b, stream, nsteps, dist):
     return {"value": world * n * nsteps / (ms / 1e3), "unit": METRIC, "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "steps": nsteps,
             "path": "simp_gpu_set_state (pinned host) + simp_gpu_step(1, no outputs) + simp_gpu_get_state (pinned host, with time and dt)",
+            "call_ms": {k: 1e3 * float(np.median(v)) for k, v in calls.items()},
+            "call_timing": "host clock around each call, median over the steps",
             "link": link_copy_rates(stream, n * (2 * 16 + 5 * 8))}
 
 
