@@ -52,6 +52,18 @@ __global__ void k_pack_fields(int n, int id_base, const int *__restrict__ id, co
     if (b) out_b[o] = b[k];
 }
 
+// Two fields of a single basin into one interleaved array in the caller's
+// order (x(2,n), vx(2,n)).
+__global__ void k_pack_pair(int n, int id_base, const int *__restrict__ id, const double *__restrict__ a,
+                            const double *__restrict__ b, double *__restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int o = id[k] - id_base;
+    if (!SIMP_IN_RANGE(o, 0, n, SITE_SORT)) return;
+    out[2 * (size_t)o] = a[k];
+    out[2 * (size_t)o + 1] = b[k];
+}
+
 // New particles [off, off + n): ids, instance, sort positions, m / rho, and
 // the summation density's kept kernel_zero (initialize.f90:60).
 __global__ void k_init_new(int n, int off, int id_base, int slot, int *id, int *pinst, State s, double *xr,
@@ -169,63 +181,91 @@ __global__ void k_grow_xabs(Scalars *sc, double xa) {
 // the particles' current places in cell order, so the sort, the cell lists
 // and the Verlet lists stay, and the displacement bounds grow as after a
 // step.  stage = [x,y interleaved | vx,vy interleaved | mass | rho | hsml |
-// A | h] in the caller's order.  Per block: [0] invalid values, [1] changed
-// hsml, [2] max squared displacement since the sort, [3] since the lists
-// were built, [4] max |coordinate|, [5] max hsml, [6] -min hsml.
-__global__ void __launch_bounds__(256) k_continue_state(int n, const int *__restrict__ id,
+// A | h] in the caller's order, uploaded in the groups below; each group's
+// kernel runs as soon as its part has landed, while the next part is
+// copied.  Per block, each group reduces its own slots of `part`:
+// [0] non-finite positions, [1] changed hsml, [2] max squared displacement
+// since the sort, [3] since the lists were built, [4] max |coordinate|
+// (positions); [5] max hsml, [6] -min hsml (hsml); [7] other invalid
+// values (velocities, then mass and rho, then A and h, adding up in stream
+// order).
+enum ContGroup { CG_POS, CG_VEL, CG_MASS, CG_HSML, CG_AH, kContGroups };
+
+template <int G>
+__global__ void __launch_bounds__(256) k_continue_group(int n, const int *__restrict__ id,
                                                        const double *__restrict__ stage, State s,
                                                        const double *__restrict__ xr,
                                                        const double *__restrict__ yr, NbrList nl, double *part) {
-    double v[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, -INFINITY};
+    double v[kRedVals] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, -INFINITY, 0.0};
     const size_t N = (size_t)n;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const size_t o = (size_t)id[i];
-        const double x = stage[2 * o], y = stage[2 * o + 1];
-        const double vx = stage[2 * N + 2 * o], vy = stage[2 * N + 2 * o + 1];
-        const double m = stage[4 * N + o], rho = stage[5 * N + o], hs = stage[6 * N + o];
-        const double A = stage[7 * N + o], h = stage[8 * N + o];
-        const bool ok = isfinite(x) && isfinite(y) && isfinite(vx) && isfinite(vy) && isfinite(m) &&
-                        isfinite(A) && isfinite(rho) && isfinite(h) && rho > 0.0 && h > 0.0;
-        if (!ok) v[0] += 1.0;
-        if (!(hs == s.hs[i])) v[1] += 1.0;
-        if (ok) {
-            const double dxr = x - xr[i], dyr = y - yr[i];
-            v[2] = fmax(v[2], dxr * dxr + dyr * dyr);
-            if (nl.count[i] >= 0) {
-                const double dxl = x - nl.xl[i], dyl = y - nl.yl[i];
-                v[3] = fmax(v[3], dxl * dxl + dyl * dyl);
+        if (G == CG_POS) {
+            const double x = stage[2 * o], y = stage[2 * o + 1];
+            if (isfinite(x) && isfinite(y)) {
+                const double dxr = x - xr[i], dyr = y - yr[i];
+                v[2] = fmax(v[2], dxr * dxr + dyr * dyr);
+                if (nl.count[i] >= 0) {
+                    const double dxl = x - nl.xl[i], dyl = y - nl.yl[i];
+                    v[3] = fmax(v[3], dxl * dxl + dyl * dyl);
+                }
+                v[4] = fmax(v[4], fmax(fabs(x), fabs(y)));
+            } else {
+                v[0] += 1.0;
             }
-            v[4] = fmax(v[4], fmax(fabs(x), fabs(y)));
+            s.x[i] = x;
+            s.y[i] = y;
+            s.xy[i] = make_double2(x, y);
+            s.pf[i] = make_float4((float)x, (float)y, s.hsf[i], 0.0f);
+        } else if (G == CG_VEL) {
+            const double vx = stage[2 * N + 2 * o], vy = stage[2 * N + 2 * o + 1];
+            if (!(isfinite(vx) && isfinite(vy))) v[7] += 1.0;
+            s.vx[i] = vx;
+            s.vy[i] = vy;
+            s.vxy[i] = make_double2(vx, vy);
+        } else if (G == CG_MASS) {
+            const double m = stage[4 * N + o], rho = stage[5 * N + o];
+            if (!(isfinite(m) && isfinite(rho) && rho > 0.0)) v[7] += 1.0;
+            const double mor = m / rho;
+            s.m[i] = m;
+            s.rho[i] = rho;
+            s.mor[i] = mor;
+            if (s.hmm) s.hmm[i] = make_float4(s.hsf[i], (float)m, (float)mor, 0.0f);
+            else s.mm[i] = make_double2(m, mor);
+        } else if (G == CG_HSML) {
+            const double hs = stage[6 * N + o];
+            if (!(hs == s.hs[i])) v[1] += 1.0;
+            v[5] = fmax(v[5], hs);
+            v[6] = fmax(v[6], -hs);
+        } else {
+            const double A = stage[7 * N + o], h = stage[8 * N + o];
+            if (!(isfinite(A) && isfinite(h) && h > 0.0)) v[7] += 1.0;
+            s.A[i] = A;
+            s.h[i] = h;
         }
-        v[5] = fmax(v[5], hs);
-        v[6] = fmax(v[6], -hs);
-        s.x[i] = x;
-        s.y[i] = y;
-        s.vx[i] = vx;
-        s.vy[i] = vy;
-        s.m[i] = m;
-        s.rho[i] = rho;
-        s.mor[i] = m / rho;
-        s.A[i] = A;
-        s.h[i] = h;
-        refresh_views(s, i);
     }
-    __shared__ double red[7][8];
+    // the slots of this group: a bit mask over [0, kRedVals)
+    constexpr unsigned own = G == CG_POS ? 0x1du : G == CG_HSML ? 0x62u : 0x80u;
+    __shared__ double red[kRedVals][8];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
-    for (int q = 0; q < 7; ++q) {
-        for (int o = 16; o > 0; o >>= 1) {
-            const double t = __shfl_xor_sync(0xffffffffu, v[q], o);
-            v[q] = (q < 2) ? v[q] + t : fmax(v[q], t);
+    for (int q = 0; q < kRedVals; ++q) {
+        if (!((own >> q) & 1u)) continue;
+        const bool sum = q == 0 || q == 1 || q == 7;
+        for (int d = 16; d > 0; d >>= 1) {
+            const double t = __shfl_xor_sync(0xffffffffu, v[q], d);
+            v[q] = sum ? v[q] + t : fmax(v[q], t);
         }
         if (lane == 0) red[q][w] = v[q];
     }
     __syncthreads();
-    if (threadIdx.x < 7) {
+    if (threadIdx.x < kRedVals && ((own >> threadIdx.x) & 1u)) {
         const int q = threadIdx.x;
+        const bool sum = q == 0 || q == 1 || q == 7;
         double r = red[q][0];
-        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) r = (q < 2) ? r + red[q][k] : fmax(r, red[q][k]);
-        part[blockIdx.x * kRedVals + q] = r;
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) r = sum ? r + red[q][k] : fmax(r, red[q][k]);
+        double &slot = part[blockIdx.x * kRedVals + q];
+        slot = (q == 7 && G != CG_VEL) ? slot + r : r;   // (the velocity group writes slot 7 first)
     }
 }
 
@@ -357,6 +397,8 @@ void free_all(simp_ctx *c) {
     for (cudaEvent_t e : c->sort_ev)
         if (e) cudaEventDestroy(e);
     if (c->ev_graph) cudaEventDestroy(c->ev_graph);
+    for (cudaEvent_t e : c->ev_up)
+        if (e) cudaEventDestroy(e);
     if (c->side) cudaStreamDestroy(c->side);
     if (c->stream) cudaStreamDestroy(c->stream);
 }
@@ -773,7 +815,7 @@ int download1(simp_ctx *c, const double *a, double *h1) {
 }
 
 int get_instance_state(simp_ctx *c, int slot, double *x, double *vx, double *mass, double *rho, double *hsml,
-                       double *A, double *h, double *t, bool with_scalars = false) {
+                       double *A, double *h, double *t) {
     const InstHost &ih = c->insts[slot];
     const int nk = ih.n;
     const size_t N = (size_t)nk;
@@ -790,8 +832,6 @@ int get_instance_state(simp_ctx *c, int slot, double *x, double *vx, double *mas
             SIMP_CUDA(c, cudaMemcpyAsync(o.dst, stage + o.off, sizeof(double) * o.len, cudaMemcpyDeviceToHost, s));
     Inst I{};
     SIMP_CUDA(c, cudaMemcpyAsync(&I, c->inst_dev + slot, sizeof(Inst), cudaMemcpyDeviceToHost, s));
-    // (the scalars in the same wait, for get_state)
-    if (with_scalars) SIMP_CUDA(c, cudaMemcpyAsync(c->sc_host, c->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, s));
     SIMP_CUDA(c, cudaStreamSynchronize(s));
     if (t) *t = I.t;
     return SIMP_OK;
@@ -1005,6 +1045,7 @@ int create(const simp_params *params, int32_t maxn, int32_t maxnb, int32_t max_i
     if (c->max_inst == 1) {
         SIMP_CUDA(c, cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
         SIMP_CUDA(c, cudaEventCreateWithFlags(&c->ev_graph, cudaEventDisableTiming));
+        for (cudaEvent_t &e : c->ev_up) SIMP_CUDA(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         TRY(dalloc(c, &c->early_stage, 2 * M));
     }
     if (c->prm.xsph_regularization || c->prm.artificial_visc) TRY(dalloc(c, &c->reg, 4 * M));
@@ -1214,7 +1255,7 @@ int batch_slot_state(simp_ctx *c, int slot, double *x, double *vx, double *mass,
 // set_state of a state that continues the resident basin: the same particle
 // count and walls, the same hsml, no particle farther than one cell from
 // where it was sorted, a finite resident state.  The values are written in
-// place (k_continue_state) and the sort, cell lists, Verlet lists and step
+// place (k_continue_group, per upload group) and the sort, cell lists, Verlet lists and step
 // graph stay.  Returns kFreshState, with the resident state overwritten or
 // not, when the state does not qualify; the caller then sets it up from
 // scratch.  Left out: Benz's kept drhodt (a fresh state zeroes it) and the
@@ -1233,13 +1274,6 @@ int continue_state(simp_ctx *c, int n, const double *x, const double *vx, const 
     cudaStream_t s = c->stream;
     const size_t N = (size_t)n;
     double *stage = c->tmp;
-    SIMP_CUDA(c, cudaMemcpyAsync(stage, x, sizeof(double) * 2 * N, cudaMemcpyHostToDevice, s));
-    SIMP_CUDA(c, cudaMemcpyAsync(stage + 2 * N, vx, sizeof(double) * 2 * N, cudaMemcpyHostToDevice, s));
-    SIMP_CUDA(c, cudaMemcpyAsync(stage + 4 * N, mass, sizeof(double) * N, cudaMemcpyHostToDevice, s));
-    SIMP_CUDA(c, cudaMemcpyAsync(stage + 5 * N, rho, sizeof(double) * N, cudaMemcpyHostToDevice, s));
-    SIMP_CUDA(c, cudaMemcpyAsync(stage + 6 * N, hsml, sizeof(double) * N, cudaMemcpyHostToDevice, s));
-    SIMP_CUDA(c, cudaMemcpyAsync(stage + 7 * N, A, sizeof(double) * N, cudaMemcpyHostToDevice, s));
-    SIMP_CUDA(c, cudaMemcpyAsync(stage + 8 * N, h, sizeof(double) * N, cudaMemcpyHostToDevice, s));
     const int rb = std::min(kRedBlocks, nblk(n, 256));
     NbrList nl;
     nl.nbr = c->nbr;
@@ -1247,18 +1281,40 @@ int continue_state(simp_ctx *c, int n, const double *x, const double *vx, const 
     nl.xl = c->xl;
     nl.yl = c->yl;
     nl.stride = c->maxn;
-    k_continue_state<<<rb, 256, 0, s>>>(n, c->id, stage, c->s0, c->xr, c->yr, nl, c->red_dev);
-    c->launches += 1;
+    // the upload on the side stream (after whatever the context stream has
+    // queued), each group's kernel on the context stream once its part is in
+    struct Part { const double *src; size_t off, len; int group; } parts[] = {
+        {x, 0, 2 * N, CG_POS}, {vx, 2 * N, 2 * N, CG_VEL}, {mass, 4 * N, N, -1}, {rho, 5 * N, N, CG_MASS},
+        {hsml, 6 * N, N, CG_HSML}, {A, 7 * N, N, -1}, {h, 8 * N, N, CG_AH}};
+    SIMP_CUDA(c, cudaEventRecord(c->ev_up[kContGroups], s));
+    SIMP_CUDA(c, cudaStreamWaitEvent(c->side, c->ev_up[kContGroups], 0));
+    for (const Part &p : parts) {
+        SIMP_CUDA(c, cudaMemcpyAsync(stage + p.off, p.src, sizeof(double) * p.len, cudaMemcpyHostToDevice, c->side));
+        if (p.group < 0) continue;
+        SIMP_CUDA(c, cudaEventRecord(c->ev_up[p.group], c->side));
+        SIMP_CUDA(c, cudaStreamWaitEvent(s, c->ev_up[p.group], 0));
+        switch (p.group) {
+            case CG_POS: k_continue_group<CG_POS><<<rb, 256, 0, s>>>(n, c->id, stage, c->s0, c->xr, c->yr, nl, c->red_dev); break;
+            case CG_VEL: k_continue_group<CG_VEL><<<rb, 256, 0, s>>>(n, c->id, stage, c->s0, c->xr, c->yr, nl, c->red_dev); break;
+            case CG_MASS: k_continue_group<CG_MASS><<<rb, 256, 0, s>>>(n, c->id, stage, c->s0, c->xr, c->yr, nl, c->red_dev); break;
+            case CG_HSML: k_continue_group<CG_HSML><<<rb, 256, 0, s>>>(n, c->id, stage, c->s0, c->xr, c->yr, nl, c->red_dev); break;
+            default: k_continue_group<CG_AH><<<rb, 256, 0, s>>>(n, c->id, stage, c->s0, c->xr, c->yr, nl, c->red_dev);
+        }
+        c->launches += 1;
+    }
     SIMP_CUDA(c, cudaGetLastError());
     SIMP_CUDA(c, cudaMemcpyAsync(c->red_host, c->red_dev, sizeof(double) * kRedVals * rb, cudaMemcpyDeviceToHost, s));
     SIMP_CUDA(c, cudaMemcpyAsync(c->sc_host, c->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, s));
     SIMP_CUDA(c, cudaStreamSynchronize(s));
+    // v: [0] invalid values, [1] changed hsml, [2] d2 since the sort, [3]
+    // since the lists, [4] max |coordinate|, [5] max hsml, [6] -min hsml
     double v[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, -INFINITY};
-    for (int b = 0; b < rb; ++b)
-        for (int q = 0; q < 7; ++q) {
-            const double u = c->red_host[b * kRedVals + q];
-            v[q] = (q < 2) ? v[q] + u : std::max(v[q], u);
-        }
+    for (int b = 0; b < rb; ++b) {
+        const double *u = c->red_host + (size_t)b * kRedVals;
+        v[0] += u[0] + u[7];
+        v[1] += u[1];
+        for (int q = 2; q < 7; ++q) v[q] = std::max(v[q], u[q]);
+    }
     const Scalars &sc = *c->sc_host;
     if (v[0] > 0.0 || v[1] > 0.0 || sc.flags != 0 || !(v[2] <= ih.I.cs * ih.I.cs)) return kFreshState;
     // a fresh state would take max_hsml from its own largest hsml: the run
@@ -1541,10 +1597,44 @@ int32_t simp_gpu_get_state(simp_ctx *c, double *x, double *vx, double *mass, dou
             SIMP_CUDA(c, cudaMemcpyAsync(early_h, c->early_stage + N, sizeof(double) * N, cudaMemcpyDeviceToHost,
                                          c->side));
     }
-    const int rc = get_instance_state(c, 0, x, vx, early_m ? nullptr : mass, rho, early_h ? nullptr : hsml, A, h,
-                                      nullptr, true);
-    if (early_m || early_h) SIMP_CUDA(c, cudaStreamSynchronize(c->side));
-    TRY(rc);
+    // the rest in groups: each group's reorder on the context stream, its
+    // copy on the side stream while the next group is reordered
+    const int n = c->n, id_base = c->insts[0].id_base;
+    const size_t N = (size_t)n;
+    cudaStream_t s = c->stream;
+    double *stage = c->tmp;   // [x,y | vx,vy | mass | rho | hsml | A | h], caller's order
+    const double *m_src = (mass && !early_m) ? c->s0.m : nullptr, *hs_src = (hsml && !early_h) ? c->s0.hs : nullptr;
+    struct Out { double *dst; size_t off, len; };
+    struct Group { Out a, b; } groups[5] = {
+        {{x, 0, 2 * N}, {nullptr, 0, 0}},
+        {{vx, 2 * N, 2 * N}, {nullptr, 0, 0}},
+        {{m_src ? mass : nullptr, 4 * N, N}, {rho, 5 * N, N}},
+        {{hs_src ? hsml : nullptr, 6 * N, N}, {A, 7 * N, N}},
+        {{h, 8 * N, N}, {nullptr, 0, 0}}};
+    for (int g = 0; g < 5; ++g) {
+        const Group &G = groups[g];
+        if (!G.a.dst && !G.b.dst) continue;
+        if (g == 0) {
+            k_pack_pair<<<nblk(n, kB), kB, 0, s>>>(n, id_base, c->id, c->s0.x, c->s0.y, stage);
+        } else if (g == 1) {
+            k_pack_pair<<<nblk(n, kB), kB, 0, s>>>(n, id_base, c->id, c->s0.vx, c->s0.vy, stage + 2 * N);
+        } else {
+            const double *sa = g == 2 ? m_src : g == 3 ? hs_src : c->s0.h;
+            const double *sb = g == 2 ? (rho ? c->s0.rho : nullptr) : g == 3 ? (A ? c->s0.A : nullptr) : nullptr;
+            k_pack_fields<<<nblk(n, kB), kB, 0, s>>>(n, id_base, c->id, sa, sb, stage + G.a.off, stage + G.b.off);
+        }
+        c->launches += 1;
+        SIMP_CUDA(c, cudaGetLastError());
+        SIMP_CUDA(c, cudaEventRecord(c->ev_up[g], s));
+        SIMP_CUDA(c, cudaStreamWaitEvent(c->side, c->ev_up[g], 0));
+        for (const Out &o : {G.a, G.b})
+            if (o.dst)
+                SIMP_CUDA(c, cudaMemcpyAsync(o.dst, stage + o.off, sizeof(double) * o.len, cudaMemcpyDeviceToHost,
+                                             c->side));
+    }
+    SIMP_CUDA(c, cudaMemcpyAsync(c->sc_host, c->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, s));
+    SIMP_CUDA(c, cudaStreamSynchronize(s));
+    SIMP_CUDA(c, cudaStreamSynchronize(c->side));
     if (dt) *dt = c->sc_host->dt;
     if (current_time) *current_time = c->sc_host->t;
     if (c->pending_check) {   // the status of steps enqueued without outputs

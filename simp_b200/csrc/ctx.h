@@ -51,6 +51,7 @@ struct simp_ctx {
     // when fixed) on a side stream while those steps run
     cudaStream_t side = nullptr;
     cudaEvent_t ev_graph = nullptr;   // recorded before each step graph launch
+    cudaEvent_t ev_up[6] = {};        // a continued set_state's upload groups, and its start
     double *early_stage = nullptr;    // 2 maxn: those fields in the caller's order
 
     // instances

@@ -10,7 +10,8 @@ current places and keeps the sort, the cell lists and the Verlet lists:
 - anything else (other walls, other hsml, particles moved farther than a
   cell) is set up from scratch, bitwise as in a new context.
 Whether a call continued is read from the kernel count: a continued
-set_state launches two kernels, a fresh one many more.
+set_state launches six kernels (one per part of the upload, which run
+while the next part is copied, and the bounds), a fresh one many more.
 """
 import numpy as np
 import pytest
@@ -23,6 +24,7 @@ from simp_b200.simp import Simp
 pytestmark = pytest.mark.gpu
 
 KEYS = ("x", "vx", "mass", "rho", "hsml", "A", "h")
+CONTINUED = 6   # kernels of a continued set_state
 
 
 def _launches(g):
@@ -62,7 +64,7 @@ def test_handing_back_the_state_is_the_device_resident_run(gpu_lib, switches):
     for _ in range(24):
         st = host.get_state()
         launched, _ = _set(host, b, st)
-        assert launched == 2
+        assert launched == CONTINUED
         host.time_integration(1)
     a, c = resident.get_state(), host.get_state()
     for k in KEYS + ("dt", "current_time"):
@@ -82,7 +84,7 @@ def test_changed_state_matches_oracle_pairs_and_fresh_rates(gpu_lib, oracle_mod)
     vx = 1.1 * st["vx"] + rng.normal(0.0, 0.05, st["vx"].shape)
     h = st["h"] * rng.uniform(0.99, 1.01, st["h"].shape)
     launched, v = _set(g, b, st, x=x, vx=vx, h=h, rho=900.0 * h)
-    assert launched == 2
+    assert launched == CONTINUED
     fresh = Simp(b.params, b.n, b.nb)
     fresh.set_state(v["x"], v["vx"], v["mass"], v["rho"], v["hsml"], v["A"], v["h"], b.xb, b.massb,
                     st["dt"], st["current_time"])
@@ -162,7 +164,7 @@ def test_host_integrator_over_gpu_single_step(gpu_lib):
 
     def rates(x, v, h, A):
         launched, _ = _set(g, b, dict(st, x=x, vx=v, h=h, A=A, rho=rho_ice * h, dt=dt, current_time=t))
-        assert launched == 2
+        assert launched == CONTINUED
         return g.single_step(t)
 
     for _ in range(10):

@@ -95,3 +95,29 @@ def test_new_state_drops_enqueued_status(gpu_lib):
     g.set_state(b.x, b.vx, b.mass, b.rho, b.hsml, b.A, b.h, b.xb, b.massb, prm.dt, 0.0)
     s = g.get_state()
     assert np.array_equal(s["x"], b.x) and s["current_time"] == 0.0
+
+
+@pytest.mark.parametrize("fields", [("x",), ("h",), ("mass", "A"), ("vx", "hsml", "rho")])
+def test_get_state_some_fields(gpu_lib, fields):
+    """get_state with only some outputs (the others NULL), after an enqueued
+    step and after a waited one: the requested fields as a full read gives
+    them, the caller's other arrays untouched."""
+    from simp_b200 import _lib
+    b = _basin()
+    g, ref = Simp.from_basin(b), Simp.from_basin(b)
+    names = ("x", "vx", "mass", "rho", "hsml", "A", "h")
+    for enqueued in (True, False):
+        if enqueued:
+            g.step_enqueue(3)
+        else:
+            g.time_integration(3)
+        ref.time_integration(3)
+        want = ref.get_state()
+        out = {k: np.full_like(want[k], -7.0) for k in names}
+        ptrs = [_lib.dptr(out[k]) if k in fields else None for k in names]
+        assert g.lib.simp_gpu_get_state(g.h, *ptrs, None, None) == 0
+        for k in names:
+            if k in fields:
+                assert np.array_equal(out[k], want[k]), k
+            else:
+                assert np.all(out[k] == -7.0), k
