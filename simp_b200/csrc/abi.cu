@@ -392,6 +392,7 @@ void free_all(simp_ctx *c) {
     if (c->sc_host) cudaFreeHost(c->sc_host);
     if (c->red_host) cudaFreeHost(c->red_host);
     if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+    if (c->sort_graph) cudaGraphExecDestroy(c->sort_graph);
     for (cudaEvent_t e : c->prof_ev)
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : c->sort_ev)
@@ -1167,6 +1168,54 @@ double bytes_per_particle(const simp_params &p, bool single_basin) {
 
 // Enqueues nsteps steps of every basin of the context on its stream without
 // waiting for them (profiling mode waits step by step).
+// A single basin's scheduled re-sort, replayed from a captured graph (one
+// launch where the re-sort is some fifteen).  Its kernels capture the
+// particle and cell counts, whether the Verlet lists are renamed, and the
+// cell arrays, which a new layout can reallocate: a change of any of those
+// captures it again.  Rebuild's host side for this case is that it counts
+// one more re-sort (a single basin keeps all its particles, and the lists
+// stay as valid as they were).
+int sort_replayed(simp_ctx *c, const DueMask &due) {
+    simp_ctx::SortKey k;
+    k.n = c->n;
+    k.total_cells = c->total_cells;
+    k.keep_lists = c->lists_valid;
+    k.cell_start = c->cell_start;
+    k.scan_tmp = c->scan_tmp;
+    if (!c->sort_graph || !(k == c->sort_key)) {
+        if (c->sort_graph) cudaGraphExecDestroy(c->sort_graph);
+        c->sort_graph = nullptr;
+        const long long l0 = c->launches, r0 = c->rebuilds;
+        const int n0 = c->n;
+        const bool lv0 = c->lists_valid;
+        cudaGraph_t g = nullptr;
+        SIMP_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = rebuild(c, due, c->n, false);
+        const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        const long long kernels = c->launches - l0;
+        c->launches = l0;   // (the launch below counts them)
+        c->rebuilds = r0;
+        c->n = n0;
+        c->lists_valid = lv0;
+        if (rc != SIMP_OK || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return rc != SIMP_OK ? rc : simp_cuda_check(c, e, "re-sort capture");
+        }
+        const cudaError_t ei = cudaGraphInstantiate(&c->sort_graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) {
+            c->sort_graph = nullptr;
+            return simp_cuda_check(c, ei, "cudaGraphInstantiate (re-sort)");
+        }
+        c->sort_kernels = kernels;
+        c->sort_key = k;
+    }
+    SIMP_CUDA(c, cudaGraphLaunch(c->sort_graph, c->stream));
+    c->launches += c->sort_kernels;
+    c->rebuilds += 1;
+    return SIMP_OK;
+}
+
 int step_enqueue(simp_ctx *c, int nsteps) {
     if (!c->have_state) return simp_fail(c, SIMP_ERR_STATE, "step before set_state");
     TRY(complete_pending(c));   // (this step resets the statistics those steps left)
@@ -1197,6 +1246,7 @@ int step_enqueue(simp_ctx *c, int nsteps) {
             if (c->graph_profiled) SIMP_CUDA(c, cudaEventRecord(c->sort_ev[0], s));
             TRY(maybe_regrid(c, &regridded));   // hsml grew past the grid (sle = 2)
             if (regridded) TRY(ensure_graph(c, c->keep_diag));
+            else if (c->max_inst == 1 && c->pass_impl != SIMP_PASSES_TILED) TRY(sort_replayed(c, due));
             else TRY(rebuild(c, due, c->n, false));
             if (c->graph_profiled) {
                 SIMP_CUDA(c, cudaEventRecord(c->sort_ev[1], s));

@@ -145,6 +145,19 @@ struct simp_ctx {
     bool graph_diag = false;
     bool graph_profiled = false;
     long long graph_kernels = 0;   // kernels per replay
+    // re-sort graph of a single basin: the kernels of one scheduled re-sort,
+    // captured once and replayed while what they capture stays the same
+    cudaGraphExec_t sort_graph = nullptr;
+    struct SortKey {
+        int n = -1, total_cells = -1;
+        bool keep_lists = false;
+        const void *cell_start = nullptr, *scan_tmp = nullptr;
+        bool operator==(const SortKey &o) const {
+            return n == o.n && total_cells == o.total_cells && keep_lists == o.keep_lists &&
+                   cell_start == o.cell_start && scan_tmp == o.scan_tmp;
+        }
+    } sort_key;
+    long long sort_kernels = 0;    // kernels per re-sort replay
     long long launches = 0;        // kernels launched by this context
     // per-kernel timing (events recorded inside the step graph)
     // (entry kProfKernels of prof_ms: the re-sorts between steps)
