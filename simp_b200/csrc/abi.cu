@@ -199,6 +199,7 @@ __global__ void __launch_bounds__(256) k_continue_group(int n, const int *__rest
     double v[kRedVals] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, -INFINITY, 0.0};
     const size_t N = (size_t)n;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (!SIMP_IN_RANGE(id[i], 0, n, SITE_SORT)) continue;
         const size_t o = (size_t)id[i];
         if (G == CG_POS) {
             const double x = stage[2 * o], y = stage[2 * o + 1];
