@@ -167,3 +167,24 @@ def test_kept_kernel_zero_through_resorts(gpu_lib, oracle_mod):
         e = rel_l2(sg[k], so[k])
         assert e < 1e-8, (k, e)
     g.close()
+
+
+def test_sum_density_step_at_headline_size(gpu_lib, oracle_mod):
+    """The headline basin (262,144 particles) with the summation density in
+    the step: 3 predictor-corrector steps against the oracle.  A particle
+    that is p_i of no pair (the corner farthest up and right, for one) has
+    no self term, as in the reference."""
+    b = basins.cfg2()
+    b.vx = smooth_velocity(b.x, b.L, amp=0.3, seed=43)
+    prm = _prm(b, den_alg=1)
+    g = Simp.from_basin(b, prm)
+    o = _oracle(oracle_mod, b, prm)
+    g.time_integration(3)
+    o.step(3)
+    sg, so = g.get_state(), o.get_state()
+    for k in ("x", "vx", "h", "rho"):
+        ref = b.x if k == "x" else 0.0
+        e = rel_l2(sg[k] - ref, so[k] - ref)
+        assert e < TOL_STEPS, (k, e)
+    assert rel_l2(sg["rho"], b.rho) > 1e-6
+    g.close()
