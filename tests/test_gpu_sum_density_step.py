@@ -176,6 +176,9 @@ def test_sum_density_step_at_headline_size(gpu_lib, oracle_mod):
     no self term, as in the reference."""
     b = basins.cfg2()
     b.vx = smooth_velocity(b.x, b.L, amp=0.3, seed=43)
+    # (a thickness gradient: the sum of a uniform density returns it exactly)
+    b.h = b.h * np.linspace(0.9, 1.1, b.n)
+    b.rho = b.h * 900.0
     prm = _prm(b, den_alg=1)
     g = Simp.from_basin(b, prm)
     o = _oracle(oracle_mod, b, prm)
