@@ -257,13 +257,15 @@ struct Nb;
 template <>
 struct Nb<double> {
     static __device__ __forceinline__ double h(const State &s, int j) { return s.hs[j]; }
-    static __device__ __forceinline__ KinNb<double> kin(const State &s, int j) {
+    // hu: the basin's hsml where every particle has the same (then hsml is
+    // not gathered), else negative
+    static __device__ __forceinline__ KinNb<double> kin(const State &s, int j, double hu) {
         const double2 q = __ldg(&s.mm[j]);
-        return {__ldg(&s.hs[j]), q.x, q.y};
+        return {hu > 0.0 ? hu : __ldg(&s.hs[j]), q.x, q.y};
     }
-    static __device__ __forceinline__ StressNb<double> stress(const State &s, const TauRec &t, int j) {
+    static __device__ __forceinline__ StressNb<double> stress(const State &s, const TauRec &t, int j, double hu) {
         const double2 a = __ldg(&t.ta[j]), b = __ldg(&t.tb[j]);
-        return {__ldg(&s.hs[j]), b.y, a.x, a.y, b.x};
+        return {hu > 0.0 ? hu : __ldg(&s.hs[j]), b.y, a.x, a.y, b.x};
     }
     static __device__ __forceinline__ StressNb<double> stress_rec(const TauRec &t, int j) {
         const double2 a = __ldg(&t.ta[j]), b = __ldg(&t.tb[j]);
@@ -273,13 +275,13 @@ struct Nb<double> {
 template <>
 struct Nb<float> {
     static __device__ __forceinline__ float h(const State &s, int j) { return s.hsf[j]; }
-    static __device__ __forceinline__ KinNb<float> kin(const State &s, int j) {
-        const float4 q = __ldg(&s.hmm[j]);
+    static __device__ __forceinline__ KinNb<float> kin(const State &s, int j, float) {
+        const float4 q = __ldg(&s.hmm[j]);   // (hsml comes in the same record)
         return {q.x, q.y, q.z};
     }
-    static __device__ __forceinline__ StressNb<float> stress(const State &s, const TauRec &t, int j) {
+    static __device__ __forceinline__ StressNb<float> stress(const State &s, const TauRec &t, int j, float hu) {
         const float4 q = __ldg(&t.tq[j]);
-        return {__ldg(&s.hsf[j]), q.w, q.x, q.y, q.z};
+        return {hu > 0.0f ? hu : __ldg(&s.hsf[j]), q.w, q.x, q.y, q.z};
     }
     static __device__ __forceinline__ StressNb<float> stress_rec(const TauRec &t, int j) {
         const float4 q = __ldg(&t.tq[j]);

@@ -79,6 +79,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<T>::kin) k_kinematic(KinArgs
     const double inv_hi = 1.0 / hi;
     KinSums<T> ks;     // -div and the velocity gradient, negated
     const T hiT = Nb<T>::h(s, i), inv_hiT = (T)inv_hi;
+    const T hu = (I.hmin == I.hmax) ? hiT : T(-1);   // (every neighbour's hsml is hi)
     typename Vec2<T>::type *dwr = reinterpret_cast<typename Vec2<T>::type *>(a.dw);
     int cnt = 0;       // entries in this thread's shared-memory list
     int npairs = 0;    // exact pairs found so far
@@ -90,7 +91,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<T>::kin) k_kinematic(KinArgs
             if (!SIMP_IN_RANGE(j, 0, a.n, SITE_NEIGHBOUR)) continue;
             if (done + k < kMaxPairs) a.pl.pj[(size_t)(done + k) * a.pl.stride + i] = j;
             const double2 q = __ldg(&s.xy[j]), v = __ldg(&s.vxy[j]);
-            const KinNb<T> nb = Nb<T>::kin(s, j);
+            const KinNb<T> nb = Nb<T>::kin(s, j, hu);
             const PairGeom<T> pg = pair_geom<T, false, SKF>(P, (T)(xi - q.x), (T)(yi - q.y), hiT, inv_hiT, nb.h);
             const T dwx = pg.gfac * pg.dx, dwy = pg.gfac * pg.dy;
             if (dwr && done + k < kDwRows) dwr[(size_t)(done + k) * a.pl.stride + i] = Vec2<T>::make(dwx, dwy);
@@ -215,7 +216,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<T>::kin) k_kin_sums(KinArgs 
     auto pair = [&](int k, int j) {
         if (!SIMP_IN_RANGE(j, 0, a.n, SITE_NEIGHBOUR)) return;
         const double2 q = __ldg(&s.xy[j]), v = __ldg(&s.vxy[j]);
-        const KinNb<T> nb = Nb<T>::kin(s, j);
+        const KinNb<T> nb = Nb<T>::kin(s, j, T(-1));
         const PairGeom<T> pg = pair_geom<T, false, SKF>(P, (T)(xi - q.x), (T)(yi - q.y), hiT, inv_hiT, nb.h);
         const T dwx = pg.gfac * pg.dx, dwy = pg.gfac * pg.dy;
         if (dwr && k < kDwRows) dwr[(size_t)k * a.pl.stride + i] = Vec2<T>::make(dwx, dwy);
@@ -249,10 +250,11 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<T>::stress) k_stress(StressA
     const bool dead = inst_dead(I.flags);   // see k_kinematic
     StressSums<T> ss;
     const T hiT = Nb<T>::h(s, i), inv_hiT = (T)inv_hi;
+    const T hu = (I.hmin == I.hmax) ? hiT : T(-1);   // (every neighbour's hsml is hi)
     auto accumulate = [&](int j) {
         if (!SIMP_IN_RANGE(j, 0, a.n, SITE_NEIGHBOUR)) return;
         const double2 q = __ldg(&s.xy[j]);
-        const StressNb<T> nb = Nb<T>::stress(s, a.rec, j);
+        const StressNb<T> nb = Nb<T>::stress(s, a.rec, j, hu);
         const PairGeom<T> pg = pair_geom<T, false, SKF>(P, (T)(xi - q.x), (T)(yi - q.y), hiT, inv_hiT, nb.h);
         ss.add(pg.gfac * pg.dx, pg.gfac * pg.dy, nb.m, nb.t11, nb.t12, nb.t22);
     };

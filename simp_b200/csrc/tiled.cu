@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(kMaxTileThreads) k_kin_tiled(KinArgs a) {
     if (fits) {
         for_halo(h, [&](int j, int k) {
             const double2 q = s.xy[j], v = s.vxy[j];
-            const KinNb<T> nb = Nb<T>::kin(s, j);
+            const KinNb<T> nb = Nb<T>::kin(s, j, T(-1));
             tl.x[k] = q.x;
             tl.y[k] = q.y;
             tl.hs[k] = s.hs[j];
@@ -330,7 +330,7 @@ __global__ void __launch_bounds__(kMaxTileThreads) k_kin_tiled(KinArgs a) {
         auto on_pair = [&](int j) {
             if (npairs < kMaxPairs) pl.pj[(size_t)npairs * pl.stride + i] = j;
             const double2 q = s.xy[j], v = s.vxy[j];
-            const KinNb<T> nb = Nb<T>::kin(s, j);
+            const KinNb<T> nb = Nb<T>::kin(s, j, T(-1));
             pair_terms(npairs, q.x, q.y, nb.h, v.x, v.y, nb.m, nb.mor);
             ++npairs;
         };
@@ -403,7 +403,7 @@ __global__ void __launch_bounds__(kMaxTileThreads) k_stress_tiled(StressArgs a) 
     if (fits) {
         for_halo(h, [&](int j, int k) {
             const double2 q = s.xy[j];
-            const StressNb<T> nb = Nb<T>::stress(s, a.rec, j);
+            const StressNb<T> nb = Nb<T>::stress(s, a.rec, j, T(-1));
             tl.x[k] = q.x;
             tl.y[k] = q.y;
             tl.hT[k] = nb.h;
@@ -429,7 +429,7 @@ __global__ void __launch_bounds__(kMaxTileThreads) k_stress_tiled(StressArgs a) 
     };
     auto global_terms = [&](int j) {
         const double2 q = s.xy[j];
-        const StressNb<T> nb = Nb<T>::stress(s, a.rec, j);
+        const StressNb<T> nb = Nb<T>::stress(s, a.rec, j, T(-1));
         terms(q.x, q.y, nb.h, nb.m, nb.t11, nb.t12, nb.t22);
     };
     auto any_terms = [&](int j) {
