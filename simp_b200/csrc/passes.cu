@@ -20,8 +20,11 @@ constexpr int kBlock = SIMP_PASS_BLOCK;   // threads per block of the gather pas
 // Up to this many particles in a context the kinematic pass runs as two
 // kernels (k_find_pairs, k_kin_sums), above it as one (k_kinematic), unless
 // the context names one form (SIMP_PASSES_GATHER_ONE / _TWO).  The
-// two-kernel pass writes and re-reads the pair list, which pays while that
-// round trip stays in L2.  Per pass, one kernel -> two (B200, basins of the
+// two-kernel pass writes and re-reads the pair list; it is the faster form
+// up to this size, the slower one above it, also when it runs in chunks
+// whose pair lists stay in L2 (1,048,576 particles in chunks of 131,072 to
+// 400,000: FP64 274 -> 310..374 us, mixed 242 -> 300..314 us against the
+// one-kernel pass).  Per pass, one kernel -> two (B200, basins of the
 // 500 m lattice), FP64: 147,456 particles 64.6 -> 55.1 us, 262,144 96.4 ->
 // 89.2, 409,600 143.0 -> 143.3, 524,176 170.5 -> 179.8, 1,048,576 305.7 ->
 // 343.9; mixed: 147,456 66.5 -> 53.3, 262,144 100.1 -> 87.5, 409,600
