@@ -232,7 +232,7 @@ int32_t simp_server_create(const simp_params *params, const simp_server_config *
     *out = s;
     s->prm = *params;
     s->cfg = *cfg;
-    const double per = simp::bytes_per_particle(s->prm) + kBytesPerWall / kWallsPerParticleDiv;
+    const double per = simp::bytes_per_particle(s->prm, cfg->max_instances == 1) + kBytesPerWall / kWallsPerParticleDiv;
     double budget = cfg->hbm_budget_bytes;
     if (cfg->spot_every > 0) {
         simp_params p64 = s->prm;
@@ -240,7 +240,9 @@ int32_t simp_server_create(const simp_params *params, const simp_server_config *
         const double spot_n = 2.0 * cfg->max_request_particles;
         s->maxn_spot = (int)spot_n;
         s->maxnb_spot = std::max(1, s->maxn_spot / kWallsPerParticleDiv);
-        budget -= spot_n * (simp::bytes_per_particle(p64, true) + kBytesPerWall / kWallsPerParticleDiv);
+        // (a batch of one slot is a single-basin context, with its read-back stage)
+        const bool single = std::min(cfg->max_instances, kSpotSlots) == 1;
+        budget -= spot_n * (simp::bytes_per_particle(p64, single) + kBytesPerWall / kWallsPerParticleDiv);
     }
     const double cap = std::floor(budget / per);
     if (cap < cfg->max_request_particles)
