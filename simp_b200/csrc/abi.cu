@@ -1479,7 +1479,10 @@ int32_t simp_gpu_set_state(simp_ctx *c, int32_t ntotal, const double *x, const d
         return simp_fail(c, SIMP_ERR_MAXN,
                          "The number of boundary particles generated is higher than the maximum "
                          "allowed. (boundaries.f90:296-303)");
-    if (ntotal < 1) return simp_fail(c, SIMP_ERR_BADARG, "set_state: bad sizes or null arrays");
+    // (refused before anything changes: the resident state stays)
+    if (ntotal < 1 || ntotalb < 0 || !x || !vx || !mass || !rho || !hsml || !A || !h ||
+        (ntotalb > 0 && (!xb || !massb)))
+        return simp_fail(c, SIMP_ERR_BADARG, "set_state: bad sizes or null arrays");
     c->pending_check = false;   // (a new state replaces what steps without outputs left)
     const int cont = simp::continue_state(c, ntotal, x, vx, mass, rho, hsml, A, h, ntotalb, xb, massb, dt,
                                           current_time);
