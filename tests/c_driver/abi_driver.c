@@ -119,6 +119,15 @@ int main(void) {
     }
     if (!(ke > 0.0)) { fprintf(stderr, "nothing moved\n"); return 1; }
 
+    /* a host that hands the state over every step: set_state of what
+       get_state returned, a step without outputs, get_state with time and dt */
+    for (int k = 0; k < 3; ++k) {
+        CHECK(simp_gpu_set_state(ctx, n, x, vx, mass, rho, hsml, A, h, nb, xb, massb, dt, t));
+        CHECK(simp_gpu_step(ctx, 1, NULL, NULL));
+        CHECK(simp_gpu_get_state(ctx, x, vx, mass, rho, hsml, A, h, &dt, &t));
+    }
+    if (t != 13.0) { fprintf(stderr, "time after the host loop %g\n", t); return 1; }
+
     /* capacity error of set_state */
     if (simp_gpu_set_state(ctx, n + 1, x, vx, mass, rho, hsml, A, h, nb, xb, massb, 1.0, 0.0) != SIMP_ERR_MAXN) {
         fprintf(stderr, "maxn not reported\n");
