@@ -32,8 +32,9 @@ constexpr int kBlock = SIMP_PASS_BLOCK;   // threads per block of the gather pas
 constexpr int kSplitMaxParticles = 400000;
 // minimum resident blocks per SM, per precision form, measured against 4..8
 // (cfg2 FP64, cfg3 mixed): the FP64 kinematic pass keeps its pair math in
-// registers (cap 102), the FP32 passes and the FP64 stress pass trade
-// registers for warps in flight (caps 64 and 73)
+// registers (cap 102), the other passes trade registers for warps in
+// flight (caps 64 and 73; the FP32 kinematic pass at 7 blocks, 241 -> 235
+// us per pass at cfg3 against 8, the same at cfg2's size)
 #ifndef SIMP_KIN_MIN_BLOCKS
 #define SIMP_KIN_MIN_BLOCKS 5
 #endif
@@ -41,7 +42,7 @@ constexpr int kSplitMaxParticles = 400000;
 #define SIMP_STRESS_MIN_BLOCKS 7
 #endif
 #ifndef SIMP_KIN_MIN_BLOCKS_F32
-#define SIMP_KIN_MIN_BLOCKS_F32 8
+#define SIMP_KIN_MIN_BLOCKS_F32 7
 #endif
 #ifndef SIMP_STRESS_MIN_BLOCKS_F32
 #define SIMP_STRESS_MIN_BLOCKS_F32 8
