@@ -30,13 +30,18 @@ constexpr int kBlock = SIMP_PASS_BLOCK;   // threads per block of the gather pas
 // 343.9; mixed: 147,456 66.5 -> 53.3, 262,144 100.1 -> 87.5, 409,600
 // 134.7 -> 131.9, 1,048,576 241 -> 267.
 constexpr int kSplitMaxParticles = 400000;
-// minimum resident blocks per SM, per precision form, measured against 4..8
-// (cfg2 FP64, cfg3 mixed): the FP64 kinematic pass keeps its pair math in
-// registers (cap 102), the other passes trade registers for warps in
-// flight (caps 64 and 73; the FP32 kinematic pass at 7 blocks, 241 -> 235
-// us per pass at cfg3 against 8, the same at cfg2's size)
+// minimum resident blocks per SM, per precision form and kernel, measured
+// against 4..8: the FP64 sums kernel of the two-kernel pass keeps its pair
+// math in registers (5 blocks, cap 102; 6 is 3% slower at cfg2); the
+// one-kernel pass, which runs above kSplitMaxParticles, at 6 blocks (cfg3
+// FP64: 274, 249, 261 us per pass at 5, 6, 7; the FP32 form at 7 blocks,
+// 253, 235, 241 at 6, 7, 8); the stress passes at 7 (FP64: 6 and 8 are
+// 23% and 9% slower at cfg2) and 8 (FP32)
 #ifndef SIMP_KIN_MIN_BLOCKS
-#define SIMP_KIN_MIN_BLOCKS 5
+#define SIMP_KIN_MIN_BLOCKS 6
+#endif
+#ifndef SIMP_SUMS_MIN_BLOCKS
+#define SIMP_SUMS_MIN_BLOCKS 5
 #endif
 #ifndef SIMP_STRESS_MIN_BLOCKS
 #define SIMP_STRESS_MIN_BLOCKS 7
@@ -49,11 +54,11 @@ constexpr int kSplitMaxParticles = 400000;
 #endif
 template <class T>
 struct MinBlocks {
-    static constexpr int kin = SIMP_KIN_MIN_BLOCKS, stress = SIMP_STRESS_MIN_BLOCKS;
+    static constexpr int kin = SIMP_KIN_MIN_BLOCKS, sums = SIMP_SUMS_MIN_BLOCKS, stress = SIMP_STRESS_MIN_BLOCKS;
 };
 template <>
 struct MinBlocks<float> {
-    static constexpr int kin = SIMP_KIN_MIN_BLOCKS_F32, stress = SIMP_STRESS_MIN_BLOCKS_F32;
+    static constexpr int kin = SIMP_KIN_MIN_BLOCKS_F32, sums = SIMP_KIN_MIN_BLOCKS_F32, stress = SIMP_STRESS_MIN_BLOCKS_F32;
 };
 // per-thread pair list in shared memory: a typical particle's pairs fit;
 // a longer list is processed in batches.  Kept small: the shared memory of
@@ -206,7 +211,7 @@ __global__ void __launch_bounds__(kBlock, SIMP_FIND_MIN_BLOCKS) k_find_pairs(Kin
 }
 
 template <class T, int SKF>
-__global__ void __launch_bounds__(kBlock, MinBlocks<T>::kin) k_kin_sums(KinArgs a) {
+__global__ void __launch_bounds__(kBlock, MinBlocks<T>::sums) k_kin_sums(KinArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const State &s = a.s;
