@@ -36,7 +36,8 @@ constexpr int kSplitMaxParticles = 400000;
 // one-kernel pass, which runs above kSplitMaxParticles, at 6 blocks (cfg3
 // FP64: 274, 249, 261 us per pass at 5, 6, 7; the FP32 form at 7 blocks,
 // 253, 235, 241 at 6, 7, 8); the stress passes at 7 (FP64: 6 and 8 are
-// 23% and 9% slower at cfg2) and 8 (FP32)
+// 23% and 9% slower at cfg2) and 8 (FP32: 6 and 7 are 10% and 9% slower at
+// cfg3)
 #ifndef SIMP_KIN_MIN_BLOCKS
 #define SIMP_KIN_MIN_BLOCKS 6
 #endif
